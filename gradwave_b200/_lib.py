@@ -1,0 +1,118 @@
+"""ctypes binding of libgwb.so (the C ABI declared in include/gwb.h).
+
+The library is loaded on first use. There is no fallback: if libgwb.so is
+missing or CUDA is unavailable, every compute entry raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+import torch
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libgwb.so"
+
+GWB_OK = 0
+GWB_ERR_ARG = 1
+GWB_ERR_CUDA = 2
+GWB_ERR_NONFINITE = 3
+GWB_ERR_TIMEOUT = 4
+GWB_ERR_NOT_CONVERGED = 5
+GWB_ERR_ALLOC = 6
+GWB_ERR_BREAKDOWN = 7
+
+GWB_C64 = 0
+GWB_C128 = 1
+GWB_FP32 = 0
+GWB_FP64 = 1
+
+_STATUS_NAMES = {1: "bad argument", 2: "CUDA error", 3: "non-finite value", 4: "device wait timeout",
+                 5: "not converged", 6: "allocation failed", 7: "Cholesky breakdown"}
+
+
+class GwbError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"libgwb status {status} ({_STATUS_NAMES.get(status, '?')}): {msg}")
+        self.status = status
+
+
+class Geometry(ctypes.Structure):
+    _fields_ = [("nk", ctypes.c_int32), ("npw_max", ctypes.c_int32), ("n", ctypes.c_int32 * 3),
+                ("nproj", ctypes.c_int32), ("npw", ctypes.POINTER(ctypes.c_int64)),
+                ("flat_idx", ctypes.POINTER(ctypes.c_int64))]
+
+
+_lock = threading.Lock()
+_lib = None
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int32
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+
+# name -> argtypes (every function returns int status unless listed in _RESTYPES)
+_SIGNATURES = {
+    "gwb_last_error": [],
+    "gwb_version": [],
+    "gwb_ham_create": [ctypes.POINTER(Geometry), ctypes.c_int, ctypes.POINTER(_P)],
+    "gwb_ham_destroy": [_P],
+    "gwb_ham_set_kinetic": [_P, _P, _P],
+    "gwb_ham_set_potential": [_P, _P, _P],
+    "gwb_ham_set_projectors": [_P, _P, _P, _P],
+    "gwb_ham_apply": [_P, _P, _P, _I, _I, _I, _P],
+    "gwb_ham_scratch_bytes": [_P],
+}
+_RESTYPES = {"gwb_last_error": ctypes.c_char_p, "gwb_version": ctypes.c_char_p,
+             "gwb_ham_scratch_bytes": ctypes.c_size_t}
+
+
+def declared_symbols() -> list[str]:
+    """Every entry point the binding expects the library to export."""
+    return sorted(_SIGNATURES)
+
+
+def load() -> ctypes.CDLL:
+    """The loaded library (raises if it was not built)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not LIB_PATH.exists():
+                raise RuntimeError(
+                    f"{LIB_PATH} is missing: build it with `python -m gradwave_b200.build` "
+                    "(there is no CPU fallback)")
+            lib = ctypes.CDLL(str(LIB_PATH))
+            for name, args in _SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.argtypes = args
+                fn.restype = _RESTYPES.get(name, ctypes.c_int)
+            _lib = lib
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != GWB_OK:
+        raise GwbError(status, load().gwb_last_error().decode())
+
+
+def call(name: str, *args) -> None:
+    check(getattr(load(), name)(*args))
+
+
+def require_cuda(t: torch.Tensor, what: str) -> None:
+    if not t.is_cuda:
+        raise RuntimeError(f"{what} must be a CUDA tensor (the band-solve path has no CPU fallback)")
+
+
+def stream_ptr(device: torch.device | None = None) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def io_dtype(t: torch.Tensor) -> int:
+    if t.dtype == torch.complex128:
+        return GWB_C128
+    if t.dtype == torch.complex64:
+        return GWB_C64
+    raise TypeError(f"expected complex64/complex128, got {t.dtype}")

@@ -1,0 +1,655 @@
+// Batched plane-wave Hamiltonian apply H c = T c + V_loc c + sum p D <p|c>
+// for all k-points and bands in a few launches (sm_100a).
+//
+// Local term (replaces gradwave core/batch.py:405-428). The sphere of each k
+// occupies Miller indices |m_a| <= M_a of a box n0 x n1 x n2, so only
+// L_a = 2 M_a + 1 planes/rows/columns per axis ever hold data:
+//
+//   K1 plane_inverse  one CTA per (axis-0 plane j0 < L0, band, k):
+//                     scatter the sphere points of the plane into a shared-
+//                     memory n1 x n2 plane, inverse FFT along axis 2 on the L1
+//                     occupied rows, inverse FFT along axis 1 on all columns,
+//                     store the plane to the scratch W (L0 planes per band).
+//   K2 pencil_vloc    one CTA per (axis-1 row i1, band, k): load the L0 planes'
+//                     row i1 as n2 pencils along axis 0, inverse FFT, multiply
+//                     by v(r)/N, forward FFT, store back the L0 occupied planes
+//                     (the V(r) psi(r) product never leaves shared memory).
+//   K3 plane_forward  one CTA per (j0, band, k): forward FFT along axis 1 and
+//                     along axis 2 on the occupied rows, gather the sphere,
+//                     add the kinetic term t c, write out (padding zeroed).
+//
+// The bands are processed in chunks whose scratch W fits in L2, so W is
+// written and re-read from L2 rather than HBM.
+//
+// Nonlocal term (replaces gradwave core/batch.py:499-500 and becp_b :590-595):
+//   K4 becp_partial   becp partial sums conj(p) . c over a slice of G
+//   K5 becp_reduce_d  sum of slices, times D  -> bd (nk, nb, nproj)
+//   K6 nl_add         out += bd . p
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace gwb {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+struct FftGeom {
+  int n[3];
+  int M[3];  // max |Miller index| per axis over all k (compact row map)
+  int L[3];  // occupied extent per axis (2M+1, capped at n)
+  AxisPlan plan[3];
+};
+
+}  // namespace gwb
+
+struct gwb_ham {
+  int device = 0;
+  int nk = 0, npw_max = 0, nproj = 0;
+  gwb::FftGeom g{};
+  std::vector<int64_t> npw_host;
+  // device tables
+  int* d_npw = nullptr;
+  int* d_plane_ptr = nullptr;  // (nk*L0 + 1)
+  int* d_plane_g = nullptr;    // sphere index of each plane entry
+  int* d_plane_pos = nullptr;  // i1*n2 + i2 of each plane entry
+  double* d_t64 = nullptr;
+  float* d_t32 = nullptr;
+  double* d_v64 = nullptr;  // v(r)/N
+  float* d_v32 = nullptr;
+  gwb::cplx<double>* d_p64 = nullptr;
+  gwb::cplx<float>* d_p32 = nullptr;
+  double* d_d64 = nullptr;
+  float* d_d32 = nullptr;
+  gwb::cplx<double>* d_tw64[3] = {nullptr, nullptr, nullptr};
+  gwb::cplx<float>* d_tw32[3] = {nullptr, nullptr, nullptr};
+  // scratch
+  void* d_W = nullptr;
+  size_t W_bytes = 0;
+  void* d_part = nullptr;  // becp partials
+  size_t part_bytes = 0;
+  void* d_bd = nullptr;  // becp * D
+  size_t bd_bytes = 0;
+  bool have_t = false, have_v = false, have_p = false;
+};
+
+namespace gwb {
+
+static bool plan_axis(int n, AxisPlan* pl) {
+  if (n < 2 || n > 128) return false;
+  pl->n = n;
+  pl->nst = 0;
+  pl->code = 0;
+  int m = n;
+  const int order[7] = {8, 4, 6, 3, 2, 5, 7};
+  while (m > 1) {
+    bool found = false;
+    for (int R : order) {
+      if (m % R == 0) {
+        if (pl->nst >= 8) return false;
+        pl->code |= (unsigned)R << (4 * pl->nst);
+        pl->nst++;
+        m /= R;
+        found = true;
+        break;
+      }
+    }
+    if (!found) return false;
+  }
+  return true;
+}
+
+static size_t w_budget_bytes() {
+  const char* s = std::getenv("GWB_W_BUDGET_MB");
+  long mb = s ? std::atol(s) : 48;
+  if (mb < 1) mb = 1;
+  return (size_t)mb << 20;
+}
+
+// ---------------------------------------------------------------------------
+// K1: sphere scatter + inverse FFT along axes 2 and 1, one plane per CTA.
+template <typename T, typename SIO, unsigned C1, unsigned C2>
+__global__ void __launch_bounds__(256, (C1 && C2) ? 3 : 1) k_plane_inverse(FftGeom g, const int* __restrict__ plane_ptr,
+                                                       const int* __restrict__ plane_g,
+                                                       const int* __restrict__ plane_pos,
+                                                       const SIO* __restrict__ c, cplx<T>* __restrict__ W,
+                                                       const cplx<T>* __restrict__ tw1,
+                                                       const cplx<T>* __restrict__ tw2, int nb, int b0,
+                                                       int nbc, int npw_max) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n1 = g.n[1], n2 = g.n[2], L0 = g.L[0];
+  const int j0 = blockIdx.x, bl = blockIdx.y, k = blockIdx.z;
+  cplx<T>* S = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* t1 = S + n1 * n2;
+  cplx<T>* t2 = t1 + n1;
+  for (int i = threadIdx.x; i < n1; i += blockDim.x) t1[i] = tw1[i];
+  for (int i = threadIdx.x; i < n2; i += blockDim.x) t2[i] = tw2[i];
+  for (int i = threadIdx.x; i < n1 * n2; i += blockDim.x) S[i] = mk<T>(0, 0);
+  __syncthreads();
+  const size_t crow = ((size_t)k * nb + (b0 + bl)) * npw_max;
+  const int e0 = plane_ptr[k * L0 + j0], e1 = plane_ptr[k * L0 + j0 + 1];
+  for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) S[plane_pos[e]] = ld<T>(c, crow + plane_g[e]);
+  __syncthreads();
+  fft_any<T, false, +1, C2>(S, g.L[1], g.plan[2], n2, 1, g.M[1], n1, t2);
+  fft_any<T, true, +1, C1>(S, n2, g.plan[1], 1, n2, n2, n2, t1);
+  cplx<T>* dst = W + (((size_t)k * nbc + bl) * L0 + j0) * (size_t)(n1 * n2);
+  for (int i = threadIdx.x; i < n1 * n2; i += blockDim.x) dst[i] = S[i];
+}
+
+// K2: pencils along axis 0 for one (i1, band, k): inverse FFT, x v(r)/N, forward FFT.
+template <typename T, unsigned C0>
+__global__ void __launch_bounds__(256, C0 ? 3 : 1) k_pencil_vloc(FftGeom g, cplx<T>* __restrict__ W,
+                                                     const T* __restrict__ v,
+                                                     const cplx<T>* __restrict__ tw0, int nbc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2], L0 = g.L[0];
+  const int i1 = blockIdx.x, bl = blockIdx.y, k = blockIdx.z;
+  cplx<T>* S = reinterpret_cast<cplx<T>*>(smem_raw);  // [i0][i2]
+  cplx<T>* t0 = S + n0 * n2;
+  for (int i = threadIdx.x; i < n0; i += blockDim.x) t0[i] = tw0[i];
+  cplx<T>* base = W + ((size_t)k * nbc + bl) * L0 * (size_t)(n1 * n2) + (size_t)i1 * n2;
+  for (int i = threadIdx.x; i < n0 * n2; i += blockDim.x) {
+    const int r = i / n2, i2 = i - r * n2;
+    // memory row r holds compact plane j0 (or stays zero)
+    int j0;
+    if (r <= g.M[0]) j0 = r;
+    else if (r >= n0 - (L0 - g.M[0] - 1)) j0 = r - (n0 - L0);
+    else j0 = -1;
+    S[i] = j0 >= 0 ? base[(size_t)j0 * n1 * n2 + i2] : mk<T>(0, 0);
+  }
+  __syncthreads();
+  fft_any<T, true, +1, C0>(S, n2, g.plan[0], 1, n2, n2, n2, t0);
+  for (int i = threadIdx.x; i < n0 * n2; i += blockDim.x) {
+    const int i0 = i / n2, i2 = i - i0 * n2;
+    S[i] = scale(S[i], v[((size_t)i0 * n1 + i1) * n2 + i2]);
+  }
+  __syncthreads();
+  fft_any<T, true, -1, C0>(S, n2, g.plan[0], 1, n2, n2, n2, t0);
+  for (int i = threadIdx.x; i < L0 * n2; i += blockDim.x) {
+    const int j0 = i / n2, i2 = i - j0 * n2;
+    const int r = rowmap(j0, g.M[0], L0, n0);
+    base[(size_t)j0 * n1 * n2 + i2] = S[r * n2 + i2];
+  }
+}
+
+// K3: forward FFT along axes 1 and 2, sphere gather, + t c, padding zeroed.
+template <typename T, typename SIO, unsigned C1, unsigned C2>
+__global__ void __launch_bounds__(256, (C1 && C2) ? 3 : 1) k_plane_forward(
+    FftGeom g, const int* __restrict__ plane_ptr, const int* __restrict__ plane_g,
+    const int* __restrict__ plane_pos, const int* __restrict__ npw, const SIO* __restrict__ c,
+    SIO* __restrict__ out, const cplx<T>* __restrict__ W, const T* __restrict__ t,
+    const cplx<T>* __restrict__ tw1, const cplx<T>* __restrict__ tw2, int nb, int b0, int nbc,
+    int npw_max) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n1 = g.n[1], n2 = g.n[2], L0 = g.L[0];
+  const int j0 = blockIdx.x, bl = blockIdx.y, k = blockIdx.z;
+  cplx<T>* S = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* t1 = S + n1 * n2;
+  cplx<T>* t2 = t1 + n1;
+  for (int i = threadIdx.x; i < n1; i += blockDim.x) t1[i] = tw1[i];
+  for (int i = threadIdx.x; i < n2; i += blockDim.x) t2[i] = tw2[i];
+  const cplx<T>* src = W + (((size_t)k * nbc + bl) * L0 + j0) * (size_t)(n1 * n2);
+  for (int i = threadIdx.x; i < n1 * n2; i += blockDim.x) S[i] = src[i];
+  __syncthreads();
+  fft_any<T, true, -1, C1>(S, n2, g.plan[1], 1, n2, n2, n2, t1);
+  fft_any<T, false, -1, C2>(S, g.L[1], g.plan[2], n2, 1, g.M[1], n1, t2);
+  const size_t crow = ((size_t)k * nb + (b0 + bl)) * npw_max;
+  const int e0 = plane_ptr[k * L0 + j0], e1 = plane_ptr[k * L0 + j0 + 1];
+  const T* tk = t + (size_t)k * npw_max;
+  for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    const int gi = plane_g[e];
+    cplx<T> cv = ld<T>(c, crow + gi);
+    st(out, crow + gi, S[plane_pos[e]] + scale(cv, tk[gi]));
+  }
+  if (j0 == 0) {
+    for (int gi = npw[k] + threadIdx.x; gi < npw_max; gi += blockDim.x) st(out, crow + gi, mk<T>(0, 0));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Nonlocal term. Tiles: TB bands x TP projectors, G slices of TG.
+constexpr int NL_TB = 16, NL_TP = 32, NL_TG = 32;
+
+// K4: part[s][k][b][p] = sum_{g in slice s} conj(P[k][p][g]) c[k][b][g]
+template <typename T, typename SIO>
+__global__ void __launch_bounds__(256) k_becp_partial(const SIO* __restrict__ c,
+                                                      const cplx<T>* __restrict__ P,
+                                                      cplx<T>* __restrict__ part, int nk, int nb,
+                                                      int nproj, int npw_max, int gslice) {
+  __shared__ cplx<T> sc[NL_TB][NL_TG + 1];
+  __shared__ cplx<T> sp[NL_TP][NL_TG + 1];
+  const int pt = blockIdx.x, bt = blockIdx.y;
+  const int k = blockIdx.z % nk, s = blockIdx.z / nk;
+  const int tid = threadIdx.x;
+  const int lb = tid / 16, lp = tid % 16;  // each thread: band lb, projectors lp and lp+16
+  cplx<T> acc0 = mk<T>(0, 0), acc1 = mk<T>(0, 0);
+  const int g_begin = s * gslice, g_end = min(npw_max, g_begin + gslice);
+  for (int gb = g_begin; gb < g_end; gb += NL_TG) {
+    for (int i = tid; i < NL_TB * NL_TG; i += blockDim.x) {
+      const int bb = i / NL_TG, gg = i % NL_TG;
+      const int b = bt * NL_TB + bb, gi = gb + gg;
+      sc[bb][gg] = (b < nb && gi < g_end) ? ld<T>(c, ((size_t)k * nb + b) * npw_max + gi) : mk<T>(0, 0);
+    }
+    for (int i = tid; i < NL_TP * NL_TG; i += blockDim.x) {
+      const int pp = i / NL_TG, gg = i % NL_TG;
+      const int p = pt * NL_TP + pp, gi = gb + gg;
+      sp[pp][gg] = (p < nproj && gi < g_end) ? P[((size_t)k * nproj + p) * npw_max + gi] : mk<T>(0, 0);
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int gg = 0; gg < NL_TG; ++gg) {
+      const cplx<T> cv = sc[lb][gg];
+      acc0 = acc0 + conj_mul(sp[lp][gg], cv);
+      acc1 = acc1 + conj_mul(sp[lp + 16][gg], cv);
+    }
+    __syncthreads();
+  }
+  const int b = bt * NL_TB + lb;
+  if (b < nb) {
+    const size_t row = (((size_t)s * nk + k) * nb + b) * nproj;
+    const int p0 = pt * NL_TP + lp, p1 = p0 + 16;
+    if (p0 < nproj) part[row + p0] = acc0;
+    if (p1 < nproj) part[row + p1] = acc1;
+  }
+}
+
+// K5: bd[k][b][q] = sum_p (sum_s part[s][k][b][p]) D[p][q]
+template <typename T>
+__global__ void k_becp_reduce_d(const cplx<T>* __restrict__ part, const T* __restrict__ D,
+                                cplx<T>* __restrict__ bd, int nk, int nb, int nproj, int nslice) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* becp = reinterpret_cast<cplx<T>*>(smem_raw);  // nproj
+  const int kb = blockIdx.x;  // k*nb + b
+  const size_t stride = (size_t)nk * nb * nproj;
+  for (int p = threadIdx.x; p < nproj; p += blockDim.x) {
+    cplx<T> a = mk<T>(0, 0);
+    for (int s = 0; s < nslice; ++s) a = a + part[s * stride + (size_t)kb * nproj + p];
+    becp[p] = a;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < nproj; q += blockDim.x) {
+    cplx<T> a = mk<T>(0, 0);
+    for (int p = 0; p < nproj; ++p) a = a + scale(becp[p], D[(size_t)p * nproj + q]);
+    bd[(size_t)kb * nproj + q] = a;
+  }
+}
+
+// K6: out[k][b][g] += sum_q bd[k][b][q] P[k][q][g]; tiles TB bands x 64 G.
+template <typename T, typename SIO>
+__global__ void __launch_bounds__(256) k_nl_add(const cplx<T>* __restrict__ bd,
+                                                const cplx<T>* __restrict__ P,
+                                                SIO* __restrict__ out, int nk, int nb, int nproj,
+                                                int npw_max) {
+  constexpr int TGO = 64, TQ = 16;
+  __shared__ cplx<T> sb[NL_TB][TQ];
+  __shared__ cplx<T> sp[TQ][TGO];
+  const int gt = blockIdx.x, bt = blockIdx.y, k = blockIdx.z;
+  const int tid = threadIdx.x;
+  const int lg = tid % TGO, lb0 = tid / TGO;  // 4 band groups x 64 g; each thread 4 bands
+  cplx<T> acc[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) acc[i] = mk<T>(0, 0);
+  for (int q0 = 0; q0 < nproj; q0 += TQ) {
+    for (int i = tid; i < NL_TB * TQ; i += blockDim.x) {
+      const int bb = i / TQ, qq = i % TQ;
+      const int b = bt * NL_TB + bb, q = q0 + qq;
+      sb[bb][qq] = (b < nb && q < nproj) ? bd[((size_t)k * nb + b) * nproj + q] : mk<T>(0, 0);
+    }
+    for (int i = tid; i < TQ * TGO; i += blockDim.x) {
+      const int qq = i / TGO, gg = i % TGO;
+      const int q = q0 + qq, gi = gt * TGO + gg;
+      sp[qq][gg] = (q < nproj && gi < npw_max) ? P[((size_t)k * nproj + q) * npw_max + gi] : mk<T>(0, 0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int qq = 0; qq < TQ; ++qq) {
+      const cplx<T> pv = sp[qq][lg];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) acc[i] = acc[i] + sb[lb0 * 4 + i][qq] * pv;
+    }
+    __syncthreads();
+  }
+  const int gi = gt * TGO + lg;
+  if (gi < npw_max) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int b = bt * NL_TB + lb0 * 4 + i;
+      if (b < nb) {
+        const size_t o = ((size_t)k * nb + b) * npw_max + gi;
+        st(out, o, ld<T>(out, o) + acc[i]);
+      }
+    }
+  }
+}
+
+template <typename T> __global__ void k_scale_copy(const double* src, T* dst, size_t n, double s) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (T)(src[i] * s);
+}
+__global__ void k_c128_to_c64(const cplx<double>* src, cplx<float>* dst, size_t n) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = mk<float>((float)src[i].x, (float)src[i].y);
+}
+
+static int ensure_buf(void** p, size_t* have, size_t need) {
+  if (*have >= need) return GWB_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *have = 0;
+  if (cudaMalloc(p, need) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("device allocation of " + std::to_string(need) + " bytes failed");
+    return GWB_ERR_ALLOC;
+  }
+  *have = need;
+  return GWB_OK;
+}
+
+static size_t plane_smem(const FftGeom& g, size_t es) {
+  return (size_t)(g.n[1] * g.n[2] + g.n[1] + g.n[2]) * es;
+}
+static size_t pencil_smem(const FftGeom& g, size_t es) {
+  return (size_t)(g.n[0] * g.n[2] + g.n[0]) * es;
+}
+
+static int nl_slices(const gwb_ham* h) {
+  // enough CTAs for the machine at small nb, bounded partial storage
+  int s = (h->npw_max + 2047) / 2048;
+  return std::max(1, std::min(s, 16));
+}
+
+// Compile-time FFT plans instantiated for the cubic boxes of the workloads
+// (24 = 8*3, 36 = 4*3*3, 72 = 8*3*3, 96 = 8*4*3); any other box runs the
+// runtime-plan kernels.
+constexpr unsigned kCode24 = 0x38u, kCode36 = 0x334u, kCode72 = 0x338u, kCode96 = 0x348u;
+
+template <typename T, typename SIO, unsigned C>
+static int local_chunks(gwb_ham* h, const SIO* c, SIO* out, int nb, int nbc, cudaStream_t st, size_t smA,
+                        size_t smB) {
+  const FftGeom& g = h->g;
+  const bool dbl = sizeof(T) == 8;
+  const cplx<T>* tw0 = dbl ? (const cplx<T>*)h->d_tw64[0] : (const cplx<T>*)h->d_tw32[0];
+  const cplx<T>* tw1 = dbl ? (const cplx<T>*)h->d_tw64[1] : (const cplx<T>*)h->d_tw32[1];
+  const cplx<T>* tw2 = dbl ? (const cplx<T>*)h->d_tw64[2] : (const cplx<T>*)h->d_tw32[2];
+  const T* v = dbl ? (const T*)h->d_v64 : (const T*)h->d_v32;
+  const T* t = dbl ? (const T*)h->d_t64 : (const T*)h->d_t32;
+  GWB_CUDA_TRY(cudaFuncSetAttribute(k_plane_inverse<T, SIO, C, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA));
+  GWB_CUDA_TRY(cudaFuncSetAttribute(k_plane_forward<T, SIO, C, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA));
+  GWB_CUDA_TRY(cudaFuncSetAttribute(k_pencil_vloc<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
+  cplx<T>* W = (cplx<T>*)h->d_W;
+  for (int b0 = 0; b0 < nb; b0 += nbc) {
+    const int cb = std::min(nbc, nb - b0);
+    dim3 gA(g.L[0], cb, h->nk), gB(g.n[1], cb, h->nk);
+    k_plane_inverse<T, SIO, C, C><<<gA, 256, smA, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos, c, W,
+                                                       tw1, tw2, nb, b0, cb, h->npw_max);
+    k_pencil_vloc<T, C><<<gB, 256, smB, st>>>(g, W, v, tw0, cb);
+    k_plane_forward<T, SIO, C, C><<<gA, 256, smA, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos,
+                                                       h->d_npw, c, out, W, t, tw1, tw2, nb, b0, cb,
+                                                       h->npw_max);
+    GWB_LAUNCH_CHECK();
+  }
+  return GWB_OK;
+}
+
+template <typename T, typename SIO>
+static int apply_impl(gwb_ham* h, const SIO* c, SIO* out, int nb, cudaStream_t st) {
+  const FftGeom& g = h->g;
+  const size_t es = sizeof(cplx<T>);
+  const size_t plane_elems = (size_t)g.n[1] * g.n[2];
+  const size_t per_band = (size_t)h->nk * g.L[0] * plane_elems * es;
+  size_t budget = std::max(w_budget_bytes(), per_band);
+  int nbc = (int)std::min<size_t>((size_t)nb, budget / per_band);
+  if (nbc < 1) nbc = 1;
+  int rc = ensure_buf(&h->d_W, &h->W_bytes, per_band * nbc);
+  if (rc) return rc;
+  const bool dbl = sizeof(T) == 8;
+  const size_t smA = plane_smem(g, es), smB = pencil_smem(g, es);
+  const unsigned c0 = g.plan[0].code, c1 = g.plan[1].code, c2 = g.plan[2].code;
+  const bool cubic = c0 == c1 && c1 == c2;
+  int rcl;
+  if (cubic && c0 == kCode24) rcl = local_chunks<T, SIO, kCode24>(h, c, out, nb, nbc, st, smA, smB);
+  else if (cubic && c0 == kCode36) rcl = local_chunks<T, SIO, kCode36>(h, c, out, nb, nbc, st, smA, smB);
+  else if (cubic && c0 == kCode72) rcl = local_chunks<T, SIO, kCode72>(h, c, out, nb, nbc, st, smA, smB);
+  else if (cubic && c0 == kCode96) rcl = local_chunks<T, SIO, kCode96>(h, c, out, nb, nbc, st, smA, smB);
+  else rcl = local_chunks<T, SIO, 0u>(h, c, out, nb, nbc, st, smA, smB);
+  if (rcl) return rcl;
+  if (h->nproj > 0) {
+    const int ns = nl_slices(h);
+    const int gslice = ((h->npw_max + ns - 1) / ns + NL_TG - 1) / NL_TG * NL_TG;
+    const int nsl = (h->npw_max + gslice - 1) / gslice;
+    rc = ensure_buf(&h->d_part, &h->part_bytes, (size_t)nsl * h->nk * nb * h->nproj * es);
+    if (rc) return rc;
+    rc = ensure_buf(&h->d_bd, &h->bd_bytes, (size_t)h->nk * nb * h->nproj * es);
+    if (rc) return rc;
+    const cplx<T>* P = dbl ? (const cplx<T>*)h->d_p64 : (const cplx<T>*)h->d_p32;
+    const T* D = dbl ? (const T*)h->d_d64 : (const T*)h->d_d32;
+    dim3 g4((h->nproj + NL_TP - 1) / NL_TP, (nb + NL_TB - 1) / NL_TB, h->nk * nsl);
+    k_becp_partial<T, SIO><<<g4, 256, 0, st>>>(c, P, (cplx<T>*)h->d_part, h->nk, nb, h->nproj, h->npw_max, gslice);
+    k_becp_reduce_d<T><<<h->nk * nb, 128, h->nproj * es, st>>>((const cplx<T>*)h->d_part, D, (cplx<T>*)h->d_bd,
+                                                            h->nk, nb, h->nproj, nsl);
+    dim3 g6((h->npw_max + 63) / 64, (nb + NL_TB - 1) / NL_TB, h->nk);
+    k_nl_add<T, SIO><<<g6, 256, 0, st>>>((const cplx<T>*)h->d_bd, P, out, h->nk, nb, h->nproj, h->npw_max);
+    GWB_LAUNCH_CHECK();
+  }
+  return GWB_OK;
+}
+
+}  // namespace gwb
+
+using namespace gwb;
+
+extern "C" {
+
+const char* gwb_last_error(void) { return g_last_error.c_str(); }
+const char* gwb_version(void) { return "gwb 0.1 sm_100a"; }
+
+int gwb_ham_create(const gwb_ham_geometry* geom, int device, gwb_ham** out) {
+  GWB_REQUIRE(geom && out, "null argument");
+  GWB_REQUIRE(geom->nk > 0 && geom->npw_max > 0 && geom->nproj >= 0, "bad nk/npw_max/nproj");
+  GWB_REQUIRE(geom->npw && geom->flat_idx, "null npw/flat_idx");
+  *out = nullptr;
+  auto* h = new gwb_ham();
+  h->device = device;
+  h->nk = geom->nk;
+  h->npw_max = geom->npw_max;
+  h->nproj = geom->nproj;
+  FftGeom& g = h->g;
+  for (int a = 0; a < 3; ++a) {
+    g.n[a] = geom->n[a];
+    if (!plan_axis(g.n[a], &g.plan[a])) {
+      delete h;
+      set_error("FFT axis length " + std::to_string(geom->n[a]) + " unsupported (need <=128, factors 2,3,5,7)");
+      return GWB_ERR_ARG;
+    }
+  }
+  const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+  const int64_t nbox = (int64_t)n0 * n1 * n2;
+  h->npw_host.assign(geom->npw, geom->npw + geom->nk);
+  // Miller extents over all k
+  int M[3] = {0, 0, 0};
+  for (int k = 0; k < h->nk; ++k) {
+    const int64_t np_k = h->npw_host[k];
+    if (np_k < 0 || np_k > h->npw_max) {
+      delete h;
+      set_error("npw[k] out of range");
+      return GWB_ERR_ARG;
+    }
+    for (int64_t gi = 0; gi < np_k; ++gi) {
+      const int64_t f = geom->flat_idx[(size_t)k * h->npw_max + gi];
+      if (f < 0 || f >= nbox) {
+        delete h;
+        set_error("flat_idx out of the box");
+        return GWB_ERR_ARG;
+      }
+      const int idx[3] = {(int)(f / ((int64_t)n1 * n2)), (int)((f / n2) % n1), (int)(f % n2)};
+      for (int a = 0; a < 3; ++a) {
+        const int m = idx[a] <= g.n[a] / 2 ? idx[a] : idx[a] - g.n[a];
+        M[a] = std::max(M[a], std::abs(m));
+      }
+    }
+  }
+  for (int a = 0; a < 3; ++a) {
+    g.L[a] = std::min(2 * M[a] + 1, g.n[a]);
+    g.M[a] = g.L[a] == g.n[a] ? g.n[a] : M[a];
+  }
+  const int L0 = g.L[0];
+  // sphere points grouped by compact axis-0 plane
+  std::vector<int> cnt((size_t)h->nk * L0 + 1, 0);
+  auto compact0 = [&](int i0) -> int {
+    if (g.L[0] == n0) return i0;
+    if (i0 <= g.M[0]) return i0;
+    return i0 - (n0 - L0);
+  };
+  for (int k = 0; k < h->nk; ++k)
+    for (int64_t gi = 0; gi < h->npw_host[k]; ++gi) {
+      const int64_t f = geom->flat_idx[(size_t)k * h->npw_max + gi];
+      cnt[(size_t)k * L0 + compact0((int)(f / ((int64_t)n1 * n2))) + 1]++;
+    }
+  for (size_t i = 1; i < cnt.size(); ++i) cnt[i] += cnt[i - 1];
+  const int total = cnt.back();
+  std::vector<int> pg(std::max(total, 1)), pp(std::max(total, 1));
+  std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+  for (int k = 0; k < h->nk; ++k)
+    for (int64_t gi = 0; gi < h->npw_host[k]; ++gi) {
+      const int64_t f = geom->flat_idx[(size_t)k * h->npw_max + gi];
+      const int slot = fill[(size_t)k * L0 + compact0((int)(f / ((int64_t)n1 * n2)))]++;
+      pg[slot] = (int)gi;
+      pp[slot] = (int)(f % ((int64_t)n1 * n2));
+    }
+  std::vector<int> npw32(h->npw_host.begin(), h->npw_host.end());
+  // twiddles exp(-2 pi i t / n), computed in double on the host
+  std::vector<cplx<double>> tw64[3];
+  std::vector<cplx<float>> tw32[3];
+  for (int a = 0; a < 3; ++a) {
+    for (int t = 0; t < g.n[a]; ++t) {
+      const double ang = -2.0 * M_PI * (double)t / (double)g.n[a];
+      tw64[a].push_back(mk<double>(std::cos(ang), std::sin(ang)));
+      tw32[a].push_back(mk<float>((float)std::cos(ang), (float)std::sin(ang)));
+    }
+  }
+  auto fail = [&](cudaError_t e) {
+    set_error(std::string("gwb_ham_create: ") + cudaGetErrorString(e));
+    gwb_ham_destroy(h);
+    return GWB_ERR_CUDA;
+  };
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return fail(e);
+#define GWB_ALLOC_COPY(dst, vec)                                                            \
+  do {                                                                                      \
+    e = cudaMalloc((void**)&(dst), (vec).size() * sizeof((vec)[0]));                        \
+    if (e != cudaSuccess) return fail(e);                                                   \
+    e = cudaMemcpy((dst), (vec).data(), (vec).size() * sizeof((vec)[0]), cudaMemcpyHostToDevice); \
+    if (e != cudaSuccess) return fail(e);                                                   \
+  } while (0)
+  GWB_ALLOC_COPY(h->d_plane_ptr, cnt);
+  GWB_ALLOC_COPY(h->d_plane_g, pg);
+  GWB_ALLOC_COPY(h->d_plane_pos, pp);
+  GWB_ALLOC_COPY(h->d_npw, npw32);
+  for (int a = 0; a < 3; ++a) {
+    GWB_ALLOC_COPY(h->d_tw64[a], tw64[a]);
+    GWB_ALLOC_COPY(h->d_tw32[a], tw32[a]);
+  }
+#undef GWB_ALLOC_COPY
+  const size_t nkp = (size_t)h->nk * h->npw_max;
+  if ((e = cudaMalloc((void**)&h->d_t64, nkp * 8)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc((void**)&h->d_t32, nkp * 4)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc((void**)&h->d_v64, nbox * 8)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc((void**)&h->d_v32, nbox * 4)) != cudaSuccess) return fail(e);
+  if (h->nproj > 0) {
+    const size_t np = (size_t)h->nk * h->nproj * h->npw_max;
+    if ((e = cudaMalloc((void**)&h->d_p64, np * 16)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc((void**)&h->d_p32, np * 8)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc((void**)&h->d_d64, (size_t)h->nproj * h->nproj * 8)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc((void**)&h->d_d32, (size_t)h->nproj * h->nproj * 4)) != cudaSuccess) return fail(e);
+  }
+  *out = h;
+  return GWB_OK;
+}
+
+int gwb_ham_destroy(gwb_ham* h) {
+  if (!h) return GWB_OK;
+  void* ptrs[] = {h->d_npw, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos, h->d_t64, h->d_t32, h->d_v64,
+                  h->d_v32, h->d_p64, h->d_p32, h->d_d64, h->d_d32, h->d_W, h->d_part, h->d_bd,
+                  h->d_tw64[0], h->d_tw64[1], h->d_tw64[2], h->d_tw32[0], h->d_tw32[1], h->d_tw32[2]};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  delete h;
+  return GWB_OK;
+}
+
+static unsigned blocks_for(size_t n, unsigned bs) { return (unsigned)((n + bs - 1) / bs); }
+
+int gwb_ham_set_kinetic(gwb_ham* h, const double* t, void* stream) {
+  GWB_REQUIRE(h && t, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t n = (size_t)h->nk * h->npw_max;
+  GWB_CUDA_TRY(cudaMemcpyAsync(h->d_t64, t, n * 8, cudaMemcpyDeviceToDevice, st));
+  k_scale_copy<float><<<blocks_for(n, 256), 256, 0, st>>>(t, h->d_t32, n, 1.0);
+  GWB_LAUNCH_CHECK();
+  h->have_t = true;
+  return GWB_OK;
+}
+
+int gwb_ham_set_potential(gwb_ham* h, const double* v, void* stream) {
+  GWB_REQUIRE(h && v, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t n = (size_t)h->g.n[0] * h->g.n[1] * h->g.n[2];
+  const double s = 1.0 / (double)n;
+  k_scale_copy<double><<<blocks_for(n, 256), 256, 0, st>>>(v, h->d_v64, n, s);
+  k_scale_copy<float><<<blocks_for(n, 256), 256, 0, st>>>(v, h->d_v32, n, s);
+  GWB_LAUNCH_CHECK();
+  h->have_v = true;
+  return GWB_OK;
+}
+
+int gwb_ham_set_projectors(gwb_ham* h, const void* p, const double* dij, void* stream) {
+  GWB_REQUIRE(h, "null handle");
+  if (h->nproj == 0) {
+    h->have_p = true;
+    return GWB_OK;
+  }
+  GWB_REQUIRE(p && dij, "null projector pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t np = (size_t)h->nk * h->nproj * h->npw_max;
+  const size_t nd = (size_t)h->nproj * h->nproj;
+  GWB_CUDA_TRY(cudaMemcpyAsync(h->d_p64, p, np * 16, cudaMemcpyDeviceToDevice, st));
+  k_c128_to_c64<<<blocks_for(np, 256), 256, 0, st>>>((const cplx<double>*)p, h->d_p32, np);
+  GWB_CUDA_TRY(cudaMemcpyAsync(h->d_d64, dij, nd * 8, cudaMemcpyDeviceToDevice, st));
+  k_scale_copy<float><<<blocks_for(nd, 256), 256, 0, st>>>(dij, h->d_d32, nd, 1.0);
+  GWB_LAUNCH_CHECK();
+  h->have_p = true;
+  return GWB_OK;
+}
+
+int gwb_ham_apply(gwb_ham* h, const void* c, void* out, int32_t nb, int32_t io_dtype, int32_t prec,
+                  void* stream) {
+  GWB_REQUIRE(h && c && out, "null argument");
+  GWB_REQUIRE(nb >= 0, "nb < 0");
+  GWB_REQUIRE(h->have_t && h->have_v && h->have_p, "kinetic, potential and projectors must be set first");
+  GWB_REQUIRE(io_dtype == GWB_C64 || io_dtype == GWB_C128, "io_dtype must be GWB_C64 or GWB_C128");
+  GWB_REQUIRE(prec == GWB_FP32 || prec == GWB_FP64, "prec must be GWB_FP32 or GWB_FP64");
+  GWB_REQUIRE(c != out, "c and out must not overlap");
+  if (nb == 0) return GWB_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (io_dtype == GWB_C128) {
+    auto* ci = (const cplx<double>*)c;
+    auto* co = (cplx<double>*)out;
+    return prec == GWB_FP64 ? apply_impl<double>(h, ci, co, nb, st) : apply_impl<float>(h, ci, co, nb, st);
+  }
+  auto* ci = (const cplx<float>*)c;
+  auto* co = (cplx<float>*)out;
+  return prec == GWB_FP64 ? apply_impl<double>(h, ci, co, nb, st) : apply_impl<float>(h, ci, co, nb, st);
+}
+
+size_t gwb_ham_scratch_bytes(const gwb_ham* h) {
+  return h ? h->W_bytes + h->part_bytes + h->bd_bytes : 0;
+}
+
+}  // extern "C"

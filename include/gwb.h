@@ -1,0 +1,108 @@
+/*
+ * gwb.h - C ABI of the B200 (sm_100a) Kohn-Sham band-solve library libgwb.so.
+ *
+ * The library replaces the hot path of gradwave's plane-wave band solve: the
+ * batched Hamiltonian apply H psi and the block-Davidson steps around it.
+ * Every entry point:
+ *   - takes plain pointers and sizes (no torch types); array arguments are
+ *     DEVICE pointers unless the comment says host;
+ *   - is stream ordered on the cudaStream_t passed as `void* stream`
+ *     (NULL = legacy default stream) and does not synchronise the host unless
+ *     the comment says so;
+ *   - returns an int status (GWB_OK = 0); gwb_last_error() gives the message
+ *     of the last failure on the calling thread. No C++ exception crosses it.
+ *
+ * Layouts (row-major, the reference's, gradwave core/batch.py:1-14):
+ *   coefficient blocks c       (nk, nb, npw_max) complex, padded slots 0
+ *   kinetic t                  (nk, npw_max) float64, 0 in padding
+ *   flat_idx                   (nk, npw_max) int64 box index
+ *                              i0*n1*n2 + i1*n2 + i2 (gradwave grids.py:171)
+ *   v_eff_r                    (n0, n1, n2) float64 [eV]
+ *   projectors p               (nk, nproj, npw_max) complex128, 0 in padding
+ *   dij                        (nproj, nproj) float64 [eV]
+ * Complex numbers are interleaved (re, im) pairs of float64 (GWB_C128) or
+ * float32 (GWB_C64), i.e. torch.complex128 / torch.complex64 storage.
+ *
+ * Handles are thread-compatible: one handle per host thread at a time.
+ */
+#ifndef GWB_H_
+#define GWB_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define GWB_OK 0
+#define GWB_ERR_ARG 1          /* bad shape, size or pointer */
+#define GWB_ERR_CUDA 2         /* a CUDA runtime or library call failed */
+#define GWB_ERR_NONFINITE 3    /* NaN/Inf found where a finite value is required */
+#define GWB_ERR_TIMEOUT 4      /* a bounded device wait ran out */
+#define GWB_ERR_NOT_CONVERGED 5
+#define GWB_ERR_ALLOC 6        /* device allocation failed */
+#define GWB_ERR_BREAKDOWN 7    /* Cholesky of a non positive-definite Gram matrix */
+
+/* io dtypes */
+#define GWB_C64 0
+#define GWB_C128 1
+/* compute precisions */
+#define GWB_FP32 0
+#define GWB_FP64 1
+
+/* Message of the last failure on this thread ("" if none). */
+const char* gwb_last_error(void);
+/* Library version string. */
+const char* gwb_version(void);
+
+/* ======================================================================= */
+/* Hamiltonian apply                                                       */
+/* ======================================================================= */
+
+typedef struct gwb_ham gwb_ham;
+
+/* Geometry of one k batch (HOST arrays, copied at create). */
+typedef struct {
+  int32_t nk;
+  int32_t npw_max;
+  int32_t n[3];            /* FFT box n0, n1, n2: each 2^a 3^b 5^c 7^d, <= 128 */
+  int32_t nproj;           /* Kleinman-Bylander projector columns (may be 0) */
+  const int64_t* npw;      /* (nk) true plane-wave count per k */
+  const int64_t* flat_idx; /* (nk*npw_max) box index of every sphere point */
+} gwb_ham_geometry;
+
+/* Replaces: gradwave core/batch.py:249-304 (BatchedHamiltonian.__init__: the
+ * persistent scatter box with its trash slot and the cached tables). Builds the
+ * sphere -> box-plane maps and allocates handle-owned scratch on `device`. */
+int gwb_ham_create(const gwb_ham_geometry* geom, int device, gwb_ham** out);
+int gwb_ham_destroy(gwb_ham* h);
+
+/* Kinetic diagonal t (nk*npw_max float64, device). Replaces the t table of
+ * gradwave core/batch.py:306-331 (_tables). */
+int gwb_ham_set_kinetic(gwb_ham* h, const double* t, void* stream);
+/* Local potential v(r) (n0*n1*n2 float64, device). Replaces v_eff of
+ * gradwave core/batch.py:306-331. */
+int gwb_ham_set_potential(gwb_ham* h, const double* v_eff_r, void* stream);
+/* Projectors (complex128, device) and D (float64, device). Replaces p, p_conj
+ * and dij of gradwave core/batch.py:306-331. */
+int gwb_ham_set_projectors(gwb_ham* h, const void* p, const double* dij, void* stream);
+
+/* out = H c over all k and nb bands, padded slots of out set to 0.
+ * Replaces gradwave core/batch.py:480-505 (BatchedHamiltonian.apply).
+ *   io_dtype: storage of c and out (GWB_C64 / GWB_C128)
+ *   prec:     arithmetic of the FFTs, kinetic and nonlocal terms
+ *             (GWB_FP32 / GWB_FP64); GWB_FP64 with GWB_C64 storage is allowed.
+ * c and out must not overlap. */
+int gwb_ham_apply(gwb_ham* h, const void* c, void* out, int32_t nb, int32_t io_dtype,
+                  int32_t prec, void* stream);
+
+/* Bytes of handle-owned device scratch currently held. */
+size_t gwb_ham_scratch_bytes(const gwb_ham* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GWB_H_ */

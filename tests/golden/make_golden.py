@@ -1,0 +1,187 @@
+"""Generate the golden fixtures of the band-solve path from the reference itself.
+
+Runs the reference (gradwave, pure Python + torch, float64) on the seeded cells
+of ``gradwave_b200/data/cells.json`` and writes small ``.npz`` fixtures next to
+this script. The reference cannot travel to the GPU machine, so its outputs do.
+
+The reference's package ``__init__`` pulls in ``ase`` (absent here); the hot-path
+modules are imported through a namespace shim that bypasses it.
+
+What is recorded, per case:
+  * set-up: npw per k and the box index of every sphere point, kinetic and
+    projector fingerprints, all from the reference's own builders
+    (``grids.py:68-184``, ``core/hamiltonian.py:46-105``, ``core/batch.py:174-235``);
+  * apply: ``BatchedHamiltonian.apply`` (``core/batch.py:480-505``) on a seeded
+    random block - in full for small cases, else as projections on seeded
+    random vectors (size-independent checksums);
+  * solve: ``davidson_batched`` (``solvers/davidson.py:528-774``) from the
+    identity start at tol 1e-10 eV: eigenvalues, residual norms, rounds, applies.
+
+Usage: python tests/golden/make_golden.py [small|big|all] [--ref /path/to/gradwave/src]
+"""
+
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+import time
+import types
+from pathlib import Path
+
+import numpy as np
+import torch
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parents[1]))
+
+from gradwave_b200.cells import make_cell  # noqa: E402
+
+TOL = 1e-10
+
+
+def shim(ref_src: str):
+    mod = types.ModuleType("gradwave")
+    mod.__path__ = [os.path.join(ref_src, "gradwave")]
+    sys.modules["gradwave"] = mod
+
+
+def random_block(seed: int, nk: int, nb: int, npw: int) -> np.ndarray:
+    """The seeded test block (every slot random, padding included)."""
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal((nk, nb, npw)) + 1j * rng.standard_normal((nk, nb, npw))
+
+
+def checksums(out: np.ndarray, seed: int, nvec: int = 4) -> np.ndarray:
+    """Projections of ``out`` on seeded random vectors, then |out|^2."""
+    rng = np.random.default_rng(seed + 1000)
+    vals = []
+    for _ in range(nvec):
+        w = rng.standard_normal(out.shape) + 1j * rng.standard_normal(out.shape)
+        vals.append(np.vdot(w, out))
+    vals.append(np.vdot(out, out))
+    return np.array(vals)
+
+
+def reference_setup(ci):
+    """Rebuild the cell's set-up with the reference's own builders."""
+    from gradwave.core.batch import build_batched, projectors_b
+    from gradwave.core.hamiltonian import build_projector_data
+    from gradwave.grids import build_fft_grid, build_gsphere
+
+    grid = build_fft_grid(ci.cell, ci.ecut, shape_override=ci.shape)
+    sph = [build_gsphere(grid, ci.ecut, k) for k in ci.kpoints]
+    from gradwave_b200.cells import _SPEC
+    sp = _SPEC["species"]["Si"]
+    rc = float(sp["rc"])
+    pds = []
+    for s in sph:
+        q = torch.sqrt(s.kpg2)
+        tab = torch.stack([torch.exp(-0.5 * (q * rc) ** 2), q * rc * torch.exp(-0.5 * (q * rc) ** 2)])
+        pds.append(build_projector_data(s, [0] * len(ci.positions), [tab], [[0, 1]],
+                                        [torch.diag(torch.tensor(sp["D"], dtype=torch.float64))],
+                                        grid.volume))
+    bk = build_batched(sph, pds)
+    p = projectors_b(bk, torch.as_tensor(ci.positions))
+    return grid, bk, p
+
+
+def run_case(name: str, seed_cell: int, apply_nb: int, full_apply: bool, solve: bool,
+             fp32_expansion: bool = False) -> dict:
+    from gradwave.core.batch import BatchedHamiltonian
+    from gradwave.solvers.davidson import davidson_batched
+
+    ci = make_cell(name, seed=seed_cell)
+    grid, bk, p = reference_setup(ci)
+    assert grid.shape == ci.shape
+    rec: dict = {"npw": bk.npw.numpy()}
+    # set-up parity: exact integer tables, float fingerprints
+    assert torch.equal(bk.flat_idx, ci.bk.flat_idx), f"{name}: flat_idx differs"
+    assert torch.equal(bk.mask, ci.bk.mask)
+    rec["flat_idx"] = bk.flat_idx.numpy().astype(np.int32)
+    rec["t_sum"] = np.array([float(bk.t.sum()), float((bk.t ** 2).sum())])
+    rec["p_chk"] = checksums(p.numpy(), 7)
+    rec["dij"] = bk.dij_full.numpy()
+    v = ci.v_eff_r
+    h = BatchedHamiltonian(bk, grid.shape, v, p)
+    nk, npw = bk.mask.shape
+    c = torch.from_numpy(random_block(11, nk, apply_nb, npw))
+    t0 = time.perf_counter()
+    out = h.apply(c).numpy()
+    rec["apply_seconds"] = np.array(time.perf_counter() - t0)
+    rec["apply_chk"] = checksums(out, 11)
+    if full_apply:
+        rec["apply_out"] = out
+    if solve:
+        if fp32_expansion:
+            os.environ["GRADWAVE_FP32_EXPANSION"] = "on"
+        try:
+            x0 = ci.identity_start()
+            t0 = time.perf_counter()
+            res = davidson_batched(h.apply, x0, bk.t, bk.mask, tol=TOL, max_iter=200)
+            rec["solve_seconds"] = np.array(time.perf_counter() - t0)
+        finally:
+            os.environ.pop("GRADWAVE_FP32_EXPANSION", None)
+        rec["eigenvalues"] = res.eigenvalues.numpy()
+        rec["residual_norms"] = res.residual_norms.numpy()
+        rec["n_iter"] = np.array(res.n_iter)
+        rec["n_apply"] = np.array([res.n_apply_low, res.n_apply_full])
+        rec["kweights"] = ci.kweights
+    return rec
+
+
+def synthetic_case(seed: int = 2, nk: int = 4, npw: int = 80, nb: int = 8) -> dict:
+    """Dense random Hermitian operator with a kinetic-like diagonal; isolates
+    the eigensolver from the FFT."""
+    from gradwave.solvers.davidson import davidson_batched
+
+    rng = np.random.default_rng(seed)
+    diag = np.linspace(1.0, 100.0, npw)
+    h = np.zeros((nk, npw, npw), dtype=np.complex128)
+    for k in range(nk):
+        a = rng.standard_normal((npw, npw)) + 1j * rng.standard_normal((npw, npw))
+        h[k] = 0.5 * (a + a.conj().T) + np.diag(diag)
+    ht = torch.from_numpy(h)
+    x0 = torch.from_numpy(rng.standard_normal((nk, nb, npw)) + 1j * rng.standard_normal((nk, nb, npw)))
+    mask = torch.ones(nk, npw, dtype=torch.bool)
+    t = torch.from_numpy(np.broadcast_to(diag, (nk, npw)).copy())
+    res = davidson_batched(lambda c: torch.einsum("kij,kbj->kbi", ht.to(c.dtype), c),
+                           x0, t, mask, tol=1e-9, max_iter=100)
+    return {"h": h, "x0": x0.numpy(), "t": t.numpy(), "eigenvalues": res.eigenvalues.numpy(),
+            "residual_norms": res.residual_norms.numpy(), "n_iter": np.array(res.n_iter),
+            "exact": np.linalg.eigvalsh(h)[:, :nb]}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("which", nargs="?", default="small", choices=["small", "big", "all"])
+    ap.add_argument("--ref", default="/root/reference/src")
+    args = ap.parse_args()
+    shim(args.ref)
+    torch.set_num_threads(os.cpu_count() or 1)
+    jobs = []
+    if args.which in ("small", "all"):
+        jobs += [
+            ("si2_fcc", lambda: run_case("si2_fcc", 0, 8, True, True)),
+            ("si8_cubic", lambda: run_case("si8_cubic", 0, 2, False, True)),
+            ("si8_cubic_fp32exp", lambda: run_case("si8_cubic", 0, 1, False, True, fp32_expansion=True)),
+            ("si8_perturbed", lambda: run_case("si8_perturbed", 1, 2, False, False)),
+            ("synthetic", synthetic_case),
+        ]
+    if args.which in ("big", "all"):
+        jobs += [
+            ("si64_cubic", lambda: run_case("si64_cubic", 0, 2, False, True)),
+            ("si216_vacancy", lambda: run_case("si216_vacancy", 0, 1, False, True)),
+        ]
+    for tag, fn in jobs:
+        t0 = time.perf_counter()
+        rec = fn()
+        np.savez_compressed(HERE / f"{tag}.npz", **rec)
+        extra = ""
+        if "n_iter" in rec:
+            extra = f" n_iter={int(rec['n_iter'])} max_res={float(np.max(rec['residual_norms'])):.2e}"
+        print(f"{tag}: {time.perf_counter() - t0:.1f}s{extra}", flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,84 @@
+"""The float64 CPU oracle against the reference's own outputs (golden fixtures).
+
+The fixtures were produced by running the reference (gradwave) on the same
+seeded cells: ``tests/golden/make_golden.py``. These tests pin the oracle
+before it is trusted as the checker of the CUDA path.
+"""
+
+import numpy as np
+import pytest
+
+from tests.conftest import load_golden
+from tests.golden.make_golden import checksums, random_block
+
+
+def test_setup_tables_match_reference():
+    from gradwave_b200.cells import make_cell
+    for name, seed in (("si2_fcc", 0), ("si8_cubic", 0), ("si8_perturbed", 1)):
+        g = load_golden(name)
+        ci = make_cell(name, seed=seed)
+        assert np.array_equal(ci.bk.npw.numpy(), g["npw"])
+        assert np.array_equal(ci.bk.flat_idx.numpy().astype(np.int32), g["flat_idx"])
+        t = ci.bk.t.numpy()
+        assert np.allclose([t.sum(), (t ** 2).sum()], g["t_sum"], rtol=1e-14, atol=0)
+        pchk = checksums(ci.p.numpy(), 7)
+        assert np.abs(pchk - g["p_chk"]).max() <= 1e-12 * np.abs(g["p_chk"]).max()
+        assert np.array_equal(ci.bk.dij_full.numpy(), g["dij"])
+
+
+def test_oracle_apply_si2_full():
+    from gradwave_b200.cells import make_cell
+    from oracle.ham import from_cell
+    g = load_golden("si2_fcc")
+    ci = make_cell("si2_fcc")
+    out = from_cell(ci).apply(random_block(11, 1, 8, ci.bk.npw_max))
+    assert np.abs(out - g["apply_out"]).max() <= 1e-12 * np.abs(g["apply_out"]).max()
+
+
+@pytest.mark.parametrize("name,seed", [("si8_cubic", 0), ("si8_perturbed", 1)])
+def test_oracle_apply_checksums(name, seed):
+    from gradwave_b200.cells import make_cell
+    from oracle.ham import from_cell
+    g = load_golden(name)
+    ci = make_cell(name, seed=seed)
+    out = from_cell(ci).apply(random_block(11, ci.bk.nk, 2, ci.bk.npw_max))
+    chk = checksums(out, 11)
+    assert np.abs(chk - g["apply_chk"]).max() <= 1e-12 * np.abs(g["apply_chk"]).max()
+
+
+def test_oracle_davidson_synthetic():
+    from oracle.davidson import davidson_batched
+    g = load_golden("synthetic")
+    h = g["h"]
+    res = davidson_batched(lambda c: np.einsum("kij,kbj->kbi", h, c), g["x0"], g["t"],
+                           np.ones(g["t"].shape, bool), tol=1e-9, max_iter=100)
+    assert res.residual_norms.max() < 1e-9
+    assert np.abs(res.eigenvalues - g["eigenvalues"]).max() < 1e-10
+    assert np.abs(res.eigenvalues - g["exact"]).max() < 1e-9
+    assert abs(res.n_iter - int(g["n_iter"])) <= 2
+
+
+def test_oracle_davidson_si2():
+    from gradwave_b200.cells import make_cell
+    from oracle.davidson import davidson_batched
+    from oracle.ham import from_cell
+    g = load_golden("si2_fcc")
+    ci = make_cell("si2_fcc")
+    h = from_cell(ci)
+    res = davidson_batched(h.apply, ci.identity_start().numpy(), ci.bk.t.numpy(), ci.bk.mask.numpy(),
+                           tol=1e-10, max_iter=200)
+    assert res.residual_norms.max() < 1e-10
+    assert np.abs(res.eigenvalues - g["eigenvalues"]).max() < 1e-10
+    assert abs(res.n_iter - int(g["n_iter"])) <= 2
+
+
+@pytest.mark.slow
+def test_oracle_davidson_si8():
+    from gradwave_b200.cells import make_cell
+    from oracle.davidson import davidson_batched
+    from oracle.ham import from_cell
+    g = load_golden("si8_cubic")
+    ci = make_cell("si8_cubic")
+    res = davidson_batched(from_cell(ci).apply, ci.identity_start().numpy(), ci.bk.t.numpy(),
+                           ci.bk.mask.numpy(), tol=1e-10, max_iter=200)
+    assert np.abs(res.eigenvalues - g["eigenvalues"]).max() < 1e-9
