@@ -1,0 +1,411 @@
+"""Benchmark: ms per converged band solve on one B200 (eigenvalues within
+1e-8 Ha of the float64 reference).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config NAME] [--impl ours|reference]
+
+A step is one converged band solve of the workload (default ``si8_cubic``: the
+8-atom cubic Si cell, 40 Ry, 10 irreducible k, 24 bands, 36^3 box) from the
+identity start. Our arm reports:
+
+* ``value``       device-timed ms per solve with the inputs resident in HBM
+                  (CUDA events on the launching stream, max over ranks); the
+                  solver is the product's fast mode (float32 expansion applies
+                  with float64 certification, then float64 polish);
+* ``e2e``         the same solve through the public API from pinned host
+                  memory: H2D of the start block, solve, D2H of eigenvalues and
+                  eigenvectors, all inside the timed region;
+* ``plain_fp64``  the plain float64 TPA Davidson on the same GPU and kernels;
+* ``roofline``    for the dominant kernel (the Hamiltonian apply), measured
+                  live with CUDA events around its launches;
+* ``cpu_baseline`` the float64 oracle (numpy restatement of the reference)
+                  on the host cores, on a bounded sample of the same workload.
+
+Between timed steps a 256 MiB buffer is written to flush L2 (126 MB).
+Eigenvalue error is checked against the reference's own eigenvalues
+(``tests/golden``) and reported; a solve outside 1e-8 Ha fails the run.
+
+With N > 1 (torchrun) every rank solves its own replica (weak scaling, no
+data-path collective) and ``value`` is the whole-job time per solve: the max
+over ranks of the step time divided by N.
+
+``--impl reference`` times the reference's CPU path (the float64 oracle port;
+the reference itself is Python and does not travel) with all host threads on
+a bounded k-point sample, scaled to the full workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+HA = 27.211386245988
+EIG_TOL_EV = 1e-8 * HA
+METRIC = "ms per converged band solve (eig err ≤1e-8 Ha): learned+mixed vs plain, 1 B200"
+GOLDEN = {"si2_fcc": "si2_fcc", "si8_cubic": "si8_cubic", "si64_cubic": "si64_cubic",
+          "si216_vacancy": "si216_vacancy"}
+
+
+def _golden(name):
+    p = ROOT / "tests" / "golden" / f"{GOLDEN.get(name, name)}.npz"
+    if not p.exists():
+        return None
+    with np.load(p) as z:
+        return {k: z[k] for k in z.files}
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _max_over_ranks(x: float, ws: int, dev) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference(args):
+    """The reference's CPU path (float64 oracle port) on a bounded k sample."""
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    import torch
+    from gradwave_b200.cells import make_cell
+    from oracle.davidson import davidson_batched
+    from oracle.ham import OracleHamiltonian
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("GWB_ORACLE_THREADS", str(threads))
+    torch.set_num_threads(threads)
+    ci = make_cell(args.config)
+    nk = ci.bk.nk
+    ks = list(range(nk)) if nk <= 2 else [0, nk // 2]
+    bk = ci.bk
+    h = OracleHamiltonian(bk.mask.numpy()[ks], bk.flat_idx.numpy()[ks], bk.t.numpy()[ks], ci.shape,
+                          ci.v_eff_r.numpy(), ci.p.numpy()[ks], bk.dij_full.numpy())
+    x0 = ci.identity_start().numpy()[ks]
+
+    def step():
+        t0 = time.perf_counter()
+        r = davidson_batched(h.apply, x0, bk.t.numpy()[ks], bk.mask.numpy()[ks], tol=args.tol, max_iter=300)
+        return (time.perf_counter() - t0) * 1e3 * nk / len(ks), r
+
+    for _ in range(args.warmup):
+        step()
+    times = []
+    for _ in range(args.steps):
+        ms, r = step()
+        times.append(ms)
+    v = statistics.mean(times)
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "ms", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128/f64", "data": "synthetic (seeded Si cells)",
+            "config": {"workload": args.config, "nk": nk, "nbands": ci.nbands, "fft": list(ci.shape),
+                       "tol_ev": args.tol, "l2": "n/a (CPU)"},
+            "cpu_baseline": {"value": round(v, 3), "unit": "ms", "cores": threads, "kind": "port",
+                             "sample": f"k-points {ks} of {nk} solved to tol {args.tol} eV, time scaled "
+                                       f"by {nk}/{len(ks)}; float64 numpy/scipy restatement of the "
+                                       "reference's davidson_batched + BatchedHamiltonian.apply"},
+            "e2e": {"value": round(v, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "n_iter": int(r.n_iter)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+class ApplyTimer:
+    """Wraps a BatchedHamiltonian's apply_into with CUDA events to time every
+    launch of the dominant kernel inside the timed region."""
+
+    def __init__(self, h):
+        import torch
+        self.h = h
+        self.torch = torch
+        self.orig = h.apply_into
+        self.events = []
+        self.rows = 0
+        self.on = False
+
+    def __enter__(self):
+        def timed(*a, **kw):
+            if not self.on:
+                return self.orig(*a, **kw)
+            e0 = self.torch.cuda.Event(enable_timing=True)
+            e1 = self.torch.cuda.Event(enable_timing=True)
+            e0.record()
+            self.orig(*a, **kw)
+            e1.record()
+            self.events.append((e0, e1, a[4], a[5]))
+        self.h.apply_into = timed
+        return self
+
+    def __exit__(self, *a):
+        self.h.apply_into = self.orig
+
+    def collect(self):
+        out = [(e0.elapsed_time(e1), nrows, prec) for e0, e1, nrows, prec in self.events]
+        self.events = []
+        return out
+
+
+def run_ours(args):
+    import torch
+    from gradwave_b200 import _lib
+    from gradwave_b200.cells import make_cell
+    from gradwave_b200.davidson import davidson_batched
+    from gradwave_b200.hamiltonian import BatchedHamiltonian
+
+    ws, rank, local = _dist()
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    torch.cuda.set_device(dev)
+    ci = make_cell(args.config)
+    bk = ci.bk.to(dev)
+    h = BatchedHamiltonian(bk, ci.shape, ci.v_eff_r, ci.p)
+    gold = _golden(args.config)
+    x0_host = ci.identity_start().pin_memory()
+    x0_dev = x0_host.to(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def solve(x0, mode):
+        return davidson_batched(h.apply, x0, bk.t, bk.mask, tol=args.tol, max_iter=300, mode=mode)
+
+    def check(res):
+        if gold is None:
+            return None
+        err = float(np.abs(res.eigenvalues.cpu().numpy() - gold["eigenvalues"]).max())
+        if err > EIG_TOL_EV:
+            raise SystemExit(f"eigenvalue error {err:.3e} eV exceeds 1e-8 Ha")
+        return err
+
+    def timed(fn, steps, warmup, clocks=None):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        ts = []
+        out = None
+        for _ in range(steps):
+            flush.zero_()
+            if ws > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize(dev)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            out = fn()
+            e1.record()
+            torch.cuda.synchronize(dev)
+            ts.append(e0.elapsed_time(e1))
+        return statistics.mean(ts), out
+
+    mode_fast = "fp32exp"
+    # value: device-resident inputs
+    n0 = _lib.launch_count()
+    with ClockSampler(dev.index) as clk:
+        with ApplyTimer(h) as at:
+            for _ in range(args.warmup):
+                solve(x0_dev, mode_fast)
+            at.on = True
+            ms_fast, res_fast = timed(lambda: solve(x0_dev, mode_fast), args.steps, 0)
+            at.on = False
+            apply_launches = at.collect()
+    launches = (_lib.launch_count() - n0) * args.steps // (args.steps + args.warmup)
+    err_fast = check(res_fast)
+    # plain float64 TPA Davidson on the same GPU
+    ms_plain, res_plain = timed(lambda: solve(x0_dev, "fp64"), max(1, args.steps // 2), 1)
+    err_plain = check(res_plain)
+
+    # e2e through the public API from pinned host memory
+    def e2e():
+        x0 = x0_host.to(dev, non_blocking=True)
+        r = solve(x0, mode_fast)
+        ev = r.eigenvalues.to("cpu", non_blocking=True)
+        vec = r.eigenvectors.to("cpu", non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+        return ev, vec
+    ms_e2e, (ev, vec) = timed(e2e, args.steps, 1)
+
+    ms_fast = _max_over_ranks(ms_fast, ws, dev)
+    ms_e2e = _max_over_ranks(ms_e2e, ws, dev)
+    ms_plain = _max_over_ranks(ms_plain, ws, dev)
+
+    # roofline of the dominant kernel: the batched Hamiltonian apply
+    hbm_peak, peak_kind = _peaks()
+    per_rows = {}
+    for ms, nrows, prec in apply_launches:
+        per_rows.setdefault(prec, []).append((ms, nrows))
+    tot_ms = sum(ms for ms, _, _ in apply_launches)
+    tot_rows = sum(n for _, n, _ in apply_launches)
+    nk = ci.bk.nk
+    npw = ci.bk.npw.numpy().astype(np.float64)
+    n_box = float(np.prod(ci.shape))
+    nproj = int(ci.p.shape[1])
+    # algorithmic bytes per band (c128 storage): c in + H c out (16+16 B per plane
+    # wave) + the dense box through HBM once per 3D FFT at fp32 (2 x 16 B per
+    # point); per launch + v(r) (4 B per point) + projectors read twice (fp32)
+    mean_npw = float(npw.mean())
+    bytes_per_band = 32.0 * mean_npw + 32.0 * n_box
+    alg_bytes = tot_rows * nk * bytes_per_band + len(apply_launches) * (4.0 * n_box + 2 * 8.0 * nk * nproj * mean_npw)
+    achieved = alg_bytes / (tot_ms * 1e-3) / 1e9 if tot_ms > 0 else 0.0
+    roof = {"kernel": "gwb_ham_apply (K1 plane_inverse + K2 pencil_vloc + K3 plane_forward + nonlocal)",
+            "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+            "frac": round(achieved / hbm_peak, 4), "peak_kind": peak_kind, "traffic": None,
+            "launches": len(apply_launches), "avg_launch_ms": round(tot_ms / max(1, len(apply_launches)), 4),
+            "share_of_step": round(tot_ms / max(1e-9, ms_fast * args.steps), 4),
+            "bytes_per_band": bytes_per_band}
+    traffic_file = ROOT / "profiles" / f"traffic_{args.config}.json"
+    if traffic_file.exists():
+        roof["traffic"] = json.loads(traffic_file.read_text()).get("bytes_per_launch")
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = _cpu_baseline(args, ci)
+    if ws > 1:
+        torch.distributed.barrier()
+    if rank == 0:
+        n_vec = vec.numel() * vec.element_size()
+        line = {"metric": METRIC, "value": round(ms_fast / ws, 3), "unit": "ms", "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_fast, 3),
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "c128 (fp32 expansion, fp64 certify)",
+                "data": "synthetic (seeded Si cells, analytic pseudopotential)",
+                "config": {"workload": args.config, "nk": nk, "nbands": ci.nbands, "fft": list(ci.shape),
+                           "npw": [int(n) for n in ci.bk.npw], "tol_ev": args.tol,
+                           "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"replicas{ws}"},
+                "eig_err_ev": err_fast, "eig_err_ha": None if err_fast is None else err_fast / HA,
+                "n_iter": res_fast.n_iter, "n_apply_low": res_fast.n_apply_low,
+                "n_apply_full": res_fast.n_apply_full,
+                "plain_fp64": {"value": round(ms_plain, 3), "unit": "ms", "n_iter": res_plain.n_iter,
+                               "eig_err_ev": err_plain},
+                "e2e": {"value": round(ms_e2e / ws, 3), "unit": "ms", "h2d_bytes_per_step": int(x0_host.numel() * 16),
+                        "d2h_bytes_per_step": int(ev.numel() * 8 + n_vec)},
+                "gpu_launches": int(launches), "roofline": roof, "clocks": clk.summary(),
+                "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def _cpu_baseline(args, ci):
+    """Oracle (float64 numpy) on a bounded sample: two k-points of the workload."""
+    import torch
+    from oracle.davidson import davidson_batched
+    from oracle.ham import OracleHamiltonian
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("GWB_ORACLE_THREADS", str(threads))
+    torch.set_num_threads(threads)
+    bk = ci.bk
+    nk = bk.nk
+    ks = list(range(nk)) if nk <= 2 else [0, nk // 2]
+    h = OracleHamiltonian(bk.mask.numpy()[ks], bk.flat_idx.numpy()[ks], bk.t.numpy()[ks], ci.shape,
+                          ci.v_eff_r.numpy(), ci.p.numpy()[ks], bk.dij_full.numpy())
+    t0 = time.perf_counter()
+    davidson_batched(h.apply, ci.identity_start().numpy()[ks], bk.t.numpy()[ks], bk.mask.numpy()[ks],
+                     tol=args.tol, max_iter=300)
+    dt = (time.perf_counter() - t0) * 1e3 * nk / len(ks)
+    return {"value": round(dt, 1), "unit": "ms", "cores": threads, "kind": "port",
+            "sample": f"k-points {ks} of {nk} solved to tol {args.tol} eV with the float64 oracle, "
+                      f"time scaled by {nk}/{len(ks)}"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", default="si8_cubic")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -57,15 +57,26 @@ _D = ctypes.c_double
 _SIGNATURES = {
     "gwb_last_error": [],
     "gwb_version": [],
+    "gwb_launch_count": [],
     "gwb_ham_create": [ctypes.POINTER(Geometry), ctypes.c_int, ctypes.POINTER(_P)],
     "gwb_ham_destroy": [_P],
     "gwb_ham_set_kinetic": [_P, _P, _P],
     "gwb_ham_set_potential": [_P, _P, _P],
     "gwb_ham_set_projectors": [_P, _P, _P, _P],
     "gwb_ham_apply": [_P, _P, _P, _I, _I, _I, _P],
+    "gwb_ham_apply_strided": [_P, _P, _I64, _P, _I64, _I, _I, _I, _P],
     "gwb_ham_scratch_bytes": [_P],
+    "gwb_zgemm": [ctypes.c_int, ctypes.c_int, _I64, _I64, _I64, _D, _D, _P, _I64, _I64, _P, _I64, _I64,
+                  _D, _D, _P, _I64, _I64, _I64, _P],
+    "gwb_residual": [_I, _I, _I, _P, _I64, _P, _I64, _P, _I64, _P, _I64, _P, _P],
+    "gwb_conv_stats": [_I, _I, _P, _D, _P, _P],
+    "gwb_select_worst": [_I, _I, _P, _I, _P, _P],
+    "gwb_precond_teter": [_I, _I, _I, _I, _P, _I64, _P, _I64, _P, _P, _P, _I64, _P],
+    "gwb_subspace_insert": [_I, _I, _I, _P, _P, _I, _I64, _P],
+    "gwb_chol_inv": [_I, _I, _P, _I, _I64, _P, _I64, _P, _P],
 }
 _RESTYPES = {"gwb_last_error": ctypes.c_char_p, "gwb_version": ctypes.c_char_p,
+             "gwb_launch_count": ctypes.c_ulonglong,
              "gwb_ham_scratch_bytes": ctypes.c_size_t}
 
 
@@ -90,6 +101,11 @@ def load() -> ctypes.CDLL:
                 fn.restype = _RESTYPES.get(name, ctypes.c_int)
             _lib = lib
     return _lib
+
+
+def launch_count() -> int:
+    """Kernels launched by libgwb.so in this process (cuBLAS/torch not included)."""
+    return int(load().gwb_launch_count())
 
 
 def check(status: int) -> None:

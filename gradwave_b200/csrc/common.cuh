@@ -77,6 +77,8 @@ template <typename S, typename T> __device__ __forceinline__ void st(S* p, size_
 }
 
 void set_error(const std::string& msg);
+// Tally of kernels this library launched (gwb_launch_count).
+void count_launches(int n);
 
 }  // namespace gwb
 

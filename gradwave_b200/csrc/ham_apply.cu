@@ -29,6 +29,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -40,6 +41,8 @@ namespace gwb {
 
 static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
+static std::atomic<unsigned long long> g_launches{0};
+void count_launches(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
 
 struct FftGeom {
   int n[3];
@@ -121,7 +124,7 @@ __global__ void __launch_bounds__(256, (C1 && C2) ? 3 : 1) k_plane_inverse(FftGe
                                                        const int* __restrict__ plane_pos,
                                                        const SIO* __restrict__ c, cplx<T>* __restrict__ W,
                                                        const cplx<T>* __restrict__ tw1,
-                                                       const cplx<T>* __restrict__ tw2, int nb, int b0,
+                                                       const cplx<T>* __restrict__ tw2, int64_t ck, int b0,
                                                        int nbc, int npw_max) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int n1 = g.n[1], n2 = g.n[2], L0 = g.L[0];
@@ -133,7 +136,7 @@ __global__ void __launch_bounds__(256, (C1 && C2) ? 3 : 1) k_plane_inverse(FftGe
   for (int i = threadIdx.x; i < n2; i += blockDim.x) t2[i] = tw2[i];
   for (int i = threadIdx.x; i < n1 * n2; i += blockDim.x) S[i] = mk<T>(0, 0);
   __syncthreads();
-  const size_t crow = ((size_t)k * nb + (b0 + bl)) * npw_max;
+  const size_t crow = (size_t)k * ck + (size_t)(b0 + bl) * npw_max;
   const int e0 = plane_ptr[k * L0 + j0], e1 = plane_ptr[k * L0 + j0 + 1];
   for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) S[plane_pos[e]] = ld<T>(c, crow + plane_g[e]);
   __syncthreads();
@@ -185,7 +188,7 @@ __global__ void __launch_bounds__(256, (C1 && C2) ? 3 : 1) k_plane_forward(
     FftGeom g, const int* __restrict__ plane_ptr, const int* __restrict__ plane_g,
     const int* __restrict__ plane_pos, const int* __restrict__ npw, const SIO* __restrict__ c,
     SIO* __restrict__ out, const cplx<T>* __restrict__ W, const T* __restrict__ t,
-    const cplx<T>* __restrict__ tw1, const cplx<T>* __restrict__ tw2, int nb, int b0, int nbc,
+    const cplx<T>* __restrict__ tw1, const cplx<T>* __restrict__ tw2, int64_t ck, int64_t ok, int b0, int nbc,
     int npw_max) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int n1 = g.n[1], n2 = g.n[2], L0 = g.L[0];
@@ -200,16 +203,17 @@ __global__ void __launch_bounds__(256, (C1 && C2) ? 3 : 1) k_plane_forward(
   __syncthreads();
   fft_any<T, true, -1, C1>(S, n2, g.plan[1], 1, n2, n2, n2, t1);
   fft_any<T, false, -1, C2>(S, g.L[1], g.plan[2], n2, 1, g.M[1], n1, t2);
-  const size_t crow = ((size_t)k * nb + (b0 + bl)) * npw_max;
+  const size_t crow = (size_t)k * ck + (size_t)(b0 + bl) * npw_max;
+  const size_t orow = (size_t)k * ok + (size_t)(b0 + bl) * npw_max;
   const int e0 = plane_ptr[k * L0 + j0], e1 = plane_ptr[k * L0 + j0 + 1];
   const T* tk = t + (size_t)k * npw_max;
   for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
     const int gi = plane_g[e];
     cplx<T> cv = ld<T>(c, crow + gi);
-    st(out, crow + gi, S[plane_pos[e]] + scale(cv, tk[gi]));
+    st(out, orow + gi, S[plane_pos[e]] + scale(cv, tk[gi]));
   }
   if (j0 == 0) {
-    for (int gi = npw[k] + threadIdx.x; gi < npw_max; gi += blockDim.x) st(out, crow + gi, mk<T>(0, 0));
+    for (int gi = npw[k] + threadIdx.x; gi < npw_max; gi += blockDim.x) st(out, orow + gi, mk<T>(0, 0));
   }
 }
 
@@ -222,7 +226,7 @@ template <typename T, typename SIO>
 __global__ void __launch_bounds__(256) k_becp_partial(const SIO* __restrict__ c,
                                                       const cplx<T>* __restrict__ P,
                                                       cplx<T>* __restrict__ part, int nk, int nb,
-                                                      int nproj, int npw_max, int gslice) {
+                                                      int nproj, int npw_max, int gslice, int64_t ck) {
   __shared__ cplx<T> sc[NL_TB][NL_TG + 1];
   __shared__ cplx<T> sp[NL_TP][NL_TG + 1];
   const int pt = blockIdx.x, bt = blockIdx.y;
@@ -235,7 +239,7 @@ __global__ void __launch_bounds__(256) k_becp_partial(const SIO* __restrict__ c,
     for (int i = tid; i < NL_TB * NL_TG; i += blockDim.x) {
       const int bb = i / NL_TG, gg = i % NL_TG;
       const int b = bt * NL_TB + bb, gi = gb + gg;
-      sc[bb][gg] = (b < nb && gi < g_end) ? ld<T>(c, ((size_t)k * nb + b) * npw_max + gi) : mk<T>(0, 0);
+      sc[bb][gg] = (b < nb && gi < g_end) ? ld<T>(c, (size_t)k * ck + (size_t)b * npw_max + gi) : mk<T>(0, 0);
     }
     for (int i = tid; i < NL_TP * NL_TG; i += blockDim.x) {
       const int pp = i / NL_TG, gg = i % NL_TG;
@@ -286,7 +290,7 @@ template <typename T, typename SIO>
 __global__ void __launch_bounds__(256) k_nl_add(const cplx<T>* __restrict__ bd,
                                                 const cplx<T>* __restrict__ P,
                                                 SIO* __restrict__ out, int nk, int nb, int nproj,
-                                                int npw_max) {
+                                                int npw_max, int64_t ok) {
   constexpr int TGO = 64, TQ = 16;
   __shared__ cplx<T> sb[NL_TB][TQ];
   __shared__ cplx<T> sp[TQ][TGO];
@@ -322,7 +326,7 @@ __global__ void __launch_bounds__(256) k_nl_add(const cplx<T>* __restrict__ bd,
     for (int i = 0; i < 4; ++i) {
       const int b = bt * NL_TB + lb0 * 4 + i;
       if (b < nb) {
-        const size_t o = ((size_t)k * nb + b) * npw_max + gi;
+        const size_t o = (size_t)k * ok + (size_t)b * npw_max + gi;
         st(out, o, ld<T>(out, o) + acc[i]);
       }
     }
@@ -371,8 +375,8 @@ static int nl_slices(const gwb_ham* h) {
 constexpr unsigned kCode24 = 0x38u, kCode36 = 0x334u, kCode72 = 0x338u, kCode96 = 0x348u;
 
 template <typename T, typename SIO, unsigned C>
-static int local_chunks(gwb_ham* h, const SIO* c, SIO* out, int nb, int nbc, cudaStream_t st, size_t smA,
-                        size_t smB) {
+static int local_chunks(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t ok, int nb, int nbc,
+                        cudaStream_t st, size_t smA, size_t smB) {
   const FftGeom& g = h->g;
   const bool dbl = sizeof(T) == 8;
   const cplx<T>* tw0 = dbl ? (const cplx<T>*)h->d_tw64[0] : (const cplx<T>*)h->d_tw32[0];
@@ -388,18 +392,19 @@ static int local_chunks(gwb_ham* h, const SIO* c, SIO* out, int nb, int nbc, cud
     const int cb = std::min(nbc, nb - b0);
     dim3 gA(g.L[0], cb, h->nk), gB(g.n[1], cb, h->nk);
     k_plane_inverse<T, SIO, C, C><<<gA, 256, smA, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos, c, W,
-                                                       tw1, tw2, nb, b0, cb, h->npw_max);
+                                                       tw1, tw2, ck, b0, cb, h->npw_max);
     k_pencil_vloc<T, C><<<gB, 256, smB, st>>>(g, W, v, tw0, cb);
     k_plane_forward<T, SIO, C, C><<<gA, 256, smA, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos,
-                                                       h->d_npw, c, out, W, t, tw1, tw2, nb, b0, cb,
+                                                       h->d_npw, c, out, W, t, tw1, tw2, ck, ok, b0, cb,
                                                        h->npw_max);
     GWB_LAUNCH_CHECK();
+    count_launches(3);
   }
   return GWB_OK;
 }
 
 template <typename T, typename SIO>
-static int apply_impl(gwb_ham* h, const SIO* c, SIO* out, int nb, cudaStream_t st) {
+static int apply_impl(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t ok, int nb, cudaStream_t st) {
   const FftGeom& g = h->g;
   const size_t es = sizeof(cplx<T>);
   const size_t plane_elems = (size_t)g.n[1] * g.n[2];
@@ -414,11 +419,11 @@ static int apply_impl(gwb_ham* h, const SIO* c, SIO* out, int nb, cudaStream_t s
   const unsigned c0 = g.plan[0].code, c1 = g.plan[1].code, c2 = g.plan[2].code;
   const bool cubic = c0 == c1 && c1 == c2;
   int rcl;
-  if (cubic && c0 == kCode24) rcl = local_chunks<T, SIO, kCode24>(h, c, out, nb, nbc, st, smA, smB);
-  else if (cubic && c0 == kCode36) rcl = local_chunks<T, SIO, kCode36>(h, c, out, nb, nbc, st, smA, smB);
-  else if (cubic && c0 == kCode72) rcl = local_chunks<T, SIO, kCode72>(h, c, out, nb, nbc, st, smA, smB);
-  else if (cubic && c0 == kCode96) rcl = local_chunks<T, SIO, kCode96>(h, c, out, nb, nbc, st, smA, smB);
-  else rcl = local_chunks<T, SIO, 0u>(h, c, out, nb, nbc, st, smA, smB);
+  if (cubic && c0 == kCode24) rcl = local_chunks<T, SIO, kCode24>(h, c, ck, out, ok, nb, nbc, st, smA, smB);
+  else if (cubic && c0 == kCode36) rcl = local_chunks<T, SIO, kCode36>(h, c, ck, out, ok, nb, nbc, st, smA, smB);
+  else if (cubic && c0 == kCode72) rcl = local_chunks<T, SIO, kCode72>(h, c, ck, out, ok, nb, nbc, st, smA, smB);
+  else if (cubic && c0 == kCode96) rcl = local_chunks<T, SIO, kCode96>(h, c, ck, out, ok, nb, nbc, st, smA, smB);
+  else rcl = local_chunks<T, SIO, 0u>(h, c, ck, out, ok, nb, nbc, st, smA, smB);
   if (rcl) return rcl;
   if (h->nproj > 0) {
     const int ns = nl_slices(h);
@@ -431,12 +436,13 @@ static int apply_impl(gwb_ham* h, const SIO* c, SIO* out, int nb, cudaStream_t s
     const cplx<T>* P = dbl ? (const cplx<T>*)h->d_p64 : (const cplx<T>*)h->d_p32;
     const T* D = dbl ? (const T*)h->d_d64 : (const T*)h->d_d32;
     dim3 g4((h->nproj + NL_TP - 1) / NL_TP, (nb + NL_TB - 1) / NL_TB, h->nk * nsl);
-    k_becp_partial<T, SIO><<<g4, 256, 0, st>>>(c, P, (cplx<T>*)h->d_part, h->nk, nb, h->nproj, h->npw_max, gslice);
+    k_becp_partial<T, SIO><<<g4, 256, 0, st>>>(c, P, (cplx<T>*)h->d_part, h->nk, nb, h->nproj, h->npw_max, gslice, ck);
     k_becp_reduce_d<T><<<h->nk * nb, 128, h->nproj * es, st>>>((const cplx<T>*)h->d_part, D, (cplx<T>*)h->d_bd,
                                                             h->nk, nb, h->nproj, nsl);
     dim3 g6((h->npw_max + 63) / 64, (nb + NL_TB - 1) / NL_TB, h->nk);
-    k_nl_add<T, SIO><<<g6, 256, 0, st>>>((const cplx<T>*)h->d_bd, P, out, h->nk, nb, h->nproj, h->npw_max);
+    k_nl_add<T, SIO><<<g6, 256, 0, st>>>((const cplx<T>*)h->d_bd, P, out, h->nk, nb, h->nproj, h->npw_max, ok);
     GWB_LAUNCH_CHECK();
+    count_launches(3);
   }
   return GWB_OK;
 }
@@ -449,6 +455,7 @@ extern "C" {
 
 const char* gwb_last_error(void) { return g_last_error.c_str(); }
 const char* gwb_version(void) { return "gwb 0.1 sm_100a"; }
+unsigned long long gwb_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 int gwb_ham_create(const gwb_ham_geometry* geom, int device, gwb_ham** out) {
   GWB_REQUIRE(geom && out, "null argument");
@@ -628,24 +635,40 @@ int gwb_ham_set_projectors(gwb_ham* h, const void* p, const double* dij, void* s
   return GWB_OK;
 }
 
-int gwb_ham_apply(gwb_ham* h, const void* c, void* out, int32_t nb, int32_t io_dtype, int32_t prec,
-                  void* stream) {
+int gwb_ham_apply_strided(gwb_ham* h, const void* c, int64_t c_kstride, void* out, int64_t out_kstride,
+                          int32_t nb, int32_t io_dtype, int32_t prec, void* stream) {
   GWB_REQUIRE(h && c && out, "null argument");
   GWB_REQUIRE(nb >= 0, "nb < 0");
   GWB_REQUIRE(h->have_t && h->have_v && h->have_p, "kinetic, potential and projectors must be set first");
   GWB_REQUIRE(io_dtype == GWB_C64 || io_dtype == GWB_C128, "io_dtype must be GWB_C64 or GWB_C128");
   GWB_REQUIRE(prec == GWB_FP32 || prec == GWB_FP64, "prec must be GWB_FP32 or GWB_FP64");
   GWB_REQUIRE(c != out, "c and out must not overlap");
+  GWB_REQUIRE(c_kstride >= (int64_t)nb * h->npw_max && out_kstride >= (int64_t)nb * h->npw_max,
+              "k stride smaller than nb * npw_max");
   if (nb == 0) return GWB_OK;
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) {
+    set_error(cudaGetErrorString(e));
+    return GWB_ERR_CUDA;
+  }
   cudaStream_t st = (cudaStream_t)stream;
   if (io_dtype == GWB_C128) {
     auto* ci = (const cplx<double>*)c;
     auto* co = (cplx<double>*)out;
-    return prec == GWB_FP64 ? apply_impl<double>(h, ci, co, nb, st) : apply_impl<float>(h, ci, co, nb, st);
+    return prec == GWB_FP64 ? apply_impl<double>(h, ci, c_kstride, co, out_kstride, nb, st)
+                            : apply_impl<float>(h, ci, c_kstride, co, out_kstride, nb, st);
   }
   auto* ci = (const cplx<float>*)c;
   auto* co = (cplx<float>*)out;
-  return prec == GWB_FP64 ? apply_impl<double>(h, ci, co, nb, st) : apply_impl<float>(h, ci, co, nb, st);
+  return prec == GWB_FP64 ? apply_impl<double>(h, ci, c_kstride, co, out_kstride, nb, st)
+                          : apply_impl<float>(h, ci, c_kstride, co, out_kstride, nb, st);
+}
+
+int gwb_ham_apply(gwb_ham* h, const void* c, void* out, int32_t nb, int32_t io_dtype, int32_t prec,
+                  void* stream) {
+  GWB_REQUIRE(h, "null handle");
+  const int64_t ks = (int64_t)nb * h->npw_max;
+  return gwb_ham_apply_strided(h, c, ks, out, ks, nb, io_dtype, prec, stream);
 }
 
 size_t gwb_ham_scratch_bytes(const gwb_ham* h) {

@@ -1,0 +1,348 @@
+"""Batched block Davidson on the B200 path (drop-in for gradwave's
+``davidson_batched``, ``solvers/davidson.py:528-774``).
+
+Same algorithm and contract as the reference:
+
+* uniform subspace over all k, max_dim = min(max_dim_factor * nb, min_k npw);
+* Rayleigh-Ritz with the subspace matrix s = v^H H v in float64;
+* the n_add worst residuals per k (n_add = max_k #(|r| > tol)), TPA-filtered
+  and unit-normalised, projected twice against the basis and orthonormalised;
+* restart when the basis would exceed max_dim, re-orthonormalising the Ritz
+  block and transforming its images by the same triangular factor;
+* ``hit max_iter`` is not an error: the last Ritz pairs come back.
+
+What differs is where it runs: every step is a libgwb.so kernel or cuBLAS
+GEMM on the device, the basis lives in preallocated (nk, max_dim, npw)
+buffers (new rows are written in place, H applies land directly in the image
+buffer), the subspace matrix is updated incrementally (only the new columns
+are formed, ``gwb_subspace_insert``), and orthonormalisation is CholQR2
+(float64 Gram, Cholesky, triangular inverse; the reference's own optional
+path, ``solvers/davidson.py:195-222``) with the reference's jitter + QR
+fallback on breakdown.
+
+Modes:
+  ``mode="fp64"``     every apply in float64 (plain TPA Davidson).
+  ``mode="fp32exp"``  expansion applies in float32 arithmetic, every
+                      convergence decision certified with a float64 apply and
+                      a float64 nb x nb Rayleigh-Ritz, float64 hand-off after
+                      the first failed certification - the reference's
+                      fp32-expansion mode (``solvers/davidson.py:226-308,
+                      581-687``).
+``precond`` is ``"teter"`` or an object with ``apply_into(...)`` (the learned
+preconditioner, ``gradwave_b200.learned``), which falls back to TPA per band.
+"""
+
+from __future__ import annotations
+
+import logging
+import math
+from dataclasses import dataclass, field
+
+import torch
+
+from . import _lib
+from .telemetry import opcount
+
+logger = logging.getLogger(__name__)
+
+_FP32_CERT_FLOOR_EPS = 32 * torch.finfo(torch.float32).eps
+_FP32_CERT_STALL = 0.7
+_N, _T, _H = 0, 1, 2
+
+
+@dataclass
+class BatchedDavidsonResult:
+    eigenvalues: torch.Tensor      # (nk, nb) ascending [eV]
+    eigenvectors: torch.Tensor     # (nk, nb, npw_max), padded slots zero
+    n_iter: int
+    residual_norms: torch.Tensor   # (nk, nb)
+    n_apply_low: int = 0
+    n_apply_full: int = 0
+    info: dict = field(default_factory=dict)
+
+
+def _ptr(t: torch.Tensor, offset_elems: int = 0) -> int:
+    return t.data_ptr() + offset_elems * t.element_size()
+
+
+def zgemm(opA, opB, M, N, K, A, lda, sA, B, ldb, sB, C, ldc, sC, batch, alpha=1.0, beta=0.0,
+          a_off=0, b_off=0, c_off=0, stream=None):
+    """Row-major batched complex128 GEMM through gwb_zgemm (offsets in elements)."""
+    s = _lib.stream_ptr(C.device) if stream is None else stream
+    a = complex(alpha)
+    b = complex(beta)
+    _lib.call("gwb_zgemm", opA, opB, M, N, K, a.real, a.imag, _ptr(A, a_off), lda, sA, _ptr(B, b_off), ldb,
+              sB, b.real, b.imag, _ptr(C, c_off), ldc, sC, batch, s)
+
+
+class _Workspace:
+    """Device buffers of one solve (allocated once, reused every round)."""
+
+    def __init__(self, nk, nb, npw, max_dim, dev):
+        c = dict(dtype=torch.complex128, device=dev)
+        self.V = torch.zeros(nk, max_dim, npw, **c)
+        self.HV = torch.zeros(nk, max_dim, npw, **c)
+        self.S = torch.zeros(nk, max_dim, max_dim, **c)
+        self.X = torch.zeros(nk, nb, npw, **c)
+        self.HX = torch.zeros(nk, nb, npw, **c)
+        self.R = torch.zeros(nk, nb, npw, **c)
+        self.D = torch.zeros(nk, nb, npw, **c)
+        self.D2 = torch.zeros(nk, nb, npw, **c)
+        self.C = torch.zeros(nk * max_dim * max_dim, **c)
+        self.G = torch.zeros(nk, nb, nb, **c)
+        self.Linv = torch.zeros(nk, nb, nb, **c)
+        self.rn = torch.zeros(nk, nb, dtype=torch.float64, device=dev)
+        self.stats = torch.zeros(2, dtype=torch.float64, device=dev)
+        self.sel = torch.zeros(nk, nb, dtype=torch.int32, device=dev)
+        self.info = torch.zeros(nk, dtype=torch.int32, device=dev)
+
+
+class _Solver:
+    def __init__(self, h_apply, x0, t, mask, tol, max_iter, max_dim_factor, mode, precond, history_out):
+        if not x0.is_cuda:
+            raise RuntimeError("davidson_batched (B200 path) needs CUDA tensors: there is no CPU fallback")
+        if mode not in ("fp64", "fp32exp"):
+            raise ValueError(f"mode must be 'fp64' or 'fp32exp', got {mode!r}")
+        self.h_apply = h_apply
+        self.ham = getattr(h_apply, "__self__", None)
+        if self.ham is not None and not hasattr(self.ham, "apply_into"):
+            self.ham = None
+        self.out_dtype = x0.dtype
+        self.nk, self.nb, self.npw = (int(s) for s in x0.shape)
+        self.dev = x0.device
+        self.mask = mask.to(self.dev)
+        self.t = t.to(self.dev, torch.float64).contiguous()
+        self.tol = float(tol)
+        self.max_iter = int(max_iter)
+        self.max_dim = min(max_dim_factor * self.nb, int(self.mask.sum(dim=1).min()))
+        if self.max_dim < self.nb:
+            raise ValueError(f"basis of {self.max_dim} cannot hold {self.nb} bands")
+        # a complex64 block is a low-precision draft: float32 applies throughout
+        self.fp32_exp = mode == "fp32exp" and x0.dtype == torch.complex128
+        self.all_fp32 = x0.dtype == torch.complex64
+        self.precond = precond
+        self.history_out = history_out
+        self.ws = _Workspace(self.nk, self.nb, self.npw, self.max_dim, self.dev)
+        self.n_low = 0
+        self.n_full = 0
+        self.n_restart = 0
+        self.n_cert = 0
+        self.n_fallback_qr = 0
+        self.stream = _lib.stream_ptr(self.dev)
+        self.x0 = x0
+
+    # -- primitives -----------------------------------------------------------
+    def apply_block(self, src: torch.Tensor, src_off: int, src_ks: int, nrows: int, dst: torch.Tensor,
+                    dst_off: int, dst_ks: int, low: bool):
+        """H on nrows rows of src (k stride src_ks) into dst rows (k stride dst_ks)."""
+        n = self.nk * nrows
+        if low:
+            self.n_low += n
+        else:
+            self.n_full += n
+        prec = _lib.GWB_FP32 if (low or self.all_fp32) else _lib.GWB_FP64
+        if self.ham is not None:
+            self.ham.apply_into(_ptr(src, src_off), src_ks, _ptr(dst, dst_off), dst_ks, nrows, prec,
+                                n_rows_counted=n)
+            return
+        # generic callable: contiguous copy in, result copied out
+        blk = src.view(-1)[src_off:].as_strided((self.nk, nrows, self.npw), (src_ks, self.npw, 1)).clone()
+        if prec == _lib.GWB_FP32:
+            out = self.h_apply(blk.to(torch.complex64)).to(torch.complex128)
+        else:
+            out = self.h_apply(blk)
+        dview = dst.view(-1)[dst_off:].as_strided((self.nk, nrows, self.npw), (dst_ks, self.npw, 1))
+        dview.copy_(out)
+
+    def cholqr2(self, Y: torch.Tensor, n: int, Ytmp: torch.Tensor, Z: torch.Tensor | None = None,
+                Ztmp: torch.Tensor | None = None):
+        """Orthonormalise the first n rows of Y (nk, >=n, npw) in place by two
+        rounds of float64 Gram -> Cholesky -> L^-1 (Z, if given, gets the same
+        row transform). Returns False on a Cholesky breakdown (Y untouched)."""
+        ws, nk, npw = self.ws, self.nk, self.npw
+        ys, zs = Y.shape[1] * npw, None if Z is None else Z.shape[1] * npw
+        for _ in range(2):
+            zgemm(_N, _H, n, n, npw, Y, npw, ys, Y, npw, ys, ws.G, n, n * n, nk, stream=self.stream)
+            _lib.call("gwb_chol_inv", nk, n, _ptr(ws.G), n, n * n, _ptr(ws.Linv), n * n, _ptr(ws.info),
+                      self.stream)
+            if int(ws.info.max()) != 0:
+                return False
+            zgemm(_N, _N, n, npw, n, ws.Linv, n, n * n, Y, npw, ys, Ytmp, npw, Ytmp.shape[1] * npw, nk,
+                  stream=self.stream)
+            Y[:, :n].copy_(Ytmp[:, :n])
+            if Z is not None:
+                zgemm(_N, _N, n, npw, n, ws.Linv, n, n * n, Z, npw, zs, Ztmp, npw, Ztmp.shape[1] * npw, nk,
+                      stream=self.stream)
+                Z[:, :n].copy_(Ztmp[:, :n])
+        return True
+
+    def project_out(self, Dblk: torch.Tensor, n: int, m: int):
+        """D -= (D V^H) V twice over the first m basis rows (float64 GEMMs)."""
+        ws, nk, npw, md = self.ws, self.nk, self.npw, self.max_dim
+        ds = Dblk.shape[1] * npw
+        for _ in range(2):
+            zgemm(_N, _H, n, m, npw, Dblk, npw, ds, ws.V, npw, md * npw, ws.C, m, n * m, nk,
+                  stream=self.stream)
+            zgemm(_N, _N, n, npw, m, ws.C, m, n * m, ws.V, npw, md * npw, Dblk, npw, ds, nk, alpha=-1.0,
+                  beta=1.0, stream=self.stream)
+
+    def orthonormalize_new(self, n: int, m: int):
+        """Rows D[:, :n] -> orthonormal, orthogonal to V[:, :m] (reference
+        ``_orthonormalize_b``, gradwave solvers/davidson.py:406-457)."""
+        ws = self.ws
+        D = ws.D
+        D[:, :n].mul_(self.mask[:, None, :])
+        if m:
+            self.project_out(D, n, m)
+        if self.cholqr2(D, n, ws.D2):
+            return
+        # breakdown: the reference's rank repair - seeded jitter on (near-)zero
+        # rows, re-projection, Householder QR
+        self.n_fallback_qr += 1
+        blk = D[:, :n]
+        bad = torch.linalg.vector_norm(blk, dim=-1, keepdim=True) < 1e-8
+        if bool(bad.any()):
+            gen = torch.Generator(device="cpu").manual_seed(n + 7919)
+            noise = torch.randn(self.nk, n, self.npw, 2, generator=gen, dtype=torch.float64)
+            jit = torch.view_as_complex(noise).to(self.dev)
+            blk.add_(bad * jit).mul_(self.mask[:, None, :])
+            if m:
+                self.project_out(D, n, m)
+        q, _ = torch.linalg.qr(D[:, :n].transpose(-1, -2), mode="reduced")
+        D[:, :n].copy_(q.transpose(-1, -2))
+
+    def rayleigh_ritz(self, m: int, m0: int):
+        """Update s (new columns m0..m-1), eigensolve, Ritz block X/HX, residuals."""
+        ws, nk, npw, nb, md = self.ws, self.nk, self.npw, self.nb, self.max_dim
+        nnew = m - m0
+        zgemm(_N, _H, m, nnew, npw, ws.V, npw, md * npw, ws.HV, npw, md * npw, ws.C, nnew, m * nnew, nk,
+              b_off=m0 * npw, stream=self.stream)
+        _lib.call("gwb_subspace_insert", nk, m, m0, _ptr(ws.C), _ptr(ws.S), md, md * md, self.stream)
+        opcount.bump("eigh")
+        w, u = torch.linalg.eigh(ws.S[:, :m, :m])
+        eig = w[:, :nb].contiguous()
+        u = u.contiguous()
+        zgemm(_T, _N, nb, npw, m, u, m, m * m, ws.V, npw, md * npw, ws.X, npw, nb * npw, nk, stream=self.stream)
+        zgemm(_T, _N, nb, npw, m, u, m, m * m, ws.HV, npw, md * npw, ws.HX, npw, nb * npw, nk,
+              stream=self.stream)
+        self.residuals(eig)
+        return eig
+
+    def residuals(self, eig):
+        ws, nk, nb, npw = self.ws, self.nk, self.nb, self.npw
+        _lib.call("gwb_residual", nk, nb, npw, _ptr(ws.X), nb * npw, _ptr(ws.HX), nb * npw, _ptr(eig), nb,
+                  _ptr(ws.R), nb * npw, _ptr(ws.rn), self.stream)
+
+    def certify(self):
+        """Float64 refresh of the Ritz block (reference ``_certify_fp64``,
+        gradwave solvers/davidson.py:287-308)."""
+        ws, nk, nb, npw = self.ws, self.nk, self.nb, self.npw
+        self.n_cert += 1
+        self.apply_block(ws.X, 0, nb * npw, nb, ws.HX, 0, nb * npw, low=False)
+        zgemm(_N, _H, nb, nb, npw, ws.X, npw, nb * npw, ws.HX, npw, nb * npw, ws.G, nb, nb * nb, nk,
+              stream=self.stream)
+        s = ws.G.conj()
+        s = 0.5 * (s + s.conj().transpose(-1, -2))
+        opcount.bump("eigh")
+        w, u = torch.linalg.eigh(s)
+        u = u.contiguous()
+        eig = w.contiguous()
+        zgemm(_T, _N, nb, npw, nb, u, nb, nb * nb, ws.X, npw, nb * npw, ws.D2, npw, nb * npw, nk,
+              stream=self.stream)
+        ws.X.copy_(ws.D2)
+        zgemm(_T, _N, nb, npw, nb, u, nb, nb * nb, ws.HX, npw, nb * npw, ws.D2, npw, nb * npw, nk,
+              stream=self.stream)
+        ws.HX.copy_(ws.D2)
+        self.residuals(eig)
+        return eig
+
+    def read_stats(self):
+        _lib.call("gwb_conv_stats", self.nk, self.nb, _ptr(self.ws.rn), self.tol, _ptr(self.ws.stats),
+                  self.stream)
+        st = self.ws.stats.tolist()
+        return st[0], int(st[1])
+
+    # -- the solve --------------------------------------------------------------
+    def run(self) -> BatchedDavidsonResult:
+        ws, nk, nb, npw, md = self.ws, self.nk, self.nb, self.npw, self.max_dim
+        ws.D[:, :nb].copy_(self.x0.to(torch.complex128))
+        self.orthonormalize_new(nb, 0)
+        ws.V[:, :nb].copy_(ws.D[:, :nb])
+        self.apply_block(ws.V, 0, md * npw, nb, ws.HV, 0, md * npw, low=self.fp32_exp)
+        # m: basis rows in use; m0: first column of s not formed yet (0 = rebuild)
+        m, m0 = nb, 0
+        cert_floor = _FP32_CERT_FLOOR_EPS * max(float(self.t.max()), 1.0) if self.fp32_exp else 0.0
+        prev_rnmax = math.inf
+        eig = None
+        for it in range(1, self.max_iter + 1):
+            eig = self.rayleigh_ritz(m, m0)
+            m0 = m
+            rnmax, n_add = self.read_stats()
+            if self.fp32_exp:
+                stalled = it > 1 and rnmax > _FP32_CERT_STALL * prev_rnmax
+                prev_rnmax = rnmax
+                if rnmax < max(self.tol, cert_floor) or stalled:
+                    eig = self.certify()
+                    rnmax, n_add = self.read_stats()
+                    if rnmax >= self.tol:
+                        # hand-off: collapse to the certified block with exact
+                        # images and continue with float64 expansion applies
+                        ws.V[:, :nb].copy_(ws.X)
+                        ws.HV[:, :nb].copy_(ws.HX)
+                        m, m0 = nb, 0
+                        self.fp32_exp = False
+            if self.history_out is not None:
+                self.history_out.append((it, ws.rn.cpu().clone(), eig.cpu().clone()))
+            if rnmax < self.tol:
+                return self.result(eig, it)
+            _lib.call("gwb_select_worst", nk, nb, _ptr(ws.rn), n_add, _ptr(ws.sel), self.stream)
+            self.precondition(n_add, eig)
+            if m + n_add > md:
+                # restart: re-orthonormalise the Ritz block, images by the same
+                # transform (no re-application), keep the new directions
+                self.n_restart += 1
+                if not self.cholqr2(ws.X, nb, ws.D2, ws.HX, ws.R):
+                    q, r = torch.linalg.qr(ws.X.transpose(-1, -2), mode="reduced")
+                    ws.X.copy_(q.transpose(-1, -2))
+                    ws.HX.copy_(torch.linalg.solve_triangular(r.transpose(-1, -2), ws.HX, upper=False))
+                ws.V[:, :nb].copy_(ws.X)
+                ws.HV[:, :nb].copy_(ws.HX)
+                m, m0 = nb, 0
+            self.orthonormalize_new(n_add, m)
+            ws.V[:, m:m + n_add].copy_(ws.D[:, :n_add])
+            self.apply_block(ws.V, m * npw, md * npw, n_add, ws.HV, m * npw, md * npw, low=self.fp32_exp)
+            m += n_add
+        if self.fp32_exp:
+            eig = self.certify()
+        if logger.isEnabledFor(logging.DEBUG):
+            logger.debug("batched Davidson hit max_iter=%d (max res=%.3e > tol=%.1e)", self.max_iter,
+                         float(ws.rn.max()), self.tol)
+        return self.result(eig, self.max_iter)
+
+    def precondition(self, n_add: int, eig: torch.Tensor):
+        """D[:, :n_add] = preconditioned, unit-normalised worst residuals."""
+        ws, nk, nb, npw = self.ws, self.nk, self.nb, self.npw
+        if self.precond is None or (isinstance(self.precond, str) and self.precond == "teter"):
+            _lib.call("gwb_precond_teter", nk, nb, n_add, npw, _ptr(ws.X), nb * npw, _ptr(ws.R), nb * npw,
+                      _ptr(self.t), _ptr(ws.sel), _ptr(ws.D), nb * npw, self.stream)
+        else:
+            self.precond.apply_into(self, n_add, eig)
+
+    def result(self, eig, it) -> BatchedDavidsonResult:
+        ws = self.ws
+        x = ws.X.clone()
+        if self.out_dtype != torch.complex128:
+            x = x.to(self.out_dtype)
+        info = {"n_restart": self.n_restart, "n_cert": self.n_cert, "n_fallback_qr": self.n_fallback_qr,
+                "max_dim": self.max_dim}
+        return BatchedDavidsonResult(eig.clone(), x, it, ws.rn.clone(), self.n_low, self.n_full, info)
+
+
+def davidson_batched(h_apply, x0, t, mask, tol: float = 1e-9, max_iter: int = 40, max_dim_factor: int = 4,
+                     sync_free: bool = False, history_out=None, *, mode: str = "fp64",
+                     precond="teter") -> BatchedDavidsonResult:
+    """Batched block Davidson (see module docstring). ``sync_free`` is
+    accepted for signature parity and ignored (every round reads two device
+    scalars, like the reference's synchronous path)."""
+    with torch.no_grad():
+        return _Solver(h_apply, x0, t, mask, tol, max_iter, max_dim_factor, mode, precond, history_out).run()

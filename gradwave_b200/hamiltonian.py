@@ -118,5 +118,18 @@ class BatchedHamiltonian:
         self._count(c)
         return torch.ops.gwb.ham_apply(self.handle, c, _lib.GWB_FP32)
 
+    def apply_into(self, src_ptr: int, src_kstride: int, dst_ptr: int, dst_kstride: int, nrows: int,
+                   prec: int, n_rows_counted: int | None = None) -> None:
+        """H on nrows complex128 rows per k read at src (k blocks src_kstride
+        elements apart) written to dst: the in-place form the Davidson basis
+        uses (``gwb_ham_apply_strided``)."""
+        n = self.nk * nrows if n_rows_counted is None else n_rows_counted
+        if _TALLY["on"]:
+            _TALLY["count"] += n
+        opcount.bump("hpsi", n)
+        opcount.bump("fft", 2)
+        _lib.call("gwb_ham_apply_strided", self._h, src_ptr, src_kstride, dst_ptr, dst_kstride, nrows,
+                  _lib.GWB_C128, prec, _lib.stream_ptr(self.device))
+
     def scratch_bytes(self) -> int:
         return int(_lib.load().gwb_ham_scratch_bytes(self._h))

@@ -56,6 +56,8 @@ extern "C" {
 const char* gwb_last_error(void);
 /* Library version string. */
 const char* gwb_version(void);
+/* Number of kernels this library has launched in the process so far. */
+unsigned long long gwb_launch_count(void);
 
 /* ======================================================================= */
 /* Hamiltonian apply                                                       */
@@ -98,8 +100,62 @@ int gwb_ham_set_projectors(gwb_ham* h, const void* p, const double* dij, void* s
 int gwb_ham_apply(gwb_ham* h, const void* c, void* out, int32_t nb, int32_t io_dtype,
                   int32_t prec, void* stream);
 
+/* As gwb_ham_apply with explicit distances (in complex elements) between the
+ * k blocks of c and of out, so a band slice of a larger (nk, m, npw_max) block
+ * (the Davidson basis) can be read or written in place. Each k block holds nb
+ * contiguous rows of npw_max. */
+int gwb_ham_apply_strided(gwb_ham* h, const void* c, int64_t c_kstride, void* out, int64_t out_kstride,
+                          int32_t nb, int32_t io_dtype, int32_t prec, void* stream);
+
 /* Bytes of handle-owned device scratch currently held. */
 size_t gwb_ham_scratch_bytes(const gwb_ham* h);
+
+/* ======================================================================= */
+/* Davidson steps (complex128 blocks, float64 reductions)                  */
+/* A "k stride" is the distance in complex elements between the blocks of   */
+/* consecutive k; rows inside a block are npw apart.                        */
+/* ======================================================================= */
+
+/* Batched row-major complex128 GEMM: C = alpha op(A) op(B) + beta C per batch,
+ * op 0 = N, 1 = T, 2 = H; op(A) is M x K, op(B) K x N. Plain cuBLAS ZGEMM.
+ * Replaces the torch.matmul/einsum products of gradwave
+ * solvers/davidson.py:428-432,648-654,752-756. */
+int gwb_zgemm(int opA, int opB, int64_t M, int64_t N, int64_t K, double alpha_re, double alpha_im,
+              const void* A, int64_t lda, int64_t strideA, const void* B, int64_t ldb, int64_t strideB,
+              double beta_re, double beta_im, void* C, int64_t ldc, int64_t strideC, int64_t batch,
+              void* stream);
+
+/* r = hx - eig * x and rn = |r| per (k, band); eig (nk, eig_kstride) float64.
+ * Replaces gradwave solvers/davidson.py:656-657. */
+int gwb_residual(int32_t nk, int32_t nb, int32_t npw, const void* x, int64_t x_kstride, const void* hx,
+                 int64_t hx_kstride, const double* eig, int64_t eig_kstride, void* r, int64_t r_kstride,
+                 double* rn, void* stream);
+
+/* out[0] = max rn, out[1] = max over k of #(rn > tol) (device doubles).
+ * Replaces the two host reads of gradwave solvers/davidson.py:692,698. */
+int gwb_conv_stats(int32_t nk, int32_t nb, const double* rn, double tol, double* out, void* stream);
+
+/* sel (nk, n_add) int32: per k the bands of the n_add largest rn, largest
+ * first, ties by band order. Replaces gradwave solvers/davidson.py:729. */
+int gwb_select_worst(int32_t nk, int32_t nb, const double* rn, int32_t n_add, int32_t* sel, void* stream);
+
+/* d[k][s] = TPA(t, <x_b|T|x_b>) * r[k][b] / |...| for b = sel[k][s].
+ * Replaces gradwave solvers/davidson.py:730-743 and solvers/precond.py:20-39. */
+int gwb_precond_teter(int32_t nk, int32_t nb, int32_t n_add, int32_t npw, const void* x, int64_t x_kstride,
+                      const void* r, int64_t r_kstride, const double* t, const int32_t* sel, void* d,
+                      int64_t d_kstride, void* stream);
+
+/* Insert the new columns m0..m-1 (and mirrored rows) of the subspace matrix
+ * S (nk, lds, lds) from C (nk, m, m-m0) = V[:m] . HV[m0:m]^H; Hermitises the
+ * new diagonal block. Replaces gradwave solvers/davidson.py:648-649. */
+int gwb_subspace_insert(int32_t nk, int32_t m, int32_t m0, const void* C, void* S, int32_t lds,
+                        int64_t s_kstride, void* stream);
+
+/* Per k: G (n x n, leading dim ldg) -> lower Cholesky factor in place and
+ * Linv = L^-1 (n x n, leading dim n); info[k] = 0 or j+1 at a non-positive
+ * pivot j. CholQR step of gradwave solvers/davidson.py:195-222. */
+int gwb_chol_inv(int32_t nk, int32_t n, void* G, int32_t ldg, int64_t g_kstride, void* Linv,
+                 int64_t linv_kstride, int32_t* info, void* stream);
 
 #ifdef __cplusplus
 }
