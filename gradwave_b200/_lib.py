@@ -74,6 +74,8 @@ _SIGNATURES = {
     "gwb_precond_teter": [_I, _I, _I, _I, _P, _I64, _P, _I64, _P, _P, _P, _I64, _P],
     "gwb_subspace_insert": [_I, _I, _I, _P, _P, _I, _I64, _P],
     "gwb_chol_inv": [_I, _I, _P, _I, _I64, _P, _I64, _P, _P],
+    "gwb_heev_lowest": [_I, _I, _I, _P, _I, _I64, _P, _P, _P, _P, _P],
+    "gwb_heev_max_dim": [],
 }
 _RESTYPES = {"gwb_last_error": ctypes.c_char_p, "gwb_version": ctypes.c_char_p,
              "gwb_launch_count": ctypes.c_ulonglong,

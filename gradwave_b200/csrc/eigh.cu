@@ -1,0 +1,291 @@
+// Batched float64 Hermitian eigensolver for the Davidson subspace matrices
+// (replaces torch.linalg.eigh in gradwave solvers/davidson.py:66-75,650).
+//
+// One CTA per matrix, the matrix in shared memory (m <= GWB_HEEV_MMAX), three
+// textbook stages:
+//   1. Householder tridiagonalisation with Hermitian reflectors
+//      P_j = I - w_j u_j u_j^H, A <- P_j A P_j (Golub & Van Loan, Matrix
+//      Computations, 4th ed., sec. 8.3.1, complex form); the complex
+//      subdiagonal is made real by a diagonal phase D (T = D T_r D^H).
+//   2. Implicit QL with Wilkinson-type shifts on the real tridiagonal T_r
+//      (Bowdler, Martin, Reinsch & Wilkinson, "The QR and QL algorithms for
+//      symmetric matrices", Numer. Math. 11 (1968), procedure tql2). One thread
+//      runs the scalar recurrence of a sweep and records its plane rotations;
+//      then every thread applies them to its rows of the eigenvector matrix Z
+//      (column-major in global scratch, coalesced).
+//   3. The lowest nb eigenpairs, ascending: y = Q D z with Q = P_0 ... P_{m-3},
+//      one warp per eigenvector, no block barriers.
+// Every loop is bounded: a QL iteration cap reports info = 1 instead of
+// spinning.
+#include <cmath>
+
+#include "common.cuh"
+
+#define GWB_HEEV_MMAX 112
+
+namespace gwb {
+
+constexpr int HEEV_THREADS = 256;
+constexpr int QL_MAX_ITER = 60;
+
+__device__ __forceinline__ double blk_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = l < HEEV_THREADS / 32 ? red[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (l == 0) red[0] = v;
+  }
+  __syncthreads();
+  v = red[0];
+  __syncthreads();
+  return v;
+}
+
+// S (nk, lds, lds) row-major Hermitian (both triangles filled), leading m x m.
+// eig (nk, nb) ascending; U (nk, m, nb) row-major eigenvector columns;
+// Z scratch (nk, m, m) float64; info (nk).
+__global__ void __launch_bounds__(HEEV_THREADS) k_heev_lowest(const cplx<double>* __restrict__ S, int lds,
+                                                              int64_t sk, int m, int nb, double* __restrict__ eig,
+                                                              cplx<double>* __restrict__ U,
+                                                              double* __restrict__ Zg, int* __restrict__ info) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<double>* A = reinterpret_cast<cplx<double>*>(smem_raw);  // m*m
+  cplx<double>* pv = A + m * m;                                  // m  (p, then q)
+  cplx<double>* ec = pv + m;                                     // m  complex subdiagonal
+  cplx<double>* ph = ec + m;                                     // m  phases
+  double* d = reinterpret_cast<double*>(ph + m);                 // m
+  double* er = d + m;                                            // m
+  double* wv = er + m;                                           // m  reflector scales
+  double* rc = wv + m;                                           // m  rotation cosines
+  double* rs = rc + m;                                           // m  rotation sines
+  int* order = reinterpret_cast<int*>(rs + m);                   // m
+  __shared__ double red[HEEV_THREADS / 32];
+  __shared__ int s_ctl[4];  // 0: mm, 1: lowest rotation index, 2: converged-l flag, 3: fail
+  const int k = blockIdx.x, tid = threadIdx.x;
+  const cplx<double>* Sk = S + k * sk;
+  double* Z = Zg + (int64_t)k * m * m;  // Z(row r, col i) at Z[i*m + r]
+
+  for (int i = tid; i < m * m; i += blockDim.x) A[i] = Sk[(int64_t)(i / m) * lds + (i % m)];
+  __syncthreads();
+
+  // ---- 1. tridiagonalisation -------------------------------------------
+  for (int j = 0; j + 2 < m; ++j) {
+    const int r0 = j + 1, nr = m - r0;
+    double s2 = 0.0;
+    for (int r = r0 + tid; r < m; r += blockDim.x) s2 += norm2(A[r * m + j]);
+    s2 = blk_sum(s2, red);
+    if (tid == 0) d[j] = A[j * m + j].x;
+    if (s2 == 0.0) {
+      if (tid == 0) {
+        wv[j] = 0.0;
+        ec[j] = mk<double>(0.0, 0.0);
+      }
+      __syncthreads();
+      continue;
+    }
+    const double sig = sqrt(s2);
+    const cplx<double> x0 = A[r0 * m + j];
+    const double a0 = sqrt(norm2(x0));
+    const cplx<double> phs = a0 > 0.0 ? scale(x0, 1.0 / a0) : mk<double>(1.0, 0.0);
+    const double w = 1.0 / (sig * (sig + a0));
+    __syncthreads();
+    if (tid == 0) {
+      A[r0 * m + j] = x0 + scale(phs, sig);  // u_0; the rest of u is the column itself
+      wv[j] = w;
+      ec[j] = scale(phs, -sig);
+    }
+    __syncthreads();
+    // p_r = w sum_c A[r][c] u_c = w sum_c conj(A[c][r]) u_c (column reads are conflict free)
+    for (int rr = tid; rr < nr; rr += blockDim.x) {
+      const int r = r0 + rr;
+      cplx<double> acc = mk<double>(0.0, 0.0);
+      for (int c = r0; c < m; ++c) acc = acc + conj_mul(A[c * m + r], A[c * m + j]);
+      pv[rr] = scale(acc, w);
+    }
+    __syncthreads();
+    double kk = 0.0;
+    for (int rr = tid; rr < nr; rr += blockDim.x) {
+      const cplx<double> u = A[(r0 + rr) * m + j];
+      kk += u.x * pv[rr].x + u.y * pv[rr].y;  // Re(conj(u) p)
+    }
+    kk = 0.5 * w * blk_sum(kk, red);
+    for (int rr = tid; rr < nr; rr += blockDim.x) pv[rr] = pv[rr] - scale(A[(r0 + rr) * m + j], kk);
+    __syncthreads();
+    for (int idx = tid; idx < nr * nr; idx += blockDim.x) {
+      const int rr = idx / nr, cc = idx % nr;
+      const cplx<double> ur = A[(r0 + rr) * m + j], uc = A[(r0 + cc) * m + j];
+      cplx<double>& a = A[(r0 + rr) * m + r0 + cc];
+      a = a - mul_conj(ur, pv[cc]) - mul_conj(pv[rr], uc);
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    if (m >= 2) {
+      d[m - 2] = A[(m - 2) * m + m - 2].x;
+      ec[m - 2] = A[(m - 1) * m + m - 2];
+      if (m == 2) wv[0] = 0.0;
+    }
+    d[m - 1] = A[(m - 1) * m + m - 1].x;
+    // phases making the subdiagonal real: ph[j+1] = ph[j] e_j / |e_j|
+    ph[0] = mk<double>(1.0, 0.0);
+    for (int j = 0; j + 1 < m; ++j) {
+      const double a = sqrt(norm2(ec[j]));
+      er[j] = a;
+      ph[j + 1] = a > 0.0 ? ph[j] * scale(ec[j], 1.0 / a) : ph[j];
+    }
+    er[m - 1] = 0.0;
+    s_ctl[3] = 0;
+  }
+  for (int i = tid; i < m * m; i += blockDim.x) Z[i] = (i / m == i % m) ? 1.0 : 0.0;
+  __syncthreads();
+
+  // ---- 2. implicit QL on (d, er), rotations deferred to Z ---------------
+  const double eps = 2.220446049250313e-16;
+  int l = 0, iter = 0;
+  while (l < m) {
+    if (tid == 0) {
+      int mm = l;
+      while (mm < m - 1) {
+        const double dd = fabs(d[mm]) + fabs(d[mm + 1]);
+        if (fabs(er[mm]) <= eps * dd) break;
+        ++mm;
+      }
+      s_ctl[0] = mm;
+      s_ctl[2] = (mm == l);
+      if (mm != l) {
+        if (iter >= QL_MAX_ITER) {
+          s_ctl[3] = 1;
+          s_ctl[2] = 1;
+        } else {
+          double g = (d[l + 1] - d[l]) / (2.0 * er[l]);
+          double r = hypot(g, 1.0);
+          g = d[mm] - d[l] + er[l] / (g + copysign(r, g));
+          double s = 1.0, c = 1.0, p = 0.0;
+          int i = mm - 1;
+          bool broke = false;
+          for (; i >= l; --i) {
+            const double f = s * er[i], b = c * er[i];
+            r = hypot(f, g);
+            er[i + 1] = r;
+            if (r == 0.0) {
+              d[i + 1] -= p;
+              er[mm] = 0.0;
+              broke = true;
+              break;
+            }
+            s = f / r;
+            c = g / r;
+            g = d[i + 1] - p;
+            r = (d[i] - g) * s + 2.0 * c * b;
+            p = s * r;
+            d[i + 1] = g + p;
+            g = c * r - b;
+            rc[i] = c;
+            rs[i] = s;
+          }
+          s_ctl[1] = broke ? i + 1 : l;  // rotations mm-1 .. s_ctl[1] were recorded
+          if (!broke) {
+            d[l] -= p;
+            er[l] = g;
+            er[mm] = 0.0;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (s_ctl[3]) break;
+    if (s_ctl[2]) {
+      ++l;
+      iter = 0;
+      __syncthreads();
+      continue;
+    }
+    ++iter;
+    const int mm = s_ctl[0], ilo = s_ctl[1];
+    for (int r = tid; r < m; r += blockDim.x) {
+      for (int i = mm - 1; i >= ilo; --i) {
+        const double zi = Z[(int64_t)i * m + r], zi1 = Z[(int64_t)(i + 1) * m + r];
+        Z[(int64_t)(i + 1) * m + r] = rs[i] * zi + rc[i] * zi1;
+        Z[(int64_t)i * m + r] = rc[i] * zi - rs[i] * zi1;
+      }
+    }
+    __syncthreads();
+  }
+  if (s_ctl[3]) {
+    if (tid == 0) info[k] = 1;
+    return;
+  }
+  // ascending order (stable)
+  for (int i = tid; i < m; i += blockDim.x) {
+    int rank = 0;
+    for (int j = 0; j < m; ++j) rank += (d[j] < d[i] || (d[j] == d[i] && j < i)) ? 1 : 0;
+    order[rank] = i;
+  }
+  __syncthreads();
+  if (tid == 0) info[k] = 0;
+  for (int a = tid; a < nb; a += blockDim.x) eig[(int64_t)k * nb + a] = d[order[a]];
+
+  // ---- 3. back-transform y = Q D z, one warp per eigenvector -------------
+  const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+  constexpr int PER = (GWB_HEEV_MMAX + 31) / 32;
+  cplx<double>* Uk = U + (int64_t)k * m * nb;
+  for (int a = warp; a < nb; a += nw) {
+    const int src = order[a];
+    cplx<double> y[PER];
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+      const int r = lane + 32 * t;
+      y[t] = r < m ? scale(ph[r], Z[(int64_t)src * m + r]) : mk<double>(0.0, 0.0);
+    }
+    for (int j = m - 3; j >= 0; --j) {
+      const double w = wv[j];
+      if (w == 0.0) continue;
+      cplx<double> dot = mk<double>(0.0, 0.0);
+#pragma unroll
+      for (int t = 0; t < PER; ++t) {
+        const int r = lane + 32 * t;
+        if (r > j && r < m) dot = dot + conj_mul(A[r * m + j], y[t]);
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        dot.x += __shfl_xor_sync(0xffffffffu, dot.x, o);
+        dot.y += __shfl_xor_sync(0xffffffffu, dot.y, o);
+      }
+      dot = scale(dot, w);
+#pragma unroll
+      for (int t = 0; t < PER; ++t) {
+        const int r = lane + 32 * t;
+        if (r > j && r < m) y[t] = y[t] - A[r * m + j] * dot;
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+      const int r = lane + 32 * t;
+      if (r < m) Uk[(int64_t)r * nb + a] = y[t];
+    }
+  }
+}
+
+size_t heev_smem(int m) { return (size_t)m * m * 16 + (size_t)m * (3 * 16 + 5 * 8 + 4) + 64; }
+
+}  // namespace gwb
+
+using namespace gwb;
+
+extern "C" int gwb_heev_lowest(int32_t nk, int32_t m, int32_t nb, const void* S, int32_t lds, int64_t s_kstride,
+                               double* eig, void* U, double* zscratch, int32_t* info, void* stream) {
+  GWB_REQUIRE(nk > 0 && m > 0 && nb > 0 && nb <= m && lds >= m, "bad sizes");
+  GWB_REQUIRE(m <= GWB_HEEV_MMAX, "m exceeds the shared-memory eigensolver limit (112)");
+  GWB_REQUIRE(S && eig && U && zscratch && info, "null pointer");
+  const size_t sm = heev_smem(m);
+  GWB_CUDA_TRY(cudaFuncSetAttribute(k_heev_lowest, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  k_heev_lowest<<<nk, HEEV_THREADS, sm, (cudaStream_t)stream>>>((const cplx<double>*)S, lds, s_kstride, m, nb, eig,
+                                                                (cplx<double>*)U, zscratch, info);
+  GWB_LAUNCH_CHECK();
+  count_launches(1);
+  return GWB_OK;
+}
+
+extern "C" int gwb_heev_max_dim(void) { return GWB_HEEV_MMAX; }

@@ -34,8 +34,10 @@ preconditioner, ``gradwave_b200.learned``), which falls back to TPA per band.
 
 from __future__ import annotations
 
+import contextlib
 import logging
 import math
+import os
 from dataclasses import dataclass, field
 
 import torch
@@ -75,10 +77,42 @@ def zgemm(opA, opB, M, N, K, A, lda, sA, B, ldb, sB, C, ldc, sC, batch, alpha=1.
               sB, b.real, b.imag, _ptr(C, c_off), ldc, sC, batch, s)
 
 
+class _PhaseTimer:
+    """CUDA-event timing of the solver phases (``GWB_PROFILE=1``): events are
+    recorded on the solve stream and read once at the end."""
+
+    def __init__(self, on: bool):
+        self.on = on
+        self.events = []
+
+    @contextlib.contextmanager
+    def __call__(self, name: str):
+        if not self.on:
+            yield
+            return
+        e0 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        try:
+            yield
+        finally:
+            e1 = torch.cuda.Event(enable_timing=True)
+            e1.record()
+            self.events.append((name, e0, e1))
+
+    def summary(self) -> dict:
+        if not self.events:
+            return {}
+        torch.cuda.synchronize()
+        out: dict = {}
+        for name, e0, e1 in self.events:
+            out[name] = out.get(name, 0.0) + e0.elapsed_time(e1)
+        return {k: round(v, 4) for k, v in sorted(out.items(), key=lambda kv: -kv[1])}
+
+
 class _Workspace:
     """Device buffers of one solve (allocated once, reused every round)."""
 
-    def __init__(self, nk, nb, npw, max_dim, dev):
+    def __init__(self, nk, nb, npw, max_dim, dev, heev_max):
         c = dict(dtype=torch.complex128, device=dev)
         self.V = torch.zeros(nk, max_dim, npw, **c)
         self.HV = torch.zeros(nk, max_dim, npw, **c)
@@ -92,9 +126,15 @@ class _Workspace:
         self.G = torch.zeros(nk, nb, nb, **c)
         self.Linv = torch.zeros(nk, nb, nb, **c)
         self.rn = torch.zeros(nk, nb, dtype=torch.float64, device=dev)
-        self.stats = torch.zeros(2, dtype=torch.float64, device=dev)
+        self.stats = torch.zeros(3, dtype=torch.float64, device=dev)
         self.sel = torch.zeros(nk, nb, dtype=torch.int32, device=dev)
         self.info = torch.zeros(nk, dtype=torch.int32, device=dev)
+        self.heev_info = torch.zeros(nk, dtype=torch.int32, device=dev)
+        self.eig = torch.zeros(nk, nb, dtype=torch.float64, device=dev)
+        hm = min(max_dim, heev_max)
+        self.U = torch.zeros(nk, max(hm, nb), nb, **c)
+        self.Z = torch.zeros(nk, hm * hm, dtype=torch.float64, device=dev)
+        self.Gs = torch.zeros(nk, nb, nb, **c)
 
 
 class _Solver:
@@ -122,7 +162,8 @@ class _Solver:
         self.all_fp32 = x0.dtype == torch.complex64
         self.precond = precond
         self.history_out = history_out
-        self.ws = _Workspace(self.nk, self.nb, self.npw, self.max_dim, self.dev)
+        self.heev_max = int(_lib.load().gwb_heev_max_dim())
+        self.ws = _Workspace(self.nk, self.nb, self.npw, self.max_dim, self.dev, self.heev_max)
         self.n_low = 0
         self.n_full = 0
         self.n_restart = 0
@@ -130,6 +171,7 @@ class _Solver:
         self.n_fallback_qr = 0
         self.stream = _lib.stream_ptr(self.dev)
         self.x0 = x0
+        self.prof = _PhaseTimer(os.environ.get("GWB_PROFILE", "0") == "1")
 
     # -- primitives -----------------------------------------------------------
     def apply_block(self, src: torch.Tensor, src_off: int, src_ks: int, nrows: int, dst: torch.Tensor,
@@ -215,18 +257,38 @@ class _Solver:
         """Update s (new columns m0..m-1), eigensolve, Ritz block X/HX, residuals."""
         ws, nk, npw, nb, md = self.ws, self.nk, self.npw, self.nb, self.max_dim
         nnew = m - m0
-        zgemm(_N, _H, m, nnew, npw, ws.V, npw, md * npw, ws.HV, npw, md * npw, ws.C, nnew, m * nnew, nk,
-              b_off=m0 * npw, stream=self.stream)
-        _lib.call("gwb_subspace_insert", nk, m, m0, _ptr(ws.C), _ptr(ws.S), md, md * md, self.stream)
-        opcount.bump("eigh")
-        w, u = torch.linalg.eigh(ws.S[:, :m, :m])
-        eig = w[:, :nb].contiguous()
-        u = u.contiguous()
-        zgemm(_T, _N, nb, npw, m, u, m, m * m, ws.V, npw, md * npw, ws.X, npw, nb * npw, nk, stream=self.stream)
-        zgemm(_T, _N, nb, npw, m, u, m, m * m, ws.HV, npw, md * npw, ws.HX, npw, nb * npw, nk,
-              stream=self.stream)
-        self.residuals(eig)
+        with self.prof("subspace_gemm"):
+            zgemm(_N, _H, m, nnew, npw, ws.V, npw, md * npw, ws.HV, npw, md * npw, ws.C, nnew, m * nnew, nk,
+                  b_off=m0 * npw, stream=self.stream)
+            _lib.call("gwb_subspace_insert", nk, m, m0, _ptr(ws.C), _ptr(ws.S), md, md * md, self.stream)
+        with self.prof("eigh"):
+            eig, u, ldu = self.eigh(m)
+        with self.prof("ritz_gemm"):
+            zgemm(_T, _N, nb, npw, m, u, ldu, m * ldu, ws.V, npw, md * npw, ws.X, npw, nb * npw, nk,
+                  stream=self.stream)
+            zgemm(_T, _N, nb, npw, m, u, ldu, m * ldu, ws.HV, npw, md * npw, ws.HX, npw, nb * npw, nk,
+                  stream=self.stream)
+        with self.prof("residual"):
+            self.residuals(eig)
         return eig
+
+    def eigh(self, m: int, S=None, lds=None):
+        """Lowest nb eigenpairs of the Hermitian matrices S[:, :m, :m]:
+        eigenvalues (nk, nb) and a row-major block U (nk, m, ldu) whose first nb
+        columns are the eigenvectors. The batched libgwb.so eigensolver runs
+        for m <= gwb_heev_max_dim(); larger subspaces use cuSOLVER (through
+        torch.linalg.eigh). A QL failure is flagged in ws.info and caught by the
+        next statistics read."""
+        ws, nk, nb = self.ws, self.nk, self.nb
+        S = ws.S if S is None else S
+        lds = self.max_dim if lds is None else lds
+        opcount.bump("eigh")
+        if m <= self.heev_max:
+            _lib.call("gwb_heev_lowest", nk, m, nb, _ptr(S), lds, S.shape[1] * S.shape[2], _ptr(ws.eig),
+                      _ptr(ws.U), _ptr(ws.Z), _ptr(ws.heev_info), self.stream)
+            return ws.eig[:, :nb], ws.U, nb
+        w, u = torch.linalg.eigh(S[:, :m, :m])
+        return w[:, :nb].contiguous(), u.contiguous(), m
 
     def residuals(self, eig):
         ws, nk, nb, npw = self.ws, self.nk, self.nb, self.npw
@@ -242,24 +304,27 @@ class _Solver:
         zgemm(_N, _H, nb, nb, npw, ws.X, npw, nb * npw, ws.HX, npw, nb * npw, ws.G, nb, nb * nb, nk,
               stream=self.stream)
         s = ws.G.conj()
-        s = 0.5 * (s + s.conj().transpose(-1, -2))
-        opcount.bump("eigh")
-        w, u = torch.linalg.eigh(s)
-        u = u.contiguous()
-        eig = w.contiguous()
-        zgemm(_T, _N, nb, npw, nb, u, nb, nb * nb, ws.X, npw, nb * npw, ws.D2, npw, nb * npw, nk,
+        ws.Gs.copy_(0.5 * (s + s.conj().transpose(-1, -2)))
+        eig, u, ldu = self.eigh(nb, ws.Gs, nb)
+        eig = eig.clone()
+        zgemm(_T, _N, nb, npw, nb, u, ldu, nb * ldu, ws.X, npw, nb * npw, ws.D2, npw, nb * npw, nk,
               stream=self.stream)
         ws.X.copy_(ws.D2)
-        zgemm(_T, _N, nb, npw, nb, u, nb, nb * nb, ws.HX, npw, nb * npw, ws.D2, npw, nb * npw, nk,
+        zgemm(_T, _N, nb, npw, nb, u, ldu, nb * ldu, ws.HX, npw, nb * npw, ws.D2, npw, nb * npw, nk,
               stream=self.stream)
         ws.HX.copy_(ws.D2)
         self.residuals(eig)
         return eig
 
     def read_stats(self):
+        """(max |r|, n_add) from the device in one small read; raises if the
+        eigensolver flagged a QL failure this round."""
         _lib.call("gwb_conv_stats", self.nk, self.nb, _ptr(self.ws.rn), self.tol, _ptr(self.ws.stats),
                   self.stream)
+        self.ws.stats[2] = self.ws.heev_info.max()
         st = self.ws.stats.tolist()
+        if st[2] != 0:
+            raise _lib.GwbError(_lib.GWB_ERR_NOT_CONVERGED, "subspace eigensolver: QL iteration limit")
         return st[0], int(st[1])
 
     # -- the solve --------------------------------------------------------------
@@ -277,13 +342,15 @@ class _Solver:
         for it in range(1, self.max_iter + 1):
             eig = self.rayleigh_ritz(m, m0)
             m0 = m
-            rnmax, n_add = self.read_stats()
+            with self.prof("stats_sync"):
+                rnmax, n_add = self.read_stats()
             if self.fp32_exp:
                 stalled = it > 1 and rnmax > _FP32_CERT_STALL * prev_rnmax
                 prev_rnmax = rnmax
                 if rnmax < max(self.tol, cert_floor) or stalled:
-                    eig = self.certify()
-                    rnmax, n_add = self.read_stats()
+                    with self.prof("certify"):
+                        eig = self.certify()
+                        rnmax, n_add = self.read_stats()
                     if rnmax >= self.tol:
                         # hand-off: collapse to the certified block with exact
                         # images and continue with float64 expansion applies
@@ -295,22 +362,27 @@ class _Solver:
                 self.history_out.append((it, ws.rn.cpu().clone(), eig.cpu().clone()))
             if rnmax < self.tol:
                 return self.result(eig, it)
-            _lib.call("gwb_select_worst", nk, nb, _ptr(ws.rn), n_add, _ptr(ws.sel), self.stream)
-            self.precondition(n_add, eig)
+            with self.prof("precond"):
+                _lib.call("gwb_select_worst", nk, nb, _ptr(ws.rn), n_add, _ptr(ws.sel), self.stream)
+                self.precondition(n_add, eig)
             if m + n_add > md:
                 # restart: re-orthonormalise the Ritz block, images by the same
                 # transform (no re-application), keep the new directions
                 self.n_restart += 1
-                if not self.cholqr2(ws.X, nb, ws.D2, ws.HX, ws.R):
+                with self.prof("restart"):
+                    restart_ok = self.cholqr2(ws.X, nb, ws.D2, ws.HX, ws.R)
+                if not restart_ok:
                     q, r = torch.linalg.qr(ws.X.transpose(-1, -2), mode="reduced")
                     ws.X.copy_(q.transpose(-1, -2))
                     ws.HX.copy_(torch.linalg.solve_triangular(r.transpose(-1, -2), ws.HX, upper=False))
                 ws.V[:, :nb].copy_(ws.X)
                 ws.HV[:, :nb].copy_(ws.HX)
                 m, m0 = nb, 0
-            self.orthonormalize_new(n_add, m)
-            ws.V[:, m:m + n_add].copy_(ws.D[:, :n_add])
-            self.apply_block(ws.V, m * npw, md * npw, n_add, ws.HV, m * npw, md * npw, low=self.fp32_exp)
+            with self.prof("orthonormalize"):
+                self.orthonormalize_new(n_add, m)
+                ws.V[:, m:m + n_add].copy_(ws.D[:, :n_add])
+            with self.prof("apply"):
+                self.apply_block(ws.V, m * npw, md * npw, n_add, ws.HV, m * npw, md * npw, low=self.fp32_exp)
             m += n_add
         if self.fp32_exp:
             eig = self.certify()
@@ -334,7 +406,7 @@ class _Solver:
         if self.out_dtype != torch.complex128:
             x = x.to(self.out_dtype)
         info = {"n_restart": self.n_restart, "n_cert": self.n_cert, "n_fallback_qr": self.n_fallback_qr,
-                "max_dim": self.max_dim}
+                "max_dim": self.max_dim, "phase_ms": self.prof.summary()}
         return BatchedDavidsonResult(eig.clone(), x, it, ws.rn.clone(), self.n_low, self.n_full, info)
 
 

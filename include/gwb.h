@@ -157,6 +157,16 @@ int gwb_subspace_insert(int32_t nk, int32_t m, int32_t m0, const void* C, void* 
 int gwb_chol_inv(int32_t nk, int32_t n, void* G, int32_t ldg, int64_t g_kstride, void* Linv,
                  int64_t linv_kstride, int32_t* info, void* stream);
 
+/* Lowest nb eigenpairs of nk Hermitian m x m matrices S (leading dim lds,
+ * both triangles filled), float64: eig (nk, nb) ascending, U (nk, m, nb)
+ * row-major eigenvector columns; zscratch (nk, m*m) float64; info[k] = 1 when
+ * the QL iteration limit was hit. m <= gwb_heev_max_dim(). Householder
+ * tridiagonalisation + implicit QL + back-transform, one CTA per matrix.
+ * Replaces torch.linalg.eigh in gradwave solvers/davidson.py:66-75,650. */
+int gwb_heev_lowest(int32_t nk, int32_t m, int32_t nb, const void* S, int32_t lds, int64_t s_kstride,
+                    double* eig, void* U, double* zscratch, int32_t* info, void* stream);
+int gwb_heev_max_dim(void);
+
 #ifdef __cplusplus
 }
 #endif
