@@ -76,6 +76,7 @@ _SIGNATURES = {
     "gwb_chol_inv": [_I, _I, _P, _I, _I64, _P, _I64, _P, _P],
     "gwb_heev_lowest": [_I, _I, _I, _P, _I, _I64, _P, _P, _P, _P, _P],
     "gwb_heev_max_dim": [],
+    "gwb_heev_lowest_noalloc": [_I, _I, _I, _P, _I, _I64, _P, _P, _P, _P],
 }
 _RESTYPES = {"gwb_last_error": ctypes.c_char_p, "gwb_version": ctypes.c_char_p,
              "gwb_launch_count": ctypes.c_ulonglong,

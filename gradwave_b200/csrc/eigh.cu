@@ -289,3 +289,75 @@ extern "C" int gwb_heev_lowest(int32_t nk, int32_t m, int32_t nb, const void* S,
 }
 
 extern "C" int gwb_heev_max_dim(void) { return GWB_HEEV_MMAX; }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of gwb_heev_lowest.
+//
+// Who needs it: a caller whose device memory is owned by a pool allocator - a
+// framework's caching allocator that holds most of HBM, or an application that
+// runs under a fixed device-memory budget - cannot call cudaMalloc itself: the
+// call fails when the pool already holds the memory, or escapes the budget the
+// pool accounts for. This entry point takes only the caller's inputs and
+// outputs and runs the eigenvector scratch Z in a fixed device array that is
+// part of the library image.
+//
+// Limits and sharing:
+//   * the array holds GWB_HEEV_NOALLOC_DOUBLES float64 (8 MiB); every GPU that
+//     loads libgwb.so holds it until the process exits;
+//   * a call needs nk * m * m float64 of it; larger problems are rejected with
+//     GWB_ERR_ARG (use gwb_heev_lowest with caller-provided scratch);
+//   * every call on a device uses the same array and leaves its last contents
+//     there; the kernel writes every element of Z it reads (identity fill), so
+//     nothing has to start at zero. Two calls whose kernels overlap on the GPU
+//     (different streams without ordering) race on the array: order them.
+//   * the first call on each device looks up the array's device address
+//     (cudaGetSymbolAddress with that device current); make that first call
+//     before any stream capture.
+#include <mutex>
+
+#define GWB_HEEV_NOALLOC_DOUBLES (1 << 20)
+#define GWB_NOALLOC_MAX_DEVICES 64
+
+static __device__ __align__(256) double g_heev_noalloc_z[GWB_HEEV_NOALLOC_DOUBLES];
+
+namespace gwb {
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_addr[GWB_NOALLOC_MAX_DEVICES] = {};
+}  // namespace gwb
+
+extern "C" int gwb_heev_lowest_noalloc(int32_t nk, int32_t m, int32_t nb, const void* S, int32_t lds,
+                                       int64_t s_kstride, double* eig, void* U, int32_t* info, void* stream) {
+  GWB_REQUIRE(nk > 0 && m > 0 && nb > 0 && nb <= m && lds >= m, "bad sizes");
+  GWB_REQUIRE(m <= GWB_HEEV_MMAX, "m exceeds the shared-memory eigensolver limit (112)");
+  GWB_REQUIRE(S && eig && U && info, "null pointer");
+  if ((int64_t)nk * m * m > (int64_t)GWB_HEEV_NOALLOC_DOUBLES) {
+    set_error("gwb_heev_lowest_noalloc: nk*m*m = " + std::to_string((int64_t)nk * m * m) +
+              " float64 of scratch exceeds the fixed " + std::to_string(GWB_HEEV_NOALLOC_DOUBLES) +
+              " (8 MiB); call gwb_heev_lowest with caller-provided scratch");
+    return GWB_ERR_ARG;
+  }
+  int dev = 0;
+  GWB_CUDA_TRY(cudaGetDevice(&dev));
+  GWB_REQUIRE(dev >= 0 && dev < GWB_NOALLOC_MAX_DEVICES, "device index beyond the supported 64");
+  double* z = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void* p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_heev_noalloc_z);
+      if (e != cudaSuccess || p == nullptr) {
+        set_error(std::string("cudaGetSymbolAddress(g_heev_noalloc_z): ") + cudaGetErrorString(e));
+        return GWB_ERR_CUDA;
+      }
+      g_noalloc_addr[dev] = static_cast<double*>(p);
+    }
+    z = g_noalloc_addr[dev];
+  }
+  const size_t sm = heev_smem(m);
+  GWB_CUDA_TRY(cudaFuncSetAttribute(k_heev_lowest, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  k_heev_lowest<<<nk, HEEV_THREADS, sm, (cudaStream_t)stream>>>((const cplx<double>*)S, lds, s_kstride, m, nb, eig,
+                                                                (cplx<double>*)U, z, info);
+  GWB_LAUNCH_CHECK();
+  count_launches(1);
+  return GWB_OK;
+}

@@ -167,6 +167,18 @@ int gwb_heev_lowest(int32_t nk, int32_t m, int32_t nb, const void* S, int32_t ld
                     double* eig, void* U, double* zscratch, int32_t* info, void* stream);
 int gwb_heev_max_dim(void);
 
+/* gwb_heev_lowest without any device allocation: the caller passes inputs and
+ * outputs only, and the eigenvector scratch lives in a fixed 8 MiB device
+ * array inside the library (held on every GPU that loads it). For callers
+ * whose device memory belongs to a pool allocator or a fixed budget and who
+ * therefore cannot call cudaMalloc. No counterpart in the reference.
+ * Limits: nk*m*m <= 1048576 (else GWB_ERR_ARG); calls share the array, so
+ * calls whose kernels may overlap on the GPU race and must be ordered; the
+ * first call on a device looks up the array's address and should come before
+ * any stream capture. */
+int gwb_heev_lowest_noalloc(int32_t nk, int32_t m, int32_t nb, const void* S, int32_t lds, int64_t s_kstride,
+                            double* eig, void* U, int32_t* info, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

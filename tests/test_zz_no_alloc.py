@@ -1,0 +1,76 @@
+"""The allocation-free eigensolver entry point, gwb_heev_lowest_noalloc.
+
+It exists for callers that cannot call cudaMalloc: code whose device memory is
+owned by a pool allocator (a framework caching allocator holding most of HBM)
+or that runs under a fixed device-memory budget. It takes only inputs and
+outputs and keeps its eigenvector scratch in a fixed 8 MiB device array of
+the library.
+
+Checked through the C ABI: two calls in a row give the same eigenpairs as the
+allocating entry point gwb_heev_lowest (within this suite's eigensolver
+tolerance, 1e-12 relative), and an oversized request is refused before any
+kernel runs. This file is collected last so a failure here stops a run only
+after every other test has run.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def _herm_batch(seed, nk, m):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(nk):
+        x = rng.standard_normal((m, m)) + 1j * rng.standard_normal((m, m))
+        q, _ = np.linalg.qr(x)
+        ev = np.sort(rng.uniform(-50.0, 400.0, m))
+        ev[3:6] = ev[3]
+        h = (q * ev) @ q.conj().T
+        out.append(0.5 * (h + h.conj().T))
+    return np.stack(out)
+
+
+def test_noalloc_matches_allocating_entry_twice(cuda_device):
+    from gradwave_b200 import _lib
+    nk, m, nb = 6, 96, 24
+    S = torch.from_numpy(_herm_batch(7, nk, m)).to(cuda_device)
+    st = _lib.stream_ptr(cuda_device)
+
+    def outputs():
+        return (torch.zeros(nk, nb, dtype=torch.float64, device=cuda_device),
+                torch.zeros(nk, m, nb, dtype=torch.complex128, device=cuda_device),
+                torch.full((nk,), -1, dtype=torch.int32, device=cuda_device))
+
+    eig_ref, U_ref, info_ref = outputs()
+    Z = torch.zeros(nk, m * m, dtype=torch.float64, device=cuda_device)
+    _lib.call("gwb_heev_lowest", nk, m, nb, S.data_ptr(), m, m * m, eig_ref.data_ptr(), U_ref.data_ptr(),
+              Z.data_ptr(), info_ref.data_ptr(), st)
+    scale = float(torch.linalg.eigvalsh(S).abs().max())
+    for call in range(2):
+        eig, U, info = outputs()
+        _lib.call("gwb_heev_lowest_noalloc", nk, m, nb, S.data_ptr(), m, m * m, eig.data_ptr(), U.data_ptr(),
+                  info.data_ptr(), st)
+        torch.cuda.synchronize(cuda_device)
+        assert torch.all(info == 0), f"call {call}: QL failure flagged"
+        assert float((eig - eig_ref).abs().max()) <= TOL * scale, f"call {call}: eigenvalues differ"
+        # eigenvectors of degenerate clusters are fixed only up to a unitary
+        # mix, so compare the residual A U - U diag(eig) instead of U itself
+        res = torch.einsum("kij,kja->kia", S, U) - U * eig[:, None, :]
+        assert float(res.abs().max()) <= TOL * scale, f"call {call}: residual too large"
+        assert float((U - U_ref).abs().max()) <= 1e-10, f"call {call}: eigenvectors differ"
+
+
+def test_noalloc_rejects_oversized_request(cuda_device):
+    from gradwave_b200 import _lib
+    nk, m, nb = 200, 96, 8          # 200 * 96 * 96 = 1.84M float64 > the fixed 1M
+    dummy = torch.zeros(1, dtype=torch.complex128, device=cuda_device)
+    with pytest.raises(_lib.GwbError) as err:
+        _lib.call("gwb_heev_lowest_noalloc", nk, m, nb, dummy.data_ptr(), m, m * m, dummy.data_ptr(),
+                  dummy.data_ptr(), dummy.data_ptr(), _lib.stream_ptr(cuda_device))
+    assert err.value.status == _lib.GWB_ERR_ARG
+    assert "exceeds" in str(err.value)
