@@ -73,7 +73,8 @@ _SIGNATURES = {
     "gwb_select_worst": [_I, _I, _P, _I, _P, _P],
     "gwb_precond_teter": [_I, _I, _I, _I, _P, _I64, _P, _I64, _P, _P, _P, _I64, _P],
     "gwb_subspace_insert": [_I, _I, _I, _P, _P, _I, _I64, _P],
-    "gwb_chol_inv": [_I, _I, _P, _I, _I64, _P, _I64, _P, _P],
+    "gwb_chol_inv": [_I, _I, _P, _I, _I64, _P, _I64, _P, _P, _P],
+    "gwb_row_repair": [_I, _I, _I, _P, _I64, _P, _D, _P, _P],
     "gwb_heev_lowest": [_I, _I, _I, _P, _I, _I64, _P, _P, _P, _P, _P],
     "gwb_heev_max_dim": [],
     "gwb_heev_lowest_noalloc": [_I, _I, _I, _P, _I, _I64, _P, _P, _P, _P],

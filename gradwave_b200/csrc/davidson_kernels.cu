@@ -175,7 +175,7 @@ __global__ void k_subspace_insert(const cplx<double>* __restrict__ C, int m, int
 // is not positive (or not finite): Linv is then not written.
 __global__ void __launch_bounds__(256) k_chol_inv(cplx<double>* __restrict__ G, int n, int ld, int64_t gk,
                                                   cplx<double>* __restrict__ Linv, int64_t lk,
-                                                  int* __restrict__ info) {
+                                                  int* __restrict__ info, int* __restrict__ flag) {
   __shared__ double red[8];
   __shared__ int bad;
   const int k = blockIdx.x;
@@ -204,7 +204,10 @@ __global__ void __launch_bounds__(256) k_chol_inv(cplx<double>* __restrict__ G, 
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) info[k] = bad;
+  if (threadIdx.x == 0) {
+    info[k] = bad;
+    if (bad && flag) atomicOr(flag, 2);
+  }
   if (bad) return;
   // Linv column jc by forward substitution (one thread per column)
   for (int jc = threadIdx.x; jc < n; jc += blockDim.x) {
@@ -215,6 +218,39 @@ __global__ void __launch_bounds__(256) k_chol_inv(cplx<double>* __restrict__ G, 
       for (int q = jc; q < i; ++q) acc = acc + A[(int64_t)i * ld + q] * Li[(int64_t)q * n + jc];
       Li[(int64_t)i * n + jc] = scale(acc, -1.0 / A[(int64_t)i * ld + i].x);
     }
+  }
+}
+
+// Deterministic pseudo-random value in [-1, 1) from an integer key
+// (SplitMix64 finaliser, Steele, Lea & Flood, OOPSLA 2014).
+__device__ __forceinline__ double hash_unit(unsigned long long x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  x ^= x >> 31;
+  return (double)(x >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+// Rank repair of the expansion block (the reference's jitter for rows that
+// vanish after projection, gradwave solvers/davidson.py:450-456): a row whose
+// norm is below thresh is replaced by masked deterministic noise and flag
+// gets bit 0. One CTA per (k, row).
+__global__ void __launch_bounds__(256) k_row_repair(int npw, int n, cplx<double>* __restrict__ D, int64_t dk,
+                                                    const unsigned char* __restrict__ mask, double thresh,
+                                                    int* __restrict__ flag) {
+  __shared__ double red[8];
+  const int k = blockIdx.x / n, s = blockIdx.x % n;
+  cplx<double>* row = D + k * dk + (int64_t)s * npw;
+  double nn = 0.0;
+  for (int g = threadIdx.x; g < npw; g += blockDim.x) nn += norm2(row[g]);
+  nn = block_sum<256>(nn, red);
+  if (sqrt(nn) < thresh) {
+    const unsigned long long base = ((unsigned long long)k * 4099ull + (unsigned long long)s) * 1000003ull;
+    for (int g = threadIdx.x; g < npw; g += blockDim.x) {
+      const unsigned long long key = (base + (unsigned long long)g) * 2ull;
+      row[g] = mask[(int64_t)k * npw + g] ? mk<double>(hash_unit(key), hash_unit(key + 1)) : mk<double>(0.0, 0.0);
+    }
+    if (threadIdx.x == 0) atomicOr(flag, 1);
   }
 }
 
@@ -282,11 +318,21 @@ int gwb_subspace_insert(int32_t nk, int32_t m, int32_t m0, const void* C, void* 
 }
 
 int gwb_chol_inv(int32_t nk, int32_t n, void* G, int32_t ldg, int64_t g_kstride, void* Linv,
-                 int64_t linv_kstride, int32_t* info, void* stream) {
+                 int64_t linv_kstride, int32_t* info, int32_t* flag, void* stream) {
   GWB_REQUIRE(nk > 0 && n > 0 && ldg >= n, "bad sizes");
   GWB_REQUIRE(G && Linv && info, "null pointer");
   k_chol_inv<<<nk, 256, 0, (cudaStream_t)stream>>>((cplx<double>*)G, n, ldg, g_kstride, (cplx<double>*)Linv,
-                                                  linv_kstride, info);
+                                                  linv_kstride, info, flag);
+  GWB_LAUNCH_CHECK();
+  count_launches(1);
+  return GWB_OK;
+}
+
+int gwb_row_repair(int32_t nk, int32_t n, int32_t npw, void* D, int64_t d_kstride, const uint8_t* mask,
+                   double thresh, int32_t* flag, void* stream) {
+  GWB_REQUIRE(nk > 0 && n > 0 && npw > 0, "bad sizes");
+  GWB_REQUIRE(D && mask && flag, "null pointer");
+  k_row_repair<<<nk * n, 256, 0, (cudaStream_t)stream>>>(npw, n, (cplx<double>*)D, d_kstride, mask, thresh, flag);
   GWB_LAUNCH_CHECK();
   count_launches(1);
   return GWB_OK;

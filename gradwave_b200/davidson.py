@@ -126,7 +126,8 @@ class _Workspace:
         self.G = torch.zeros(nk, nb, nb, **c)
         self.Linv = torch.zeros(nk, nb, nb, **c)
         self.rn = torch.zeros(nk, nb, dtype=torch.float64, device=dev)
-        self.stats = torch.zeros(3, dtype=torch.float64, device=dev)
+        self.stats = torch.zeros(4, dtype=torch.float64, device=dev)
+        self.flags = torch.zeros(1, dtype=torch.int32, device=dev)
         self.sel = torch.zeros(nk, nb, dtype=torch.int32, device=dev)
         self.info = torch.zeros(nk, dtype=torch.int32, device=dev)
         self.heev_info = torch.zeros(nk, dtype=torch.int32, device=dev)
@@ -169,6 +170,10 @@ class _Solver:
         self.n_restart = 0
         self.n_cert = 0
         self.n_fallback_qr = 0
+        self.n_repair = 0
+        self.n_rollback = 0
+        self.breakdown = False
+        self.mask_u8 = self.mask.to(torch.uint8).contiguous()
         self.stream = _lib.stream_ptr(self.dev)
         self.x0 = x0
         self.prof = _PhaseTimer(os.environ.get("GWB_PROFILE", "0") == "1")
@@ -197,17 +202,19 @@ class _Solver:
         dview.copy_(out)
 
     def cholqr2(self, Y: torch.Tensor, n: int, Ytmp: torch.Tensor, Z: torch.Tensor | None = None,
-                Ztmp: torch.Tensor | None = None):
+                Ztmp: torch.Tensor | None = None, sync: bool = True):
         """Orthonormalise the first n rows of Y (nk, >=n, npw) in place by two
         rounds of float64 Gram -> Cholesky -> L^-1 (Z, if given, gets the same
-        row transform). Returns False on a Cholesky breakdown (Y untouched)."""
+        row transform). With sync, a Cholesky breakdown is checked on the host
+        and reported as False (Y untouched by the failing round); without, it
+        only sets bit 1 of ws.flags, read with the next round's statistics."""
         ws, nk, npw = self.ws, self.nk, self.npw
         ys, zs = Y.shape[1] * npw, None if Z is None else Z.shape[1] * npw
         for _ in range(2):
             zgemm(_N, _H, n, n, npw, Y, npw, ys, Y, npw, ys, ws.G, n, n * n, nk, stream=self.stream)
             _lib.call("gwb_chol_inv", nk, n, _ptr(ws.G), n, n * n, _ptr(ws.Linv), n * n, _ptr(ws.info),
-                      self.stream)
-            if int(ws.info.max()) != 0:
+                      None if sync else _ptr(ws.flags), self.stream)
+            if sync and int(ws.info.max()) != 0:
                 return False
             zgemm(_N, _N, n, npw, n, ws.Linv, n, n * n, Y, npw, ys, Ytmp, npw, Ytmp.shape[1] * npw, nk,
                   stream=self.stream)
@@ -218,28 +225,41 @@ class _Solver:
                 Z[:, :n].copy_(Ztmp[:, :n])
         return True
 
-    def project_out(self, Dblk: torch.Tensor, n: int, m: int):
-        """D -= (D V^H) V twice over the first m basis rows (float64 GEMMs)."""
+    def project_out(self, Dblk: torch.Tensor, n: int, m: int, passes: int = 2):
+        """D -= (D V^H) V over the first m basis rows (float64 GEMMs)."""
         ws, nk, npw, md = self.ws, self.nk, self.npw, self.max_dim
         ds = Dblk.shape[1] * npw
-        for _ in range(2):
+        for _ in range(passes):
             zgemm(_N, _H, n, m, npw, Dblk, npw, ds, ws.V, npw, md * npw, ws.C, m, n * m, nk,
                   stream=self.stream)
             zgemm(_N, _N, n, npw, m, ws.C, m, n * m, ws.V, npw, md * npw, Dblk, npw, ds, nk, alpha=-1.0,
                   beta=1.0, stream=self.stream)
 
-    def orthonormalize_new(self, n: int, m: int):
+    def orthonormalize_new(self, n: int, m: int, safe: bool = False):
         """Rows D[:, :n] -> orthonormal, orthogonal to V[:, :m] (reference
-        ``_orthonormalize_b``, gradwave solvers/davidson.py:406-457)."""
+        ``_orthonormalize_b``, gradwave solvers/davidson.py:406-457).
+
+        Default (no host synchronisation): projection, device rank repair of
+        vanished rows, second projection, CholQR2; a breakdown is only flagged
+        and the caller rolls the expansion back. ``safe``: the reference's
+        order with host checks - two projections, seeded jitter of vanished
+        rows, re-projection, CholQR2 with Householder QR on breakdown."""
         ws = self.ws
         D = ws.D
         D[:, :n].mul_(self.mask[:, None, :])
+        if not safe:
+            if m:
+                self.project_out(D, n, m, passes=1)
+            _lib.call("gwb_row_repair", self.nk, n, self.npw, _ptr(D), D.shape[1] * self.npw,
+                      _ptr(self.mask_u8), 1e-8, _ptr(ws.flags), self.stream)
+            if m:
+                self.project_out(D, n, m, passes=1)
+            self.cholqr2(D, n, ws.D2, sync=False)
+            return
         if m:
             self.project_out(D, n, m)
         if self.cholqr2(D, n, ws.D2):
             return
-        # breakdown: the reference's rank repair - seeded jitter on (near-)zero
-        # rows, re-projection, Householder QR
         self.n_fallback_qr += 1
         blk = D[:, :n]
         bad = torch.linalg.vector_norm(blk, dim=-1, keepdim=True) < 1e-8
@@ -257,10 +277,11 @@ class _Solver:
         """Update s (new columns m0..m-1), eigensolve, Ritz block X/HX, residuals."""
         ws, nk, npw, nb, md = self.ws, self.nk, self.npw, self.nb, self.max_dim
         nnew = m - m0
-        with self.prof("subspace_gemm"):
-            zgemm(_N, _H, m, nnew, npw, ws.V, npw, md * npw, ws.HV, npw, md * npw, ws.C, nnew, m * nnew, nk,
-                  b_off=m0 * npw, stream=self.stream)
-            _lib.call("gwb_subspace_insert", nk, m, m0, _ptr(ws.C), _ptr(ws.S), md, md * md, self.stream)
+        if nnew > 0:
+            with self.prof("subspace_gemm"):
+                zgemm(_N, _H, m, nnew, npw, ws.V, npw, md * npw, ws.HV, npw, md * npw, ws.C, nnew, m * nnew, nk,
+                      b_off=m0 * npw, stream=self.stream)
+                _lib.call("gwb_subspace_insert", nk, m, m0, _ptr(ws.C), _ptr(ws.S), md, md * md, self.stream)
         with self.prof("eigh"):
             eig, u, ldu = self.eigh(m)
         with self.prof("ritz_gemm"):
@@ -321,29 +342,48 @@ class _Solver:
         eigensolver flagged a QL failure this round."""
         _lib.call("gwb_conv_stats", self.nk, self.nb, _ptr(self.ws.rn), self.tol, _ptr(self.ws.stats),
                   self.stream)
-        self.ws.stats[2] = self.ws.heev_info.max()
-        st = self.ws.stats.tolist()
+        ws = self.ws
+        ws.stats[2] = ws.heev_info.max()
+        ws.stats[3] = ws.flags[0]
+        ws.flags.zero_()
+        st = ws.stats.tolist()
         if st[2] != 0:
             raise _lib.GwbError(_lib.GWB_ERR_NOT_CONVERGED, "subspace eigensolver: QL iteration limit")
+        flags = int(st[3])
+        if flags & 1:
+            self.n_repair += 1
+        self.breakdown = bool(flags & 2)
         return st[0], int(st[1])
 
     # -- the solve --------------------------------------------------------------
     def run(self) -> BatchedDavidsonResult:
         ws, nk, nb, npw, md = self.ws, self.nk, self.nb, self.npw, self.max_dim
         ws.D[:, :nb].copy_(self.x0.to(torch.complex128))
-        self.orthonormalize_new(nb, 0)
+        self.orthonormalize_new(nb, 0, safe=True)
         ws.V[:, :nb].copy_(ws.D[:, :nb])
         self.apply_block(ws.V, 0, md * npw, nb, ws.HV, 0, md * npw, low=self.fp32_exp)
         # m: basis rows in use; m0: first column of s not formed yet (0 = rebuild)
         m, m0 = nb, 0
+        m_prev = m
+        safe_next = False
         cert_floor = _FP32_CERT_FLOOR_EPS * max(float(self.t.max()), 1.0) if self.fp32_exp else 0.0
         prev_rnmax = math.inf
         eig = None
-        for it in range(1, self.max_iter + 1):
+        it = 0
+        while it < self.max_iter:
+            it += 1
             eig = self.rayleigh_ritz(m, m0)
             m0 = m
             with self.prof("stats_sync"):
                 rnmax, n_add = self.read_stats()
+            if self.breakdown:
+                # the last expansion block lost rank in CholQR2: drop it, redo
+                # this round on the previous basis, orthonormalise safely
+                self.n_rollback += 1
+                m = m0 = m_prev
+                safe_next = True
+                it -= 1
+                continue
             if self.fp32_exp:
                 stalled = it > 1 and rnmax > _FP32_CERT_STALL * prev_rnmax
                 prev_rnmax = rnmax
@@ -379,10 +419,12 @@ class _Solver:
                 ws.HV[:, :nb].copy_(ws.HX)
                 m, m0 = nb, 0
             with self.prof("orthonormalize"):
-                self.orthonormalize_new(n_add, m)
+                self.orthonormalize_new(n_add, m, safe=safe_next)
+                safe_next = False
                 ws.V[:, m:m + n_add].copy_(ws.D[:, :n_add])
             with self.prof("apply"):
                 self.apply_block(ws.V, m * npw, md * npw, n_add, ws.HV, m * npw, md * npw, low=self.fp32_exp)
+            m_prev = m
             m += n_add
         if self.fp32_exp:
             eig = self.certify()
@@ -406,6 +448,7 @@ class _Solver:
         if self.out_dtype != torch.complex128:
             x = x.to(self.out_dtype)
         info = {"n_restart": self.n_restart, "n_cert": self.n_cert, "n_fallback_qr": self.n_fallback_qr,
+                "n_repair": self.n_repair, "n_rollback": self.n_rollback,
                 "max_dim": self.max_dim, "phase_ms": self.prof.summary()}
         return BatchedDavidsonResult(eig.clone(), x, it, ws.rn.clone(), self.n_low, self.n_full, info)
 

@@ -153,9 +153,17 @@ int gwb_subspace_insert(int32_t nk, int32_t m, int32_t m0, const void* C, void* 
 
 /* Per k: G (n x n, leading dim ldg) -> lower Cholesky factor in place and
  * Linv = L^-1 (n x n, leading dim n); info[k] = 0 or j+1 at a non-positive
- * pivot j. CholQR step of gradwave solvers/davidson.py:195-222. */
+ * pivot j, and bit 1 of *flag is set on any breakdown (flag may be NULL).
+ * CholQR step of gradwave solvers/davidson.py:195-222. */
 int gwb_chol_inv(int32_t nk, int32_t n, void* G, int32_t ldg, int64_t g_kstride, void* Linv,
-                 int64_t linv_kstride, int32_t* info, void* stream);
+                 int64_t linv_kstride, int32_t* info, int32_t* flag, void* stream);
+
+/* Rank repair: rows of D (nk blocks of n rows, d_kstride apart) with norm
+ * below thresh are replaced by deterministic noise on the mask (uint8
+ * (nk, npw)); bit 0 of *flag is set if any row was repaired. Replaces the
+ * jitter of gradwave solvers/davidson.py:450-456. */
+int gwb_row_repair(int32_t nk, int32_t n, int32_t npw, void* D, int64_t d_kstride, const uint8_t* mask,
+                   double thresh, int32_t* flag, void* stream);
 
 /* Lowest nb eigenpairs of nk Hermitian m x m matrices S (leading dim lds,
  * both triangles filled), float64: eig (nk, nb) ascending, U (nk, m, nb)

@@ -42,7 +42,7 @@ def _random_herm(rng, m, degenerate=True):
     return 0.5 * (h + h.conj().T)
 
 
-@pytest.mark.parametrize("m,nb", [(1, 1), (2, 2), (3, 2), (24, 24), (96, 24), (112, 40)])
+@pytest.mark.parametrize("m,nb", [(1, 1), (2, 2), (3, 2), (13, 5), (24, 24), (57, 20), (96, 24), (97, 24), (112, 40)])
 def test_heev_matches_lapack(cuda_device, m, nb):
     from gradwave_b200 import _lib
     assert m <= _lib.load().gwb_heev_max_dim()
