@@ -392,6 +392,33 @@ def _cpu_baseline(args, ci):
                       f"time scaled by {nk}/{len(ks)}"}
 
 
+def run_apply(args):
+    """Apply-only loop (for profiling the Hamiltonian kernels under ncu): K
+    applies of the full band block of the workload, float32 or float64."""
+    import torch
+    from gradwave_b200.cells import make_cell
+    from gradwave_b200.hamiltonian import BatchedHamiltonian
+    dev = torch.device("cuda", 0)
+    ci = make_cell(args.config)
+    h = BatchedHamiltonian(ci.bk.to(dev), ci.shape, ci.v_eff_r, ci.p)
+    g = torch.Generator().manual_seed(1)
+    c = torch.randn(ci.bk.nk, ci.nbands, ci.bk.npw_max, dtype=torch.complex128, generator=g)
+    c = (c * ci.bk.mask[:, None, :]).to(dev)
+    fn = h.apply_fp32 if args.prec == "fp32" else h.apply
+    for _ in range(args.warmup):
+        fn(c)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        fn(c)
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"mode": "apply", "config": args.config, "prec": args.prec, "nk": ci.bk.nk,
+                      "nbands": ci.nbands, "ms_per_apply": e0.elapsed_time(e1) / args.steps}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -401,7 +428,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--mode", default="solve", choices=["solve", "apply"],
+                    help="apply: only time Hamiltonian applies (profiling)")
+    ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64"], help="arithmetic of --mode apply")
     args = ap.parse_args()
+    if args.mode == "apply":
+        return run_apply(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

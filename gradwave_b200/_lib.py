@@ -45,6 +45,20 @@ class Geometry(ctypes.Structure):
                 ("flat_idx", ctypes.POINTER(ctypes.c_int64))]
 
 
+class DavidsonParams(ctypes.Structure):
+    _fields_ = [("nk", ctypes.c_int32), ("nb", ctypes.c_int32), ("npw", ctypes.c_int32),
+                ("max_dim", ctypes.c_int32), ("max_iter", ctypes.c_int32), ("mode", ctypes.c_int32),
+                ("precond", ctypes.c_int32), ("reserved", ctypes.c_int32), ("tol", ctypes.c_double),
+                ("t_max", ctypes.c_double)]
+
+
+class DavidsonStats(ctypes.Structure):
+    _fields_ = [("n_iter", ctypes.c_int32), ("hit_max_iter", ctypes.c_int32), ("n_restart", ctypes.c_int32),
+                ("n_cert", ctypes.c_int32), ("n_repair", ctypes.c_int32), ("n_rollback", ctypes.c_int32),
+                ("n_apply_low", ctypes.c_int64), ("n_apply_full", ctypes.c_int64),
+                ("max_residual", ctypes.c_double)]
+
+
 _lock = threading.Lock()
 _lib = None
 
@@ -78,6 +92,9 @@ _SIGNATURES = {
     "gwb_heev_lowest": [_I, _I, _I, _P, _I, _I64, _P, _P, _P, _P, _P],
     "gwb_heev_max_dim": [],
     "gwb_heev_lowest_noalloc": [_I, _I, _I, _P, _I, _I64, _P, _P, _P, _P],
+    "gwb_davidson_workspace_bytes": [ctypes.POINTER(DavidsonParams), ctypes.POINTER(ctypes.c_size_t)],
+    "gwb_davidson_solve": [_P, ctypes.POINTER(DavidsonParams), _P, _P, _P, _P, _P, ctypes.c_size_t, _P, _P, _P,
+                           ctypes.POINTER(DavidsonStats), _P],
 }
 _RESTYPES = {"gwb_last_error": ctypes.c_char_p, "gwb_version": ctypes.c_char_p,
              "gwb_launch_count": ctypes.c_ulonglong,

@@ -221,6 +221,74 @@ __global__ void __launch_bounds__(256) k_chol_inv(cplx<double>* __restrict__ G, 
   }
 }
 
+// Shared-memory version for n <= CHOL_SMEM_MAX: the same column-by-column
+// Cholesky and forward substitution, with L and L^-1 kept on chip (the global
+// version is bound by L2 latency on these tiny dependent loops). The inverse
+// runs row by row: row i of L^-1 needs rows < i only, all columns in parallel.
+constexpr int CHOL_SMEM_MAX = 64;
+__global__ void __launch_bounds__(256) k_chol_inv_smem(cplx<double>* __restrict__ G, int n, int ld, int64_t gk,
+                                                       cplx<double>* __restrict__ Linv, int64_t lk,
+                                                       int* __restrict__ info, int* __restrict__ flag) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<double>* A = reinterpret_cast<cplx<double>*>(smem_raw);  // n*n
+  cplx<double>* Li = A + n * n;                                 // n*n
+  __shared__ double red[8];
+  __shared__ int bad;
+  const int k = blockIdx.x;
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) A[i] = G[k * gk + (int64_t)(i / n) * ld + (i % n)];
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    double s = 0.0;
+    for (int q = threadIdx.x; q < j; q += blockDim.x) s += norm2(A[j * n + q]);
+    s = block_sum<256>(s, red);
+    const double dj = A[j * n + j].x - s;
+    if (!(dj > 0.0) || !isfinite(dj)) {
+      if (threadIdx.x == 0) bad = j + 1;
+      __syncthreads();
+      break;
+    }
+    const double ljj = sqrt(dj), inv = 1.0 / ljj;
+    for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) {
+      cplx<double> acc = A[i * n + j];
+      for (int q = 0; q < j; ++q) acc = acc - mul_conj(A[i * n + q], A[j * n + q]);
+      A[i * n + j] = scale(acc, inv);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) A[j * n + j] = mk<double>(ljj, 0.0);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    info[k] = bad;
+    if (bad && flag) atomicOr(flag, 2);
+  }
+  if (bad) return;
+  for (int i = 0; i < n; ++i) {
+    const double dinv = 1.0 / A[i * n + i].x;
+    for (int jc = threadIdx.x; jc < n; jc += blockDim.x) {
+      cplx<double> v;
+      if (jc > i) {
+        v = mk<double>(0.0, 0.0);
+      } else if (jc == i) {
+        v = mk<double>(dinv, 0.0);
+      } else {
+        cplx<double> acc = mk<double>(0.0, 0.0);
+        for (int q = jc; q < i; ++q) acc = acc + A[i * n + q] * Li[q * n + jc];
+        v = scale(acc, -dinv);
+      }
+      Li[i * n + jc] = v;
+    }
+    __syncthreads();
+  }
+  cplx<double>* Lo = Linv + k * lk;
+  cplx<double>* Gw = G + k * gk;
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) {
+    Lo[i] = Li[i];
+    const int r = i / n, c = i % n;
+    if (c <= r) Gw[(int64_t)r * ld + c] = A[i];  // the factor in place, as the global version
+  }
+}
+
 // Deterministic pseudo-random value in [-1, 1) from an integer key
 // (SplitMix64 finaliser, Steele, Lea & Flood, OOPSLA 2014).
 __device__ __forceinline__ double hash_unit(unsigned long long x) {
@@ -321,8 +389,15 @@ int gwb_chol_inv(int32_t nk, int32_t n, void* G, int32_t ldg, int64_t g_kstride,
                  int64_t linv_kstride, int32_t* info, int32_t* flag, void* stream) {
   GWB_REQUIRE(nk > 0 && n > 0 && ldg >= n, "bad sizes");
   GWB_REQUIRE(G && Linv && info, "null pointer");
-  k_chol_inv<<<nk, 256, 0, (cudaStream_t)stream>>>((cplx<double>*)G, n, ldg, g_kstride, (cplx<double>*)Linv,
-                                                  linv_kstride, info, flag);
+  if (n <= CHOL_SMEM_MAX) {
+    const size_t sm = (size_t)2 * n * n * sizeof(cplx<double>);
+    GWB_CUDA_TRY(cudaFuncSetAttribute(k_chol_inv_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_chol_inv_smem<<<nk, 256, sm, (cudaStream_t)stream>>>((cplx<double>*)G, n, ldg, g_kstride,
+                                                          (cplx<double>*)Linv, linv_kstride, info, flag);
+  } else {
+    k_chol_inv<<<nk, 256, 0, (cudaStream_t)stream>>>((cplx<double>*)G, n, ldg, g_kstride, (cplx<double>*)Linv,
+                                                    linv_kstride, info, flag);
+  }
   GWB_LAUNCH_CHECK();
   count_launches(1);
   return GWB_OK;

@@ -363,10 +363,13 @@ static size_t pencil_smem(const FftGeom& g, size_t es) {
   return (size_t)(g.n[0] * g.n[2] + g.n[0]) * es;
 }
 
-static int nl_slices(const gwb_ham* h) {
-  // enough CTAs for the machine at small nb, bounded partial storage
-  int s = (h->npw_max + 2047) / 2048;
-  return std::max(1, std::min(s, 16));
+// G slices of the becp reduction: enough CTAs to fill the GPU (4 per SM)
+// with every slice at least 256 plane waves long.
+static int nl_slices(const gwb_ham* h, int nb) {
+  const int tiles = ((h->nproj + NL_TP - 1) / NL_TP) * ((nb + NL_TB - 1) / NL_TB) * h->nk;
+  const int want = (4 * 148 + tiles - 1) / tiles;
+  const int cap = std::max(1, h->npw_max / 256);
+  return std::max(1, std::min(want, cap));
 }
 
 // Compile-time FFT plans instantiated for the cubic boxes of the workloads
@@ -409,8 +412,11 @@ static int apply_impl(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t ok
   const size_t es = sizeof(cplx<T>);
   const size_t plane_elems = (size_t)g.n[1] * g.n[2];
   const size_t per_band = (size_t)h->nk * g.L[0] * plane_elems * es;
-  size_t budget = std::max(w_budget_bytes(), per_band);
-  int nbc = (int)std::min<size_t>((size_t)nb, budget / per_band);
+  // balanced chunks: as few as the L2 budget allows, all of (nearly) equal size
+  const size_t budget = std::max(w_budget_bytes(), per_band);
+  const size_t max_nbc = std::max<size_t>(1, budget / per_band);
+  const size_t nchunks = ((size_t)nb + max_nbc - 1) / max_nbc;
+  int nbc = (int)(((size_t)nb + nchunks - 1) / nchunks);
   if (nbc < 1) nbc = 1;
   int rc = ensure_buf(&h->d_W, &h->W_bytes, per_band * nbc);
   if (rc) return rc;
@@ -426,7 +432,7 @@ static int apply_impl(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t ok
   else rcl = local_chunks<T, SIO, 0u>(h, c, ck, out, ok, nb, nbc, st, smA, smB);
   if (rcl) return rcl;
   if (h->nproj > 0) {
-    const int ns = nl_slices(h);
+    const int ns = nl_slices(h, nb);
     const int gslice = ((h->npw_max + ns - 1) / ns + NL_TG - 1) / NL_TG * NL_TG;
     const int nsl = (h->npw_max + gslice - 1) / gslice;
     rc = ensure_buf(&h->d_part, &h->part_bytes, (size_t)nsl * h->nk * nb * h->nproj * es);

@@ -453,11 +453,93 @@ class _Solver:
         return BatchedDavidsonResult(eig.clone(), x, it, ws.rn.clone(), self.n_low, self.n_full, info)
 
 
+def _native_solve(ham, x0, t, mask, tol, max_iter, max_dim, mode) -> BatchedDavidsonResult | None:
+    """The whole solve inside libgwb.so (``gwb_davidson_solve``); None when the
+    library reports a breakdown it does not repair (the host driver retries)."""
+    import ctypes
+    nk, nb, npw = (int(s) for s in x0.shape)
+    dev = x0.device
+    p = _lib.DavidsonParams(nk, nb, npw, max_dim, int(max_iter), 1 if mode == "fp32exp" else 0, 0, 0,
+                            float(tol), float(t.max()))
+    nbytes = ctypes.c_size_t()
+    _lib.call("gwb_davidson_workspace_bytes", ctypes.byref(p), ctypes.byref(nbytes))
+    ws = ham._native_workspace(int(nbytes.value))
+    x0c = x0.contiguous()
+    tc = t.to(dev, torch.float64).contiguous()
+    mk = mask.to(dev, torch.uint8).contiguous()
+    eig = torch.empty(nk, nb, dtype=torch.float64, device=dev)
+    vec = torch.empty(nk, nb, npw, dtype=torch.complex128, device=dev)
+    rn = torch.empty(nk, nb, dtype=torch.float64, device=dev)
+    st = _lib.DavidsonStats()
+    status = _lib.load().gwb_davidson_solve(ham._h, ctypes.byref(p), None, x0c.data_ptr(), tc.data_ptr(),
+                                            mk.data_ptr(), ws.data_ptr(), ws.numel(), eig.data_ptr(),
+                                            vec.data_ptr(), rn.data_ptr(), ctypes.byref(st), _lib.stream_ptr(dev))
+    if status == _lib.GWB_ERR_BREAKDOWN:
+        logger.debug("native Davidson: %s; retrying on the host driver", _lib.load().gwb_last_error().decode())
+        return None
+    _lib.check(status)
+    n_rows = st.n_apply_low + st.n_apply_full
+    ham._count_rows(n_rows)
+    info = {"n_restart": st.n_restart, "n_cert": st.n_cert, "n_repair": st.n_repair, "n_rollback": st.n_rollback,
+            "max_dim": max_dim, "native": True}
+    return BatchedDavidsonResult(eig, vec, int(st.n_iter), rn, int(st.n_apply_low), int(st.n_apply_full), info)
+
+
 def davidson_batched(h_apply, x0, t, mask, tol: float = 1e-9, max_iter: int = 40, max_dim_factor: int = 4,
                      sync_free: bool = False, history_out=None, *, mode: str = "fp64",
                      precond="teter") -> BatchedDavidsonResult:
-    """Batched block Davidson (see module docstring). ``sync_free`` is
-    accepted for signature parity and ignored (every round reads two device
-    scalars, like the reference's synchronous path)."""
+    """Batched block Davidson (see module docstring).
+
+    When ``h_apply`` is ``BatchedHamiltonian.apply`` of this package, the
+    block is complex128, the preconditioner is TPA, no history is requested and
+    the basis fits the batched eigensolver, the whole solve runs natively in
+    libgwb.so (``gwb_davidson_solve``); otherwise this module's host driver
+    runs the same steps kernel by kernel. ``GWB_NATIVE=0`` forces the host
+    driver. ``sync_free`` is accepted for signature parity and ignored (every
+    round reads four device scalars, like the reference's synchronous path)."""
+    if mode not in ("fp64", "fp32exp"):
+        raise ValueError(f"mode must be 'fp64' or 'fp32exp', got {mode!r}")
     with torch.no_grad():
+        ham = getattr(h_apply, "__self__", None)
+        max_dim = min(max_dim_factor * int(x0.shape[1]), int(mask.sum(dim=1).min()))
+        native = (os.environ.get("GWB_NATIVE", "1") != "0" and ham is not None
+                  and getattr(h_apply, "__func__", None) is getattr(type(ham), "apply", None)
+                  and hasattr(ham, "_native_workspace") and x0.is_cuda and x0.dtype == torch.complex128
+                  and (precond is None or (isinstance(precond, str) and precond == "teter"))
+                  and history_out is None and int(x0.shape[1]) <= max_dim <= int(_lib.load().gwb_heev_max_dim()))
+        if native:
+            res = _native_solve(ham, x0, t, mask, tol, max_iter, max_dim, mode)
+            if res is not None:
+                return res
         return _Solver(h_apply, x0, t, mask, tol, max_iter, max_dim_factor, mode, precond, history_out).run()
+
+
+LOW = torch.complex64  # the draft dtype of the two-stage schedule
+
+
+def mixed_precision_solve(x0, tol, crossover, mixed_precision, *, full, make_stages):
+    """Draft -> polish scaffold (gradwave ``solvers/_ms.py:26-52``): a single
+    full-precision solve when mixed precision is off, x0 is already complex64
+    or crossover >= tol; otherwise draft at complex64 to ``crossover`` and
+    polish at x0's precision to ``tol`` from the drafted vectors."""
+    if (not mixed_precision) or x0.dtype == LOW or crossover >= tol:
+        return full()
+    hi = x0.dtype
+    draft, polish = make_stages()
+    d = draft(x0.to(LOW))
+    return polish(d.eigenvectors.to(hi))
+
+
+def davidson_batched_ms(h_apply, x0, t, mask, tol: float = 1e-9, max_iter: int = 40, max_dim_factor: int = 4,
+                        crossover: float = 1e-5, mixed_precision: bool = True) -> BatchedDavidsonResult:
+    """Two-stage Davidson (gradwave ``solvers/davidson.py:778-812``): a
+    complex64 draft (float32 applies) to ``crossover``, then a full-precision
+    polish to ``tol`` warm-started from it."""
+
+    def solve(x, tl):
+        return davidson_batched(h_apply, x, t, mask, tol=tl, max_iter=max_iter, max_dim_factor=max_dim_factor)
+
+    return mixed_precision_solve(x0, tol, crossover, mixed_precision,
+                                 full=lambda: solve(x0, tol),
+                                 make_stages=lambda: (lambda xlo: solve(xlo, crossover),
+                                                      lambda x1: solve(x1, tol)))

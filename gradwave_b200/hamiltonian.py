@@ -131,5 +131,18 @@ class BatchedHamiltonian:
         _lib.call("gwb_ham_apply_strided", self._h, src_ptr, src_kstride, dst_ptr, dst_kstride, nrows,
                   _lib.GWB_C128, prec, _lib.stream_ptr(self.device))
 
+    def _count_rows(self, n: int) -> None:
+        if _TALLY["on"]:
+            _TALLY["count"] += n
+        opcount.bump("hpsi", n)
+
+    def _native_workspace(self, nbytes: int) -> torch.Tensor:
+        """Device workspace of the native Davidson driver, kept across solves."""
+        ws = getattr(self, "_ws", None)
+        if ws is None or ws.numel() < nbytes:
+            ws = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+            self._ws = ws
+        return ws
+
     def scratch_bytes(self) -> int:
         return int(_lib.load().gwb_ham_scratch_bytes(self._h))

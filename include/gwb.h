@@ -187,6 +187,42 @@ int gwb_heev_max_dim(void);
 int gwb_heev_lowest_noalloc(int32_t nk, int32_t m, int32_t nb, const void* S, int32_t lds, int64_t s_kstride,
                             double* eig, void* U, int32_t* info, void* stream);
 
+/* ======================================================================= */
+/* Native Davidson driver                                                  */
+/* ======================================================================= */
+
+typedef struct {
+  int32_t nk, nb, npw;   /* block (nk, nb, npw) with npw = npw_max of the handle */
+  int32_t max_dim;       /* basis capacity: min(max_dim_factor * nb, min_k npw), <= gwb_heev_max_dim() */
+  int32_t max_iter;
+  int32_t mode;          /* 0: float64 applies; 1: float32 expansion applies with float64 certification */
+  int32_t precond;       /* 0: Teter-Payne-Allan */
+  int32_t reserved;
+  double tol;            /* residual-norm gate [eV] */
+  double t_max;          /* largest kinetic energy of the batch (float32 residual-floor estimate) */
+} gwb_davidson_params;
+
+typedef struct {
+  int32_t n_iter, hit_max_iter, n_restart, n_cert, n_repair, n_rollback;
+  int64_t n_apply_low, n_apply_full;  /* band*k applies in float32 / float64 */
+  double max_residual;
+} gwb_davidson_stats;
+
+/* Device workspace the solve needs (bytes, 256-byte aligned base). */
+int gwb_davidson_workspace_bytes(const gwb_davidson_params* p, size_t* bytes);
+
+/* Lowest nb eigenpairs of the handle's Hamiltonian by batched block Davidson
+ * from the start block x0 (complex128, device): eig_out (nk, nb) ascending,
+ * vec_out (nk, nb, npw) orthonormal rows with padded slots 0, rn_out (nk, nb)
+ * residual norms; stats (HOST) gets the counters. t (nk, npw) kinetic diagonal,
+ * mask (nk, npw) uint8. model must be NULL for precond 0. Returns GWB_OK also
+ * when max_iter is hit (stats->hit_max_iter = 1), like the reference.
+ * Replaces gradwave solvers/davidson.py:528-774 (davidson_batched) and the
+ * registry adapter core of solvers/registry.py:154-182. */
+int gwb_davidson_solve(gwb_ham* h, const gwb_davidson_params* p, const void* model, const void* x0,
+                       const double* t, const uint8_t* mask, void* workspace, size_t workspace_bytes,
+                       double* eig_out, void* vec_out, double* rn_out, gwb_davidson_stats* stats, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

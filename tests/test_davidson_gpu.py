@@ -96,3 +96,47 @@ def test_si8_fp32_expansion_within_bar(cuda_device):
     assert float(res.residual_norms.max()) < 1e-10
     assert np.abs(eig - g["eigenvalues"]).max() < EIG_TOL_HA
     assert res.n_apply_low > 0 and res.n_apply_full > 0
+
+
+def test_native_and_host_driver_agree(cuda_device, monkeypatch):
+    """The native driver (one libgwb.so call) and the host driver (kernel by
+    kernel from Python) run the same algorithm: same eigenpairs."""
+    from gradwave_b200.davidson import davidson_batched
+    g = load_golden("si8_cubic")
+    ci, bk, h = _cell_ham("si8_cubic")
+    x0 = ci.identity_start().to(cuda_device)
+    for mode in ("fp64", "fp32exp"):
+        native = davidson_batched(h.apply, x0, bk.t, bk.mask, tol=1e-10, max_iter=200, mode=mode)
+        assert native.info.get("native")
+        monkeypatch.setenv("GWB_NATIVE", "0")
+        host = davidson_batched(h.apply, x0, bk.t, bk.mask, tol=1e-10, max_iter=200, mode=mode)
+        monkeypatch.delenv("GWB_NATIVE")
+        assert not host.info.get("native")
+        for res in (native, host):
+            assert float(res.residual_norms.max()) < 1e-10
+            assert np.abs(res.eigenvalues.cpu().numpy() - g["eigenvalues"]).max() < 1e-9
+        assert abs(native.n_iter - host.n_iter) <= 3
+
+
+def test_registry_adapters_and_two_stage(cuda_device):
+    """Registry contract (reference solvers/registry.py) and the complex64
+    draft -> complex128 polish schedule (reference davidson_batched_ms)."""
+    from gradwave_b200 import registry
+    from gradwave_b200.davidson import davidson_batched_ms
+    g = load_golden("si8_cubic")
+    ci, bk, h = _cell_ham("si8_cubic")
+    x0 = ci.identity_start().to(cuda_device)
+    with pytest.raises(ValueError):
+        registry.register("davidson", registry.davidson_adapter)
+    with pytest.raises(ValueError, match="registered"):
+        registry.get("nope")
+    for name in ("davidson", "davidson_mixed"):
+        r = registry.get(name)(h.apply, x0, bk.t, bk.mask, tol=1e-10, nbands=ci.nbands, max_iter=200)
+        assert isinstance(r, registry.EigResult)
+        assert np.abs(r.eigenvalues.cpu().numpy() - g["eigenvalues"]).max() < EIG_TOL_HA
+        assert r.diagnostics["hit_max_iter"] is False
+    r = registry.get("davidson")(h.apply, x0, bk.t, bk.mask, tol=1e-10, nbands=ci.nbands, max_iter=3)
+    assert r.diagnostics["hit_max_iter"] is True and r.n_iter == 3
+    ms = davidson_batched_ms(h.apply, x0, bk.t, bk.mask, tol=1e-10, max_iter=200, crossover=1e-4)
+    assert float(ms.residual_norms.max()) < 1e-10
+    assert np.abs(ms.eigenvalues.cpu().numpy() - g["eigenvalues"]).max() < 1e-9
