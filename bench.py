@@ -419,6 +419,29 @@ def run_apply(args):
     return 0
 
 
+def run_once(args):
+    """One warm-up and one timed solve of the workload (for ncu launch lists)."""
+    import torch
+    from gradwave_b200.cells import make_cell
+    from gradwave_b200.davidson import davidson_batched
+    from gradwave_b200.hamiltonian import BatchedHamiltonian
+    dev = torch.device("cuda", 0)
+    ci = make_cell(args.config)
+    bk = ci.bk.to(dev)
+    h = BatchedHamiltonian(bk, ci.shape, ci.v_eff_r, ci.p)
+    x0 = ci.identity_start().to(dev)
+    mode = "fp64" if args.prec == "fp64" else "fp32exp"
+    for _ in range(args.warmup):
+        davidson_batched(h.apply, x0, bk.t, bk.mask, tol=args.tol, max_iter=300, mode=mode)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = davidson_batched(h.apply, x0, bk.t, bk.mask, tol=args.tol, max_iter=300, mode=mode)
+    torch.cuda.synchronize()
+    print(json.dumps({"mode": "once", "config": args.config, "solver_mode": mode, "n_iter": r.n_iter,
+                      "wall_ms": (time.perf_counter() - t0) * 1e3}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -428,12 +451,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--mode", default="solve", choices=["solve", "apply"],
-                    help="apply: only time Hamiltonian applies (profiling)")
+    ap.add_argument("--mode", default="solve", choices=["solve", "apply", "once"],
+                    help="apply: only time Hamiltonian applies; once: a single solve (profiling)")
     ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64"], help="arithmetic of --mode apply")
     args = ap.parse_args()
     if args.mode == "apply":
         return run_apply(args)
+    if args.mode == "once":
+        return run_once(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

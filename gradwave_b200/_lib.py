@@ -82,6 +82,8 @@ _SIGNATURES = {
     "gwb_ham_scratch_bytes": [_P],
     "gwb_zgemm": [ctypes.c_int, ctypes.c_int, _I64, _I64, _I64, _D, _D, _P, _I64, _I64, _P, _I64, _I64,
                   _D, _D, _P, _I64, _I64, _I64, _P],
+    "gwb_zgemm_nh": [_I64, _I64, _I64, _D, _D, _P, _I64, _I64, _P, _I64, _I64, _D, _D, _P, _I64, _I64, _I64, _P,
+                     ctypes.c_size_t, _P],
     "gwb_residual": [_I, _I, _I, _P, _I64, _P, _I64, _P, _I64, _P, _I64, _P, _P],
     "gwb_conv_stats": [_I, _I, _P, _D, _P, _P],
     "gwb_select_worst": [_I, _I, _P, _I, _P, _P],

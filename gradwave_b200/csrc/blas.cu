@@ -7,6 +7,7 @@
 // C^T = op(B)^T op(A)^T in cuBLAS terms with the operands swapped.
 #include <cublas_v2.h>
 
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -68,5 +69,116 @@ extern "C" int gwb_zgemm(int opA, int opB, int64_t M, int64_t N, int64_t K, doub
     set_error("cublasZgemmStridedBatched failed with status " + std::to_string((int)s));
     return GWB_ERR_CUDA;
   }
+  return GWB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Inner-product GEMM with a long reduction: C = alpha A B^H + beta C with
+// A (M x K), B (N x K) row-major and M, N small (the subspace, projection and
+// Gram products of the Davidson step: M, N <= a few hundred, K = npw). cuBLAS
+// tiles such shapes into a few dozen CTAs; here K is split into slices so the
+// grid fills the GPU, each CTA accumulates a 32 x 32 output tile of one slice
+// (2 x 2 outputs per thread, float64), and a second kernel sums the slices in
+// a fixed order (deterministic).
+namespace gwb {
+
+constexpr int NH_T = 32, NH_K = 16;
+
+__global__ void __launch_bounds__(256) k_zgemm_nh_part(int M, int N, int K, int kslice,
+                                                       const cplx<double>* __restrict__ A, int64_t lda, int64_t sA,
+                                                       const cplx<double>* __restrict__ B, int64_t ldb, int64_t sB,
+                                                       cplx<double>* __restrict__ part, int batch) {
+  __shared__ cplx<double> sa[NH_T][NH_K + 1];
+  __shared__ cplx<double> sb[NH_T][NH_K + 1];
+  const int tilesN = (N + NH_T - 1) / NH_T;
+  const int ti = blockIdx.x / tilesN, tj = blockIdx.x % tilesN;
+  const int s = blockIdx.y, b = blockIdx.z;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const cplx<double>* Ab = A + b * sA;
+  const cplx<double>* Bb = B + b * sB;
+  const int g0 = s * kslice, g1 = min(K, g0 + kslice);
+  cplx<double> acc[2][2];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int c = 0; c < 2; ++c) acc[a][c] = mk<double>(0.0, 0.0);
+  for (int gb = g0; gb < g1; gb += NH_K) {
+    for (int idx = threadIdx.x; idx < NH_T * NH_K; idx += 256) {
+      const int r = idx / NH_K, kk = idx % NH_K;
+      const int g = gb + kk;
+      const int ia = ti * NH_T + r, jb = tj * NH_T + r;
+      sa[r][kk] = (ia < M && g < g1) ? Ab[(int64_t)ia * lda + g] : mk<double>(0.0, 0.0);
+      sb[r][kk] = (jb < N && g < g1) ? Bb[(int64_t)jb * ldb + g] : mk<double>(0.0, 0.0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < NH_K; ++kk) {
+      const cplx<double> a0 = sa[ty][kk], a1 = sa[ty + 16][kk];
+      const cplx<double> b0 = sb[tx][kk], b1 = sb[tx + 16][kk];
+      acc[0][0] = acc[0][0] + mul_conj(a0, b0);
+      acc[0][1] = acc[0][1] + mul_conj(a0, b1);
+      acc[1][0] = acc[1][0] + mul_conj(a1, b0);
+      acc[1][1] = acc[1][1] + mul_conj(a1, b1);
+    }
+    __syncthreads();
+  }
+  cplx<double>* P = part + ((int64_t)s * batch + b) * M * N;
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const int i = ti * NH_T + ty + 16 * a, j = tj * NH_T + tx + 16 * c;
+      if (i < M && j < N) P[(int64_t)i * N + j] = acc[a][c];
+    }
+}
+
+__global__ void k_zgemm_nh_reduce(int M, int N, int nslice, int batch, const cplx<double>* __restrict__ part,
+                                  cplx<double> alpha, cplx<double> beta, cplx<double>* __restrict__ C, int64_t ldc,
+                                  int64_t sC) {
+  const int64_t total = (int64_t)batch * M * N;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int b = (int)(idx / ((int64_t)M * N));
+    const int64_t r = idx % ((int64_t)M * N);
+    const int i = (int)(r / N), j = (int)(r % N);
+    cplx<double> a = mk<double>(0.0, 0.0);
+    for (int s = 0; s < nslice; ++s) a = a + part[(int64_t)s * total + idx];
+    cplx<double>* c = C + b * sC + (int64_t)i * ldc + j;
+    cplx<double> v = alpha * a;
+    if (beta.x != 0.0 || beta.y != 0.0) v = v + beta * (*c);
+    *c = v;
+  }
+}
+
+}  // namespace gwb
+
+extern "C" int gwb_zgemm_nh(int64_t M, int64_t N, int64_t K, double alpha_re, double alpha_im, const void* A,
+                            int64_t lda, int64_t strideA, const void* B, int64_t ldb, int64_t strideB,
+                            double beta_re, double beta_im, void* C, int64_t ldc, int64_t strideC, int64_t batch,
+                            void* work, size_t work_bytes, void* stream) {
+  GWB_REQUIRE(M >= 0 && N >= 0 && K >= 0 && batch >= 0, "negative size");
+  if (M == 0 || N == 0 || batch == 0) return GWB_OK;
+  GWB_REQUIRE(A && B && C && work, "null pointer");
+  GWB_REQUIRE(M * N * batch * 16 <= (int64_t)work_bytes, "work smaller than one M*N*batch slice");
+  const int tiles = (int)(((M + NH_T - 1) / NH_T) * ((N + NH_T - 1) / NH_T));
+  const int64_t slice_bytes = M * N * batch * 16;
+  int64_t want = (4 * 148 + (int64_t)tiles * batch - 1) / ((int64_t)tiles * batch);
+  want = std::min<int64_t>(want, std::max<int64_t>(1, K / 128));
+  want = std::min<int64_t>(want, (int64_t)work_bytes / slice_bytes);
+  const int nslice = (int)std::max<int64_t>(1, want);
+  const int kslice = (int)(((K + nslice - 1) / nslice + NH_K - 1) / NH_K * NH_K);
+  const int ns = (int)((K + kslice - 1) / kslice);
+  dim3 g1(tiles, ns, (unsigned)batch);
+  k_zgemm_nh_part<<<g1, 256, 0, (cudaStream_t)stream>>>((int)M, (int)N, (int)K, kslice, (const cplx<double>*)A, lda,
+                                                        strideA, (const cplx<double>*)B, ldb, strideB,
+                                                        (cplx<double>*)work, (int)batch);
+  const int64_t total = M * N * batch;
+  const int blocks = (int)std::min<int64_t>((total + 255) / 256, 4096);
+  k_zgemm_nh_reduce<<<blocks, 256, 0, (cudaStream_t)stream>>>((int)M, (int)N, ns, (int)batch,
+                                                              (const cplx<double>*)work, mk<double>(alpha_re, alpha_im),
+                                                              mk<double>(beta_re, beta_im), (cplx<double>*)C, ldc,
+                                                              strideC);
+  GWB_LAUNCH_CHECK();
+  count_launches(2);
   return GWB_OK;
 }

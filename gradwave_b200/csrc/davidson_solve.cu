@@ -22,6 +22,9 @@ extern "C" {
 int gwb_zgemm(int opA, int opB, int64_t M, int64_t N, int64_t K, double alpha_re, double alpha_im,
               const void* A, int64_t lda, int64_t strideA, const void* B, int64_t ldb, int64_t strideB,
               double beta_re, double beta_im, void* C, int64_t ldc, int64_t strideC, int64_t batch, void* stream);
+int gwb_zgemm_nh(int64_t M, int64_t N, int64_t K, double alpha_re, double alpha_im, const void* A, int64_t lda,
+                 int64_t strideA, const void* B, int64_t ldb, int64_t strideB, double beta_re, double beta_im,
+                 void* C, int64_t ldc, int64_t strideC, int64_t batch, void* work, size_t work_bytes, void* stream);
 }
 
 namespace gwb {
@@ -94,7 +97,10 @@ struct Buf {
 
 typedef cplx<double> Z16;
 
+constexpr size_t NH_WORK_BYTES = (size_t)24 << 20;  // split-K partials of the A B^H products
+
 struct Work {
+  unsigned char* nh_work;
   Z16 *V, *HV, *S, *X, *HX, *R, *D, *D2, *C, *G, *Linv, *Gs, *U;
   double *Zs, *rn, *eig, *eig2, *stats;
   int *sel, *info, *heev_info, *flags;
@@ -127,6 +133,7 @@ static size_t layout(const gwb_davidson_params& p, unsigned char* base, Work* w)
   t.info = b.take<int>(base, nk);
   t.heev_info = b.take<int>(base, nk);
   t.flags = b.take<int>(base, 1);
+  t.nh_work = b.take<unsigned char>(base, NH_WORK_BYTES);
   if (w) *w = t;
   return b.off + 256;
 }
@@ -275,8 +282,13 @@ class Solver {
     return gwb_ham_apply_strided(h_, src, sk, dst, dk, rows, GWB_C128, low ? GWB_FP32 : GWB_FP64, st_);
   }
 
+  // A B^H products (long reduction over plane waves) go to the split-K kernel,
+  // the rest (long output rows) to cuBLAS.
   int zgemm(int oa, int ob, int64_t M, int64_t N, int64_t K, const void* A, int64_t lda, int64_t sA, const void* B,
             int64_t ldb, int64_t sB, void* C, int64_t ldc, int64_t sC, double alpha = 1.0, double beta = 0.0) {
+    if (oa == 0 && ob == 2 && M * N * nk_ * 16 <= (int64_t)NH_WORK_BYTES)
+      return gwb_zgemm_nh(M, N, K, alpha, 0.0, A, lda, sA, B, ldb, sB, beta, 0.0, C, ldc, sC, nk_, w_.nh_work,
+                          NH_WORK_BYTES, st_);
     return gwb_zgemm(oa, ob, M, N, K, alpha, 0.0, A, lda, sA, B, ldb, sB, beta, 0.0, C, ldc, sC, nk_, st_);
   }
 

@@ -67,12 +67,30 @@ def _ptr(t: torch.Tensor, offset_elems: int = 0) -> int:
     return t.data_ptr() + offset_elems * t.element_size()
 
 
+_NH_WORK: dict = {}
+
+
+def _nh_work(dev) -> torch.Tensor:
+    w = _NH_WORK.get(dev)
+    if w is None:
+        w = torch.empty(24 << 20, dtype=torch.uint8, device=dev)
+        _NH_WORK[dev] = w
+    return w
+
+
 def zgemm(opA, opB, M, N, K, A, lda, sA, B, ldb, sB, C, ldc, sC, batch, alpha=1.0, beta=0.0,
           a_off=0, b_off=0, c_off=0, stream=None):
-    """Row-major batched complex128 GEMM through gwb_zgemm (offsets in elements)."""
+    """Row-major batched complex128 GEMM (offsets in elements): A B^H products
+    with a small output go to the split-K kernel gwb_zgemm_nh, the rest to
+    cuBLAS through gwb_zgemm."""
     s = _lib.stream_ptr(C.device) if stream is None else stream
     a = complex(alpha)
     b = complex(beta)
+    if opA == _N and opB == _H and M * N * batch * 16 <= (24 << 20):
+        w = _nh_work(C.device)
+        _lib.call("gwb_zgemm_nh", M, N, K, a.real, a.imag, _ptr(A, a_off), lda, sA, _ptr(B, b_off), ldb, sB,
+                  b.real, b.imag, _ptr(C, c_off), ldc, sC, batch, w.data_ptr(), w.numel(), s)
+        return
     _lib.call("gwb_zgemm", opA, opB, M, N, K, a.real, a.imag, _ptr(A, a_off), lda, sA, _ptr(B, b_off), ldb,
               sB, b.real, b.imag, _ptr(C, c_off), ldc, sC, batch, s)
 

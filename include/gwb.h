@@ -125,6 +125,16 @@ int gwb_zgemm(int opA, int opB, int64_t M, int64_t N, int64_t K, double alpha_re
               double beta_re, double beta_im, void* C, int64_t ldc, int64_t strideC, int64_t batch,
               void* stream);
 
+/* C = alpha A B^H + beta C per batch for row-major A (M x K), B (N x K) with
+ * a long reduction K (plane waves) and a small output: K is split into slices
+ * accumulated in `work` (at least M*N*batch*16 bytes; more bytes allow more
+ * slices), then summed in a fixed order. The subspace, projection and Gram
+ * products of gradwave solvers/davidson.py:428-432,648-649,215. */
+int gwb_zgemm_nh(int64_t M, int64_t N, int64_t K, double alpha_re, double alpha_im, const void* A, int64_t lda,
+                 int64_t strideA, const void* B, int64_t ldb, int64_t strideB, double beta_re, double beta_im,
+                 void* C, int64_t ldc, int64_t strideC, int64_t batch, void* work, size_t work_bytes,
+                 void* stream);
+
 /* r = hx - eig * x and rn = |r| per (k, band); eig (nk, eig_kstride) float64.
  * Replaces gradwave solvers/davidson.py:656-657. */
 int gwb_residual(int32_t nk, int32_t nb, int32_t npw, const void* x, int64_t x_kstride, const void* hx,

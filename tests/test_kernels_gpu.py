@@ -79,3 +79,18 @@ def test_precond_residual_select(cuda_device):
     d_ref = teter_b(rsel, t, np.take_along_axis(tband, sel_ref, 1))
     d_ref /= np.linalg.norm(d_ref, axis=-1, keepdims=True)
     assert np.abs(D.cpu().numpy()[:, :n_add] - d_ref).max() < 1e-12
+
+
+@pytest.mark.parametrize("M,N,K,batch", [(96, 24, 4645, 10), (7, 3, 100, 2), (640, 160, 37073, 1), (24, 24, 33, 4)])
+def test_zgemm_nh_split_k(cuda_device, M, N, K, batch):
+    from gradwave_b200 import _lib
+    rng = np.random.default_rng(M + N)
+    a = rng.standard_normal((batch, M, K)) + 1j * rng.standard_normal((batch, M, K))
+    b = rng.standard_normal((batch, N, K)) + 1j * rng.standard_normal((batch, N, K))
+    c0 = rng.standard_normal((batch, M, N)) + 1j * rng.standard_normal((batch, M, N))
+    A, B, C = (torch.from_numpy(x).to(cuda_device) for x in (a, b, c0))
+    work = torch.empty(24 << 20, dtype=torch.uint8, device=cuda_device)
+    _lib.call("gwb_zgemm_nh", M, N, K, 0.5, 0.25, A.data_ptr(), K, M * K, B.data_ptr(), K, N * K, -1.0, 0.0,
+              C.data_ptr(), N, M * N, batch, work.data_ptr(), work.numel(), _lib.stream_ptr(cuda_device))
+    ref = (0.5 + 0.25j) * a @ b.conj().transpose(0, 2, 1) - c0
+    assert np.abs(C.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
