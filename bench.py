@@ -193,41 +193,6 @@ def run_reference(args):
     return 0
 
 
-class ApplyTimer:
-    """Wraps a BatchedHamiltonian's apply_into with CUDA events to time every
-    launch of the dominant kernel inside the timed region."""
-
-    def __init__(self, h):
-        import torch
-        self.h = h
-        self.torch = torch
-        self.orig = h.apply_into
-        self.events = []
-        self.rows = 0
-        self.on = False
-
-    def __enter__(self):
-        def timed(*a, **kw):
-            if not self.on:
-                return self.orig(*a, **kw)
-            e0 = self.torch.cuda.Event(enable_timing=True)
-            e1 = self.torch.cuda.Event(enable_timing=True)
-            e0.record()
-            self.orig(*a, **kw)
-            e1.record()
-            self.events.append((e0, e1, a[4], a[5]))
-        self.h.apply_into = timed
-        return self
-
-    def __exit__(self, *a):
-        self.h.apply_into = self.orig
-
-    def collect(self):
-        out = [(e0.elapsed_time(e1), nrows, prec) for e0, e1, nrows, prec in self.events]
-        self.events = []
-        return out
-
-
 def run_ours(args):
     import torch
     from gradwave_b200 import _lib
@@ -283,17 +248,17 @@ def run_ours(args):
         return statistics.mean(ts), out
 
     mode_fast = "fp32exp"
-    # value: device-resident inputs
+    # value: device-resident inputs; every H apply inside the timed native
+    # solves is bracketed by CUDA events on the solve stream (GWB_TIME_APPLIES)
     n0 = _lib.launch_count()
+    os.environ["GWB_TIME_APPLIES"] = "1"
     with ClockSampler(dev.index) as clk:
-        with ApplyTimer(h) as at:
-            for _ in range(args.warmup):
-                solve(x0_dev, mode_fast)
-            at.on = True
-            ms_fast, res_fast = timed(lambda: solve(x0_dev, mode_fast), args.steps, 0)
-            at.on = False
-            apply_launches = at.collect()
-    launches = (_lib.launch_count() - n0) * args.steps // (args.steps + args.warmup)
+        for _ in range(args.warmup):
+            solve(x0_dev, mode_fast)
+        n1 = _lib.launch_count()
+        ms_fast, res_fast = timed(lambda: solve(x0_dev, mode_fast), args.steps, 0)
+        launches = (_lib.launch_count() - n1) // max(1, args.steps)
+    os.environ["GWB_TIME_APPLIES"] = "0"
     err_fast = check(res_fast)
     # plain float64 TPA Davidson on the same GPU
     ms_plain, res_plain = timed(lambda: solve(x0_dev, "fp64"), max(1, args.steps // 2), 1)
@@ -313,33 +278,35 @@ def run_ours(args):
     ms_e2e = _max_over_ranks(ms_e2e, ws, dev)
     ms_plain = _max_over_ranks(ms_plain, ws, dev)
 
-    # roofline of the dominant kernel: the batched Hamiltonian apply
+    # roofline of the H apply (the path's bandwidth kernel) from the last timed solve
     hbm_peak, peak_kind = _peaks()
-    per_rows = {}
-    for ms, nrows, prec in apply_launches:
-        per_rows.setdefault(prec, []).append((ms, nrows))
-    tot_ms = sum(ms for ms, _, _ in apply_launches)
-    tot_rows = sum(n for _, n, _ in apply_launches)
+    info = res_fast.info
+    n_calls = int(info.get("n_apply_calls", 0))
+    apply_ms = float(info.get("apply_ms", 0.0))
+    units = res_fast.n_apply_low + res_fast.n_apply_full          # band*k applied
     nk = ci.bk.nk
     npw = ci.bk.npw.numpy().astype(np.float64)
     n_box = float(np.prod(ci.shape))
     nproj = int(ci.p.shape[1])
-    # algorithmic bytes per band (c128 storage): c in + H c out (16+16 B per plane
-    # wave) + the dense box through HBM once per 3D FFT at fp32 (2 x 16 B per
-    # point); per launch + v(r) (4 B per point) + projectors read twice (fp32)
     mean_npw = float(npw.mean())
-    bytes_per_band = 32.0 * mean_npw + 32.0 * n_box
-    alg_bytes = tot_rows * nk * bytes_per_band + len(apply_launches) * (4.0 * n_box + 2 * 8.0 * nk * nproj * mean_npw)
-    achieved = alg_bytes / (tot_ms * 1e-3) / 1e9 if tot_ms > 0 else 0.0
-    roof = {"kernel": "gwb_ham_apply (K1 plane_inverse + K2 pencil_vloc + K3 plane_forward + nonlocal)",
+    # algorithmic bytes (per band*k: 16 npw + 32 N; per launch: 4 N for v(r)
+    # and the projectors read twice, 16 nk nproj npw)
+    bytes_per_unit = 16.0 * mean_npw + 32.0 * n_box
+    per_launch = 4.0 * n_box + 16.0 * nk * nproj * mean_npw
+    alg_bytes = units * bytes_per_unit + n_calls * per_launch
+    achieved = alg_bytes / (apply_ms * 1e-3) / 1e9 if apply_ms > 0 else 0.0
+    roof = {"kernel": "gwb_ham_apply (plane_inverse + pencil_vloc + plane_forward + becp + nl_add)",
             "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
             "frac": round(achieved / hbm_peak, 4), "peak_kind": peak_kind, "traffic": None,
-            "launches": len(apply_launches), "avg_launch_ms": round(tot_ms / max(1, len(apply_launches)), 4),
-            "share_of_step": round(tot_ms / max(1e-9, ms_fast * args.steps), 4),
-            "bytes_per_band": bytes_per_band}
-    traffic_file = ROOT / "profiles" / f"traffic_{args.config}.json"
-    if traffic_file.exists():
-        roof["traffic"] = json.loads(traffic_file.read_text()).get("bytes_per_launch")
+            "launches": n_calls, "avg_launch_ms": round(apply_ms / max(1, n_calls), 4),
+            "share_of_step": round(apply_ms / max(1e-9, ms_fast), 4),
+            "bytes_per_unit": bytes_per_unit, "units_per_step": int(units)}
+    summary = ROOT / "profiles" / f"gwb_ham_apply_{args.config}.md"
+    if summary.exists():
+        import re
+        m = re.search(r"dram_bytes_per_band_k:\s*([0-9.eE+]+)", summary.read_text())
+        if m and n_calls:
+            roof["traffic"] = round(float(m.group(1)) * units / n_calls)
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -363,6 +330,7 @@ def run_ours(args):
                 "e2e": {"value": round(ms_e2e / ws, 3), "unit": "ms", "h2d_bytes_per_step": int(x0_host.numel() * 16),
                         "d2h_bytes_per_step": int(ev.numel() * 8 + n_vec)},
                 "gpu_launches": int(launches), "roofline": roof, "clocks": clk.summary(),
+                "eigh_note": "subspace eigensolver is latency bound (one CTA per k); see profiles/",
                 "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     if ws > 1:

@@ -48,7 +48,7 @@ class Geometry(ctypes.Structure):
 class DavidsonParams(ctypes.Structure):
     _fields_ = [("nk", ctypes.c_int32), ("nb", ctypes.c_int32), ("npw", ctypes.c_int32),
                 ("max_dim", ctypes.c_int32), ("max_iter", ctypes.c_int32), ("mode", ctypes.c_int32),
-                ("precond", ctypes.c_int32), ("reserved", ctypes.c_int32), ("tol", ctypes.c_double),
+                ("precond", ctypes.c_int32), ("flags", ctypes.c_int32), ("tol", ctypes.c_double),
                 ("t_max", ctypes.c_double)]
 
 
@@ -56,7 +56,8 @@ class DavidsonStats(ctypes.Structure):
     _fields_ = [("n_iter", ctypes.c_int32), ("hit_max_iter", ctypes.c_int32), ("n_restart", ctypes.c_int32),
                 ("n_cert", ctypes.c_int32), ("n_repair", ctypes.c_int32), ("n_rollback", ctypes.c_int32),
                 ("n_apply_low", ctypes.c_int64), ("n_apply_full", ctypes.c_int64),
-                ("max_residual", ctypes.c_double)]
+                ("max_residual", ctypes.c_double), ("apply_ms", ctypes.c_double),
+                ("n_apply_calls", ctypes.c_int64)]
 
 
 _lock = threading.Lock()

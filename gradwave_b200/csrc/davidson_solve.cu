@@ -249,6 +249,13 @@ class Solver {
     GWB_CUDA_TRY(cudaMemcpyAsync(rn_out, w_.rn, sizeof(double) * nk_ * nb_, cudaMemcpyDeviceToDevice, st_));
     GWB_CUDA_TRY(cudaMemcpyAsync(vec_out, w_.X, sizeof(Z16) * nk_ * nbp, cudaMemcpyDeviceToDevice, st_));
     if (out) {
+      if (p_.flags & 1) {
+        GWB_CUDA_TRY(cudaStreamSynchronize(st_));
+        out->apply_ms = apply_ms();
+      } else {
+        out->apply_ms = 0.0;
+      }
+      out->n_apply_calls = n_apply_calls_;
       out->n_iter = it;
       out->hit_max_iter = it >= p_.max_iter ? 1 : 0;
       out->n_restart = n_restart_;
@@ -279,7 +286,35 @@ class Solver {
   int apply(const Z16* src, int64_t sk, Z16* dst, int64_t dk, int rows, bool low) {
     if (low) n_low_ += (int64_t)nk_ * rows;
     else n_full_ += (int64_t)nk_ * rows;
-    return gwb_ham_apply_strided(h_, src, sk, dst, dk, rows, GWB_C128, low ? GWB_FP32 : GWB_FP64, st_);
+    ++n_apply_calls_;
+    const bool timed = (p_.flags & 1) && n_events_ + 2 <= kMaxEvents;
+    if (timed) {
+      GWB_CUDA_TRY(cudaEventCreate(&ev_[n_events_]));
+      GWB_CUDA_TRY(cudaEventRecord(ev_[n_events_], st_));
+    }
+    const int rc = gwb_ham_apply_strided(h_, src, sk, dst, dk, rows, GWB_C128, low ? GWB_FP32 : GWB_FP64, st_);
+    if (timed) {
+      GWB_CUDA_TRY(cudaEventCreate(&ev_[n_events_ + 1]));
+      GWB_CUDA_TRY(cudaEventRecord(ev_[n_events_ + 1], st_));
+      n_events_ += 2;
+    }
+    return rc;
+  }
+
+ public:
+  ~Solver() {
+    for (int i = 0; i < n_events_; ++i) cudaEventDestroy(ev_[i]);
+  }
+
+ private:
+  // sum of the timed apply intervals (the stream is drained by then)
+  double apply_ms() {
+    double tot = 0.0;
+    for (int i = 0; i + 1 < n_events_; i += 2) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, ev_[i], ev_[i + 1]) == cudaSuccess) tot += ms;
+    }
+    return tot;
   }
 
   // A B^H products (long reduction over plane waves) go to the split-K kernel,
@@ -411,7 +446,10 @@ class Solver {
   bool fp32_exp_ = false;
   const double* last_eig_ = nullptr;
   int n_restart_ = 0, n_cert_ = 0, n_repair_ = 0, n_rollback_ = 0;
-  int64_t n_low_ = 0, n_full_ = 0;
+  int64_t n_low_ = 0, n_full_ = 0, n_apply_calls_ = 0;
+  static constexpr int kMaxEvents = 2048;
+  cudaEvent_t ev_[kMaxEvents];
+  int n_events_ = 0;
 };
 
 }  // namespace gwb

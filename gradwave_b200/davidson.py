@@ -471,14 +471,15 @@ class _Solver:
         return BatchedDavidsonResult(eig.clone(), x, it, ws.rn.clone(), self.n_low, self.n_full, info)
 
 
-def _native_solve(ham, x0, t, mask, tol, max_iter, max_dim, mode) -> BatchedDavidsonResult | None:
+def _native_solve(ham, x0, t, mask, tol, max_iter, max_dim, mode, time_applies=False
+                  ) -> BatchedDavidsonResult | None:
     """The whole solve inside libgwb.so (``gwb_davidson_solve``); None when the
     library reports a breakdown it does not repair (the host driver retries)."""
     import ctypes
     nk, nb, npw = (int(s) for s in x0.shape)
     dev = x0.device
-    p = _lib.DavidsonParams(nk, nb, npw, max_dim, int(max_iter), 1 if mode == "fp32exp" else 0, 0, 0,
-                            float(tol), float(t.max()))
+    p = _lib.DavidsonParams(nk, nb, npw, max_dim, int(max_iter), 1 if mode == "fp32exp" else 0, 0,
+                            1 if time_applies else 0, float(tol), float(t.max()))
     nbytes = ctypes.c_size_t()
     _lib.call("gwb_davidson_workspace_bytes", ctypes.byref(p), ctypes.byref(nbytes))
     ws = ham._native_workspace(int(nbytes.value))
@@ -499,7 +500,9 @@ def _native_solve(ham, x0, t, mask, tol, max_iter, max_dim, mode) -> BatchedDavi
     n_rows = st.n_apply_low + st.n_apply_full
     ham._count_rows(n_rows)
     info = {"n_restart": st.n_restart, "n_cert": st.n_cert, "n_repair": st.n_repair, "n_rollback": st.n_rollback,
-            "max_dim": max_dim, "native": True}
+            "max_dim": max_dim, "native": True, "n_apply_calls": int(st.n_apply_calls)}
+    if time_applies:
+        info["apply_ms"] = float(st.apply_ms)
     return BatchedDavidsonResult(eig, vec, int(st.n_iter), rn, int(st.n_apply_low), int(st.n_apply_full), info)
 
 
@@ -526,7 +529,8 @@ def davidson_batched(h_apply, x0, t, mask, tol: float = 1e-9, max_iter: int = 40
                   and (precond is None or (isinstance(precond, str) and precond == "teter"))
                   and history_out is None and int(x0.shape[1]) <= max_dim <= int(_lib.load().gwb_heev_max_dim()))
         if native:
-            res = _native_solve(ham, x0, t, mask, tol, max_iter, max_dim, mode)
+            res = _native_solve(ham, x0, t, mask, tol, max_iter, max_dim, mode,
+                                time_applies=os.environ.get("GWB_TIME_APPLIES", "0") == "1")
             if res is not None:
                 return res
         return _Solver(h_apply, x0, t, mask, tol, max_iter, max_dim_factor, mode, precond, history_out).run()

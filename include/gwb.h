@@ -207,7 +207,7 @@ typedef struct {
   int32_t max_iter;
   int32_t mode;          /* 0: float64 applies; 1: float32 expansion applies with float64 certification */
   int32_t precond;       /* 0: Teter-Payne-Allan */
-  int32_t reserved;
+  int32_t flags;         /* bit 0: time every H apply with CUDA events (stats->apply_ms) */
   double tol;            /* residual-norm gate [eV] */
   double t_max;          /* largest kinetic energy of the batch (float32 residual-floor estimate) */
 } gwb_davidson_params;
@@ -216,6 +216,8 @@ typedef struct {
   int32_t n_iter, hit_max_iter, n_restart, n_cert, n_repair, n_rollback;
   int64_t n_apply_low, n_apply_full;  /* band*k applies in float32 / float64 */
   double max_residual;
+  double apply_ms;                    /* device time of the H applies (timing flag only) */
+  int64_t n_apply_calls;              /* gwb_ham_apply launches of the solve */
 } gwb_davidson_stats;
 
 /* Device workspace the solve needs (bytes, 256-byte aligned base). */
