@@ -95,6 +95,14 @@ _SIGNATURES = {
     "gwb_heev_lowest": [_I, _I, _I, _P, _I, _I64, _P, _P, _P, _P, _P],
     "gwb_heev_max_dim": [],
     "gwb_heev_lowest_noalloc": [_I, _I, _I, _P, _I, _I64, _P, _P, _P, _P],
+    "gwb_mlp_param_count": [],
+    "gwb_mlp_forward": [_P, _I, _P, _P, _P],
+    "gwb_mlp_loss_grad": [_P, _I, _P, _P, _P, _P, _P, _P],
+    "gwb_mlp_backward": [_P, _I, _P, _P, _P, _P],
+    "gwb_mlp_adam": [_P, _P, _P, _P, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _P],
+    "gwb_precond_features": [_I, _I, _I, _I, _P, _I64, _P, _I64, _P, _P, _P, _P, _P],
+    "gwb_precond_learned": [_P, _I, _I, _I, _I, _P, _I64, _P, _I64, _P, _P, _P, _P, _P, _I64, _P],
+    "gwb_stall_update": [_P, _P, _P, _I, _D, _P],
     "gwb_davidson_workspace_bytes": [ctypes.POINTER(DavidsonParams), ctypes.POINTER(ctypes.c_size_t)],
     "gwb_davidson_solve": [_P, ctypes.POINTER(DavidsonParams), _P, _P, _P, _P, _P, ctypes.c_size_t, _P, _P, _P,
                            ctypes.POINTER(DavidsonStats), _P],

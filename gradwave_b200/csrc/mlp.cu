@@ -1,0 +1,492 @@
+// Learned Davidson preconditioner: a per-plane-wave MLP with BF16 weights and
+// activations and FP32 accumulation, trained on the GPU by these kernels.
+//
+//   features u (4) -> 64 -> 64 -> 64 -> 1, SiLU between layers
+//   K(G) = TPA(x) * exp(clamp(o, -3, 3)),  d = K r / |K r|
+//
+// Features of plane wave G of band b (one shared definition for logging,
+// training and inference, gwb_precond_features):
+//   u0 = log(1 + x),            x = t_G / t_b        (|k+G|^2, kinetic of psi)
+//   u1 = clamp(eps_b / t_b, -8, 8) / 4               (band eigenvalue)
+//   u2 = log10(|r_G| / r_rms + 1e-6) / 3             (residual amplitude)
+//   u3 = log10(max(t_b, 1e-3) / 10)                  (kinetic scale of psi)
+// with t_b = <x_b|T|x_b> and r_rms = |r_b| / sqrt(npw).
+//
+// Parameters: one float32 master array of GWB_MLP_NPARAM values,
+//   W1[64][4] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[64] b4
+// rounded to BF16 on load for the forward pass (straight-through gradients).
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "common.cuh"
+
+namespace gwb {
+
+constexpr int HID = 64, NIN = 4;
+constexpr int O_W1 = 0, O_B1 = O_W1 + HID * NIN, O_W2 = O_B1 + HID, O_B2 = O_W2 + HID * HID, O_W3 = O_B2 + HID,
+              O_B3 = O_W3 + HID * HID, O_W4 = O_B3 + HID, O_B4 = O_W4 + HID, NPARAM = O_B4 + 1;
+
+__device__ __forceinline__ float bf(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+__device__ __forceinline__ float sigm(float z) { return 1.f / (1.f + expf(-z)); }
+__device__ __forceinline__ float silu(float z) { return z * sigm(z); }
+__device__ __forceinline__ float dsilu(float z) {
+  const float s = sigm(z);
+  return s * (1.f + z * (1.f - s));
+}
+
+__device__ __forceinline__ void features(double tg, double tb, double eps, double rabs, double rrms, float* u) {
+  const double t = fmax(tb, 1e-12);
+  const double x = tg / t;
+  u[0] = (float)log1p(x);
+  u[1] = (float)(fmin(fmax(eps / t, -8.0), 8.0) / 4.0);
+  u[2] = (float)(log10(rabs / fmax(rrms, 1e-300) + 1e-6) / 3.0);
+  u[3] = (float)log10(fmax(tb, 1e-3) / 10.0);
+}
+
+__device__ __forceinline__ double tpa_coeff(double tg, double tb) {
+  const double x = tg / fmax(tb, 1e-12);
+  const double x2 = x * x;
+  const double p = 27.0 + 18.0 * x + 12.0 * x2 + 8.0 * x2 * x;
+  return p / (p + 16.0 * x2 * x2);
+}
+
+// BF16-rounded copy of the parameters into shared memory (floats).
+__device__ void load_params(const float* __restrict__ P, float* s) {
+  for (int i = threadIdx.x; i < NPARAM; i += blockDim.x) s[i] = bf(P[i]);
+  __syncthreads();
+}
+
+// Forward of one sample by one thread: a3 kept for nothing; returns o.
+__device__ float forward_one(const float* s, const float* u) {
+  float a0[NIN], h1[HID], h2[HID];
+#pragma unroll
+  for (int i = 0; i < NIN; ++i) a0[i] = bf(u[i]);
+#pragma unroll 4
+  for (int o = 0; o < HID; ++o) {
+    float z = s[O_B1 + o];
+#pragma unroll
+    for (int i = 0; i < NIN; ++i) z = fmaf(s[O_W1 + o * NIN + i], a0[i], z);
+    h1[o] = bf(silu(z));
+  }
+#pragma unroll 2
+  for (int o = 0; o < HID; ++o) {
+    float z = s[O_B2 + o];
+#pragma unroll
+    for (int i = 0; i < HID; ++i) z = fmaf(s[O_W2 + o * HID + i], h1[i], z);
+    h2[o] = bf(silu(z));
+  }
+  float out = s[O_B4];
+#pragma unroll 2
+  for (int o = 0; o < HID; ++o) {
+    float z = s[O_B3 + o];
+#pragma unroll
+    for (int i = 0; i < HID; ++i) z = fmaf(s[O_W3 + o * HID + i], h2[i], z);
+    out = fmaf(s[O_W4 + o], bf(silu(z)), out);
+  }
+  return out;
+}
+
+__global__ void __launch_bounds__(256) k_mlp_forward(const float* __restrict__ P, int n, const float* __restrict__ U,
+                                                     float* __restrict__ out) {
+  extern __shared__ float sp[];
+  load_params(P, sp);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float u[NIN];
+#pragma unroll
+    for (int q = 0; q < NIN; ++q) u[q] = U[(int64_t)i * NIN + q];
+    out[i] = forward_one(sp, u);
+  }
+}
+
+// Forward + backward over tiles of TS samples: with targets Y the loss is
+// sum_i w_i (o_i - y_i)^2; with Y == NULL, Wt holds dL/do_i of any loss.
+// Activations of a tile stay in shared memory; weight gradients accumulate per
+// CTA in shared memory and are added to G once per CTA.
+constexpr int TS = 32;
+__global__ void __launch_bounds__(256) k_mlp_loss_grad(const float* __restrict__ P, int n, const float* __restrict__ U,
+                                                       const float* __restrict__ Y, const float* __restrict__ Wt,
+                                                       float* __restrict__ G, float* __restrict__ loss) {
+  extern __shared__ float sm[];
+  float* sp = sm;                      // NPARAM   bf16-rounded params
+  float* sg = sp + NPARAM;             // NPARAM   gradient accumulators
+  float* a0 = sg + NPARAM;             // TS*NIN
+  float* z1 = a0 + TS * NIN;           // TS*HID  (pre-activations)
+  float* a1 = z1 + TS * HID;
+  float* z2 = a1 + TS * HID;
+  float* a2 = z2 + TS * HID;
+  float* z3 = a2 + TS * HID;
+  float* a3 = z3 + TS * HID;
+  float* dz = a3 + TS * HID;           // TS*HID  (current layer dz)
+  float* dz2 = dz + TS * HID;          // TS*HID
+  float* dout = dz2 + TS * HID;        // TS
+  __shared__ float sloss;
+  load_params(P, sp);
+  for (int i = threadIdx.x; i < NPARAM; i += blockDim.x) sg[i] = 0.f;
+  if (threadIdx.x == 0) sloss = 0.f;
+  __syncthreads();
+  const int ntiles = (n + TS - 1) / TS;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int s0 = tile * TS;
+    for (int i = threadIdx.x; i < TS * NIN; i += blockDim.x) {
+      const int s = s0 + i / NIN;
+      a0[i] = s < n ? bf(U[(int64_t)s * NIN + i % NIN]) : 0.f;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < TS * HID; i += blockDim.x) {
+      const int s = i / HID, o = i % HID;
+      float z = sp[O_B1 + o];
+      for (int q = 0; q < NIN; ++q) z = fmaf(sp[O_W1 + o * NIN + q], a0[s * NIN + q], z);
+      z1[i] = z;
+      a1[i] = bf(silu(z));
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < TS * HID; i += blockDim.x) {
+      const int s = i / HID, o = i % HID;
+      float z = sp[O_B2 + o];
+      for (int q = 0; q < HID; ++q) z = fmaf(sp[O_W2 + o * HID + q], a1[s * HID + q], z);
+      z2[i] = z;
+      a2[i] = bf(silu(z));
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < TS * HID; i += blockDim.x) {
+      const int s = i / HID, o = i % HID;
+      float z = sp[O_B3 + o];
+      for (int q = 0; q < HID; ++q) z = fmaf(sp[O_W3 + o * HID + q], a2[s * HID + q], z);
+      z3[i] = z;
+      a3[i] = bf(silu(z));
+    }
+    __syncthreads();
+    if (threadIdx.x < TS) {
+      const int s = threadIdx.x, gs = s0 + s;
+      float o = sp[O_B4];
+      for (int q = 0; q < HID; ++q) o = fmaf(sp[O_W4 + q], a3[s * HID + q], o);
+      float d = 0.f;
+      if (gs < n) {
+        if (Y) {
+          const float e = o - Y[gs];
+          d = 2.f * Wt[gs] * e;
+          atomicAdd(&sloss, Wt[gs] * e * e);
+        } else {
+          d = Wt[gs];  // caller-supplied dL/do
+        }
+      }
+      dout[s] = d;
+    }
+    __syncthreads();
+    // output layer
+    for (int q = threadIdx.x; q < HID; q += blockDim.x) {
+      float g = 0.f;
+      for (int s = 0; s < TS; ++s) g = fmaf(dout[s], a3[s * HID + q], g);
+      sg[O_W4 + q] += g;
+    }
+    if (threadIdx.x == 0) {
+      float g = 0.f;
+      for (int s = 0; s < TS; ++s) g += dout[s];
+      sg[O_B4] += g;
+    }
+    for (int i = threadIdx.x; i < TS * HID; i += blockDim.x) {
+      const int s = i / HID, q = i % HID;
+      dz[i] = dout[s] * sp[O_W4 + q] * dsilu(z3[i]);
+    }
+    __syncthreads();
+    // layer 3: W3 grads, propagate to dz2
+    for (int i = threadIdx.x; i < HID * HID; i += blockDim.x) {
+      const int o = i / HID, q = i % HID;
+      float g = 0.f;
+      for (int s = 0; s < TS; ++s) g = fmaf(dz[s * HID + o], a2[s * HID + q], g);
+      sg[O_W3 + i] += g;
+    }
+    for (int o = threadIdx.x; o < HID; o += blockDim.x) {
+      float g = 0.f;
+      for (int s = 0; s < TS; ++s) g += dz[s * HID + o];
+      sg[O_B3 + o] += g;
+    }
+    for (int i = threadIdx.x; i < TS * HID; i += blockDim.x) {
+      const int s = i / HID, q = i % HID;
+      float g = 0.f;
+      for (int o = 0; o < HID; ++o) g = fmaf(sp[O_W3 + o * HID + q], dz[s * HID + o], g);
+      dz2[i] = g * dsilu(z2[i]);
+    }
+    __syncthreads();
+    // layer 2
+    for (int i = threadIdx.x; i < HID * HID; i += blockDim.x) {
+      const int o = i / HID, q = i % HID;
+      float g = 0.f;
+      for (int s = 0; s < TS; ++s) g = fmaf(dz2[s * HID + o], a1[s * HID + q], g);
+      sg[O_W2 + i] += g;
+    }
+    for (int o = threadIdx.x; o < HID; o += blockDim.x) {
+      float g = 0.f;
+      for (int s = 0; s < TS; ++s) g += dz2[s * HID + o];
+      sg[O_B2 + o] += g;
+    }
+    for (int i = threadIdx.x; i < TS * HID; i += blockDim.x) {
+      const int s = i / HID, q = i % HID;
+      float g = 0.f;
+      for (int o = 0; o < HID; ++o) g = fmaf(sp[O_W2 + o * HID + q], dz2[s * HID + o], g);
+      dz[i] = g * dsilu(z1[i]);
+    }
+    __syncthreads();
+    // layer 1
+    for (int i = threadIdx.x; i < HID * NIN; i += blockDim.x) {
+      const int o = i / NIN, q = i % NIN;
+      float g = 0.f;
+      for (int s = 0; s < TS; ++s) g = fmaf(dz[s * HID + o], a0[s * NIN + q], g);
+      sg[O_W1 + i] += g;
+    }
+    for (int o = threadIdx.x; o < HID; o += blockDim.x) {
+      float g = 0.f;
+      for (int s = 0; s < TS; ++s) g += dz[s * HID + o];
+      sg[O_B1 + o] += g;
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < NPARAM; i += blockDim.x) atomicAdd(&G[i], sg[i]);
+  if (threadIdx.x == 0 && Y) atomicAdd(loss, sloss);
+}
+
+// Adam (Kingma & Ba, 2015) on the float32 master parameters.
+__global__ void k_mlp_adam(float* __restrict__ P, const float* __restrict__ G, float* __restrict__ M,
+                           float* __restrict__ V, int n, float lr, float b1, float b2, float eps, float c1, float c2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float g = G[i];
+    const float m = b1 * M[i] + (1.f - b1) * g;
+    const float v = b2 * V[i] + (1.f - b2) * g * g;
+    M[i] = m;
+    V[i] = v;
+    P[i] -= lr * (m / c1) / (sqrtf(v / c2) + eps);
+  }
+}
+
+// Features of the selected rows at every plane wave: U (nk, n_add, npw, 4).
+__global__ void __launch_bounds__(256) k_features(int npw, int nb, int n_add, const cplx<double>* __restrict__ x,
+                                                  int64_t xk, const cplx<double>* __restrict__ r, int64_t rk,
+                                                  const double* __restrict__ t, const double* __restrict__ eig,
+                                                  const int* __restrict__ sel, float* __restrict__ U) {
+  __shared__ double red[8];
+  __shared__ double sv[2];
+  const int k = blockIdx.x / n_add, s = blockIdx.x % n_add;
+  const int b = sel[(int64_t)k * n_add + s];
+  const cplx<double>* xr = x + k * xk + (int64_t)b * npw;
+  const cplx<double>* rr = r + k * rk + (int64_t)b * npw;
+  const double* tk = t + (int64_t)k * npw;
+  double tb = 0.0, r2 = 0.0;
+  for (int g = threadIdx.x; g < npw; g += blockDim.x) {
+    tb += tk[g] * norm2(xr[g]);
+    r2 += norm2(rr[g]);
+  }
+  // two block sums
+  for (int o = 16; o > 0; o >>= 1) {
+    tb += __shfl_xor_sync(0xffffffffu, tb, o);
+    r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5] = tb;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int w = 0; w < 8; ++w) a += red[w];
+    sv[0] = a;
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = r2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int w = 0; w < 8; ++w) a += red[w];
+    sv[1] = a;
+  }
+  __syncthreads();
+  const double tbv = sv[0], rrms = sqrt(sv[1] / npw), eps = eig[(int64_t)k * nb + b];
+  float* Uo = U + ((int64_t)k * n_add + s) * npw * NIN;
+  for (int g = threadIdx.x; g < npw; g += blockDim.x) {
+    float u[NIN];
+    features(tk[g], tbv, eps, sqrt(norm2(rr[g])), rrms, u);
+#pragma unroll
+    for (int q = 0; q < NIN; ++q) Uo[(int64_t)g * NIN + q] = u[q];
+  }
+}
+
+// The learned preconditioner step: like k_precond_teter, with the TPA
+// coefficient corrected by the network; bands flagged in tpa_only (the stall
+// fallback) keep plain TPA.
+__global__ void __launch_bounds__(256) k_precond_learned(const float* __restrict__ P, int npw, int nb, int n_add,
+                                                         const cplx<double>* __restrict__ x, int64_t xk,
+                                                         const cplx<double>* __restrict__ r, int64_t rk,
+                                                         const double* __restrict__ t, const double* __restrict__ eig,
+                                                         const int* __restrict__ sel,
+                                                         const unsigned char* __restrict__ tpa_only,
+                                                         cplx<double>* __restrict__ d, int64_t dk) {
+  extern __shared__ float sp[];
+  __shared__ double red[8];
+  __shared__ double sv[3];
+  load_params(P, sp);
+  const int k = blockIdx.x / n_add, s = blockIdx.x % n_add;
+  const int b = sel[(int64_t)k * n_add + s];
+  const bool plain = tpa_only && tpa_only[(int64_t)k * nb + b];
+  const cplx<double>* xr = x + k * xk + (int64_t)b * npw;
+  const cplx<double>* rr = r + k * rk + (int64_t)b * npw;
+  const double* tk = t + (int64_t)k * npw;
+  cplx<double>* dr = d + k * dk + (int64_t)s * npw;
+  double tb = 0.0, r2 = 0.0;
+  for (int g = threadIdx.x; g < npw; g += blockDim.x) {
+    tb += tk[g] * norm2(xr[g]);
+    r2 += norm2(rr[g]);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    tb += __shfl_xor_sync(0xffffffffu, tb, o);
+    r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = tb;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int w = 0; w < 8; ++w) a += red[w];
+    sv[0] = a;
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = r2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int w = 0; w < 8; ++w) a += red[w];
+    sv[1] = a;
+  }
+  __syncthreads();
+  const double tbv = sv[0], rrms = sqrt(sv[1] / npw), eps = eig[(int64_t)k * nb + b];
+  double nn = 0.0;
+  for (int g = threadIdx.x; g < npw; g += blockDim.x) {
+    const cplx<double> rv = rr[g];
+    double c = tpa_coeff(tk[g], tbv);
+    if (!plain && (rv.x != 0.0 || rv.y != 0.0)) {
+      float u[NIN];
+      features(tk[g], tbv, eps, sqrt(norm2(rv)), rrms, u);
+      const float o = fminf(fmaxf(forward_one(sp, u), -3.f), 3.f);
+      c *= (double)expf(o);
+    }
+    const cplx<double> v = scale(rv, c);
+    dr[g] = v;
+    nn += norm2(v);
+  }
+  for (int o = 16; o > 0; o >>= 1) nn += __shfl_xor_sync(0xffffffffu, nn, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = nn;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int w = 0; w < 8; ++w) a += red[w];
+    sv[2] = sqrt(a);
+  }
+  __syncthreads();
+  if (sv[2] > 1e-300) {
+    const double inv = 1.0 / sv[2];
+    for (int g = threadIdx.x; g < npw; g += blockDim.x) dr[g] = scale(dr[g], inv);
+  }
+}
+
+// tpa_only[k][b] |= rn[k][b] > ratio * rn_prev[k][b]; rn_prev = rn.
+__global__ void k_stall_update(const double* __restrict__ rn, double* __restrict__ rn_prev,
+                               unsigned char* __restrict__ tpa_only, int n, double ratio) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (rn[i] > ratio * rn_prev[i]) tpa_only[i] = 1;
+    rn_prev[i] = rn[i];
+  }
+}
+
+}  // namespace gwb
+
+using namespace gwb;
+
+extern "C" {
+
+int gwb_mlp_param_count(void) { return NPARAM; }
+
+int gwb_mlp_forward(const float* params, int32_t n, const float* feats, float* out, void* stream) {
+  GWB_REQUIRE(params && feats && out && n >= 0, "bad arguments");
+  if (n == 0) return GWB_OK;
+  const size_t sm = NPARAM * sizeof(float);
+  GWB_CUDA_TRY(cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const int blocks = std::min((n + 255) / 256, 4 * 148);
+  k_mlp_forward<<<blocks, 256, sm, (cudaStream_t)stream>>>(params, n, feats, out);
+  GWB_LAUNCH_CHECK();
+  count_launches(1);
+  return GWB_OK;
+}
+
+int gwb_mlp_loss_grad(const float* params, int32_t n, const float* feats, const float* target, const float* weight,
+                      float* grad, float* loss, void* stream) {
+  GWB_REQUIRE(params && feats && target && weight && grad && loss && n >= 0, "bad arguments");
+  if (n == 0) return GWB_OK;
+  const size_t sm = (2 * NPARAM + TS * NIN + 8 * TS * HID + TS) * sizeof(float);
+  GWB_CUDA_TRY(cudaFuncSetAttribute(k_mlp_loss_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const int tiles = (n + TS - 1) / TS;
+  const int blocks = std::min(tiles, 2 * 148);
+  k_mlp_loss_grad<<<blocks, 256, sm, (cudaStream_t)stream>>>(params, n, feats, target, weight, grad, loss);
+  GWB_LAUNCH_CHECK();
+  count_launches(1);
+  return GWB_OK;
+}
+
+int gwb_mlp_adam(float* params, const float* grad, float* m, float* v, int32_t step, float lr, float beta1,
+                 float beta2, float eps, void* stream) {
+  GWB_REQUIRE(params && grad && m && v && step >= 1, "bad arguments");
+  const float c1 = 1.f - powf(beta1, (float)step), c2 = 1.f - powf(beta2, (float)step);
+  k_mlp_adam<<<(NPARAM + 255) / 256, 256, 0, (cudaStream_t)stream>>>(params, grad, m, v, NPARAM, lr, beta1, beta2,
+                                                                     eps, c1, c2);
+  GWB_LAUNCH_CHECK();
+  count_launches(1);
+  return GWB_OK;
+}
+
+int gwb_mlp_backward(const float* params, int32_t n, const float* feats, const float* dout, float* grad,
+                     void* stream) {
+  GWB_REQUIRE(params && feats && dout && grad && n >= 0, "bad arguments");
+  if (n == 0) return GWB_OK;
+  const size_t sm = (2 * NPARAM + TS * NIN + 8 * TS * HID + TS) * sizeof(float);
+  GWB_CUDA_TRY(cudaFuncSetAttribute(k_mlp_loss_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const int tiles = (n + TS - 1) / TS;
+  const int blocks = std::min(tiles, 2 * 148);
+  k_mlp_loss_grad<<<blocks, 256, sm, (cudaStream_t)stream>>>(params, n, feats, nullptr, dout, grad, nullptr);
+  GWB_LAUNCH_CHECK();
+  count_launches(1);
+  return GWB_OK;
+}
+
+int gwb_precond_features(int32_t nk, int32_t nb, int32_t n_add, int32_t npw, const void* x, int64_t x_kstride,
+                         const void* r, int64_t r_kstride, const double* t, const double* eig, const int32_t* sel,
+                         float* feats, void* stream) {
+  GWB_REQUIRE(nk > 0 && nb > 0 && n_add > 0 && npw > 0, "bad sizes");
+  GWB_REQUIRE(x && r && t && eig && sel && feats, "null pointer");
+  k_features<<<nk * n_add, 256, 0, (cudaStream_t)stream>>>(npw, nb, n_add, (const cplx<double>*)x, x_kstride,
+                                                          (const cplx<double>*)r, r_kstride, t, eig, sel, feats);
+  GWB_LAUNCH_CHECK();
+  count_launches(1);
+  return GWB_OK;
+}
+
+int gwb_precond_learned(const float* params, int32_t nk, int32_t nb, int32_t n_add, int32_t npw, const void* x,
+                        int64_t x_kstride, const void* r, int64_t r_kstride, const double* t, const double* eig,
+                        const int32_t* sel, const uint8_t* tpa_only, void* d, int64_t d_kstride, void* stream) {
+  GWB_REQUIRE(params && nk > 0 && nb > 0 && n_add > 0 && n_add <= nb && npw > 0, "bad sizes");
+  GWB_REQUIRE(x && r && t && eig && sel && d, "null pointer");
+  const size_t sm = NPARAM * sizeof(float);
+  GWB_CUDA_TRY(cudaFuncSetAttribute(k_precond_learned, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  k_precond_learned<<<nk * n_add, 256, sm, (cudaStream_t)stream>>>(params, npw, nb, n_add, (const cplx<double>*)x,
+                                                                  x_kstride, (const cplx<double>*)r, r_kstride, t,
+                                                                  eig, sel, tpa_only, (cplx<double>*)d, d_kstride);
+  GWB_LAUNCH_CHECK();
+  count_launches(1);
+  return GWB_OK;
+}
+
+int gwb_stall_update(const double* rn, double* rn_prev, uint8_t* tpa_only, int32_t n, double ratio, void* stream) {
+  GWB_REQUIRE(rn && rn_prev && tpa_only && n > 0, "bad arguments");
+  k_stall_update<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(rn, rn_prev, tpa_only, n, ratio);
+  GWB_LAUNCH_CHECK();
+  count_launches(1);
+  return GWB_OK;
+}
+
+}  // extern "C"

@@ -198,6 +198,38 @@ int gwb_heev_lowest_noalloc(int32_t nk, int32_t m, int32_t nb, const void* S, in
                             double* eig, void* U, int32_t* info, void* stream);
 
 /* ======================================================================= */
+/* Learned preconditioner (per-plane-wave MLP, BF16, FP32 accumulation).   */
+/* No counterpart in the reference: it replaces the TPA coefficient of     */
+/* gradwave solvers/precond.py:20-39 by TPA * exp(network), with TPA as    */
+/* the per-band fallback. params: float32 master array of                 */
+/* gwb_mlp_param_count() values; feats: (n, 4) float32.                   */
+/* ======================================================================= */
+
+int gwb_mlp_param_count(void);
+/* out[i] = network(feats[i]) (BF16 weights/activations, FP32 accumulation). */
+int gwb_mlp_forward(const float* params, int32_t n, const float* feats, float* out, void* stream);
+/* grad += d/dparams sum_i w_i (o_i - y_i)^2; loss += the sum (caller zeroes). */
+int gwb_mlp_loss_grad(const float* params, int32_t n, const float* feats, const float* target, const float* weight,
+                      float* grad, float* loss, void* stream);
+/* grad += d/dparams of any loss given dL/do per sample (dout, n floats). */
+int gwb_mlp_backward(const float* params, int32_t n, const float* feats, const float* dout, float* grad,
+                     void* stream);
+/* One Adam step (step >= 1) on the float32 master parameters. */
+int gwb_mlp_adam(float* params, const float* grad, float* m, float* v, int32_t step, float lr, float beta1,
+                 float beta2, float eps, void* stream);
+/* Network features of the selected rows at every plane wave: feats (nk, n_add, npw, 4). */
+int gwb_precond_features(int32_t nk, int32_t nb, int32_t n_add, int32_t npw, const void* x, int64_t x_kstride,
+                         const void* r, int64_t r_kstride, const double* t, const double* eig, const int32_t* sel,
+                         float* feats, void* stream);
+/* As gwb_precond_teter with the coefficient TPA * exp(clamp(network, -3, 3));
+ * bands with tpa_only[k][b] != 0 (uint8 (nk, nb), may be NULL) keep TPA. */
+int gwb_precond_learned(const float* params, int32_t nk, int32_t nb, int32_t n_add, int32_t npw, const void* x,
+                        int64_t x_kstride, const void* r, int64_t r_kstride, const double* t, const double* eig,
+                        const int32_t* sel, const uint8_t* tpa_only, void* d, int64_t d_kstride, void* stream);
+/* Stall fallback: tpa_only[i] |= rn[i] > ratio * rn_prev[i]; rn_prev = rn. */
+int gwb_stall_update(const double* rn, double* rn_prev, uint8_t* tpa_only, int32_t n, double ratio, void* stream);
+
+/* ======================================================================= */
 /* Native Davidson driver                                                  */
 /* ======================================================================= */
 

@@ -82,3 +82,21 @@ def test_oracle_davidson_si8():
     res = davidson_batched(from_cell(ci).apply, ci.identity_start().numpy(), ci.bk.t.numpy(),
                            ci.bk.mask.numpy(), tol=1e-10, max_iter=200)
     assert np.abs(res.eigenvalues - g["eigenvalues"]).max() < 1e-9
+
+
+def test_mlp_oracle_backward_matches_finite_differences():
+    from oracle import mlp
+    rng = np.random.default_rng(0)
+    p = mlp.init_params(1)
+    p[-65:] = rng.standard_normal(65) * 0.3
+    u = rng.standard_normal((40, 4))
+    y = rng.standard_normal(40)
+    w = rng.uniform(0, 1, 40)
+    _, g = mlp.loss_grad(p, u, y, w, emulate_bf16=False)
+    for i in rng.choice(len(p), 25, replace=False):
+        h = 1e-6
+        pp, pm = p.copy(), p.copy()
+        pp[i] += h
+        pm[i] -= h
+        fd = (mlp.loss_grad(pp, u, y, w, False)[0] - mlp.loss_grad(pm, u, y, w, False)[0]) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 * (abs(fd) + abs(g[i])) + 1e-12
