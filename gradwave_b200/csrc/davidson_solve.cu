@@ -53,6 +53,10 @@ __global__ void k_masked_copy(const cplx<double>* __restrict__ src, int64_t sk, 
   }
 }
 
+__global__ void k_fill(double* __restrict__ p, int n, double v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+
 // stats[2] = max info (eigensolver), stats[3] = flags; flags reset.
 __global__ void k_pack_flags(const int* __restrict__ heev_info, int nk, int* __restrict__ flags,
                              double* __restrict__ stats) {
@@ -81,6 +85,9 @@ int gwb_heev_lowest(int32_t, int32_t, int32_t, const void*, int32_t, int64_t, do
                     void*);
 int gwb_heev_max_dim(void);
 int gwb_ham_apply_strided(gwb_ham*, const void*, int64_t, void*, int64_t, int32_t, int32_t, int32_t, void*);
+int gwb_precond_learned(const float*, int32_t, int32_t, int32_t, int32_t, const void*, int64_t, const void*, int64_t,
+                        const double*, const double*, const int32_t*, const uint8_t*, void*, int64_t, void*);
+int gwb_stall_update(const double*, double*, uint8_t*, int32_t, double, void*);
 }
 
 namespace gwb {
@@ -102,8 +109,9 @@ constexpr size_t NH_WORK_BYTES = (size_t)24 << 20;  // split-K partials of the A
 struct Work {
   unsigned char* nh_work;
   Z16 *V, *HV, *S, *X, *HX, *R, *D, *D2, *C, *G, *Linv, *Gs, *U;
-  double *Zs, *rn, *eig, *eig2, *stats;
+  double *Zs, *rn, *eig, *eig2, *stats, *rn_prev;
   int *sel, *info, *heev_info, *flags;
+  unsigned char* tpa_only;
 };
 
 static size_t layout(const gwb_davidson_params& p, unsigned char* base, Work* w) {
@@ -134,6 +142,8 @@ static size_t layout(const gwb_davidson_params& p, unsigned char* base, Work* w)
   t.heev_info = b.take<int>(base, nk);
   t.flags = b.take<int>(base, 1);
   t.nh_work = b.take<unsigned char>(base, NH_WORK_BYTES);
+  t.rn_prev = b.take<double>(base, nk * nb);
+  t.tpa_only = b.take<unsigned char>(base, nk * nb);
   if (w) *w = t;
   return b.off + 256;
 }
@@ -157,7 +167,12 @@ class Solver {
 
   int run(const void* x0, double* eig_out, void* vec_out, double* rn_out, gwb_davidson_stats* out) {
     const int64_t nbp = (int64_t)nb_ * npw_, mdp = (int64_t)md_ * npw_;
-    fp32_exp_ = p_.mode == 1;
+    fp32_exp_ = p_.mode == 1 || p_.mode == 2;
+    if (p_.precond == 1) {
+      k_fill<<<(nk_ * nb_ + 255) / 256, 256, 0, st_>>>(w_.rn_prev, nk_ * nb_, INFINITY);
+      GWB_LAUNCH_CHECK();
+      GWB_CUDA_TRY(cudaMemsetAsync(w_.tpa_only, 0, (size_t)nk_ * nb_, st_));
+    }
     // initial block: masked copy, orthonormalised with host-checked CholQR2
     GWB_TRY(masked_copy(static_cast<const Z16*>(x0), nbp, w_.D, nbp, nb_));
     int ok = 0;
@@ -192,7 +207,11 @@ class Solver {
         continue;
       }
       if (fp32_exp_) {
-        const bool stalled = it > 1 && rnmax > 0.7 * prev;
+        // mode 1 (the reference's rule) treats any round that shrinks the
+        // residual by < 30 % as a float32 stall; mode 2 only once the residual
+        // is within 100x of the float32 floor (early rounds often stagnate)
+        const bool gated = p_.mode == 1 || rnmax < 100.0 * cert_floor;
+        const bool stalled = it > 1 && rnmax > 0.7 * prev && gated;
         prev = rnmax;
         if (rnmax < std::max(p_.tol, cert_floor) || stalled) {
           GWB_TRY(certify());
@@ -385,7 +404,12 @@ class Solver {
 
   int precondition(int n_add, const double* eig) {
     const int64_t nbp = (int64_t)nb_ * npw_;
-    (void)eig;
+    if (p_.precond == 1) {
+      // stall fallback: a band whose residual shrank by less than 10 % keeps TPA
+      GWB_TRY(gwb_stall_update(w_.rn, w_.rn_prev, w_.tpa_only, nk_ * nb_, 0.9, st_));
+      return gwb_precond_learned(static_cast<const float*>(model_), nk_, nb_, n_add, npw_, w_.X, nbp, w_.R, nbp, t_,
+                                 eig, w_.sel, w_.tpa_only, w_.D, nbp, st_);
+    }
     return gwb_precond_teter(nk_, nb_, n_add, npw_, w_.X, nbp, w_.R, nbp, t_, w_.sel, w_.D, nbp, st_);
   }
 
@@ -472,8 +496,8 @@ int gwb_davidson_solve(gwb_ham* h, const gwb_davidson_params* p, const void* mod
   GWB_REQUIRE(p->nk > 0 && p->nb > 0 && p->npw > 0 && p->max_dim >= p->nb && p->max_iter > 0, "bad sizes");
   GWB_REQUIRE(p->max_dim <= gwb_heev_max_dim(),
               "max_dim exceeds the batched eigensolver limit; use the host-driven solver");
-  GWB_REQUIRE(p->mode == 0 || p->mode == 1, "mode must be 0 (float64) or 1 (float32 expansion)");
-  GWB_REQUIRE(p->precond == 0, "the native driver runs the TPA preconditioner (precond 0)");
+  GWB_REQUIRE(p->mode >= 0 && p->mode <= 2, "mode must be 0 (float64), 1 or 2 (float32 expansion)");
+  GWB_REQUIRE(p->precond == 0 || (p->precond == 1 && model), "precond must be 0 (TPA) or 1 (learned, model set)");
   Work w;
   const size_t need = layout(*p, static_cast<unsigned char*>(workspace), &w);
   GWB_REQUIRE(workspace_bytes >= need, "workspace too small (see gwb_davidson_workspace_bytes)");

@@ -36,13 +36,15 @@ __device__ __forceinline__ float dsilu(float z) {
   return s * (1.f + z * (1.f - s));
 }
 
+// float32 with fast intrinsics: the values feed a BF16 network
 __device__ __forceinline__ void features(double tg, double tb, double eps, double rabs, double rrms, float* u) {
-  const double t = fmax(tb, 1e-12);
-  const double x = tg / t;
-  u[0] = (float)log1p(x);
-  u[1] = (float)(fmin(fmax(eps / t, -8.0), 8.0) / 4.0);
-  u[2] = (float)(log10(rabs / fmax(rrms, 1e-300) + 1e-6) / 3.0);
-  u[3] = (float)log10(fmax(tb, 1e-3) / 10.0);
+  const float t = (float)fmax(tb, 1e-12);
+  const float x = (float)tg / t;
+  const float inv_ln10 = 0.43429448190325176f;
+  u[0] = __logf(1.f + x);
+  u[1] = fminf(fmaxf((float)eps / t, -8.f), 8.f) * 0.25f;
+  u[2] = __logf((float)(rabs / fmax(rrms, 1e-300)) + 1e-6f) * (inv_ln10 / 3.f);
+  u[3] = __logf(fmaxf((float)tb, 1e-3f) * 0.1f) * inv_ln10;
 }
 
 __device__ __forceinline__ double tpa_coeff(double tg, double tb) {
@@ -386,6 +388,217 @@ __global__ void __launch_bounds__(256) k_precond_learned(const float* __restrict
   }
 }
 
+// ---------------------------------------------------------------------------
+// Tensor-core inference (mma.sync m16n8k16, BF16 in, FP32 accumulate). A warp
+// evaluates 16 plane waves at a time: layer 1 (4 -> 64) on the CUDA cores
+// writes its SiLU outputs straight into the A fragments of layer 2; the FP32
+// accumulators of n-tiles 2j and 2j+1 of a layer are, element for element,
+// the A fragment of k-tile j of the next layer, so activations never leave
+// registers; layer 4 (64 -> 1) is a quad shuffle reduction.
+constexpr int WSTR = HID + 8;  // padded row stride (BF16) of W2/W3 in shared memory: conflict-free B loads
+
+__device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<unsigned*>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16(float* d, const unsigned* a, unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ float silu_fast(float z) { return __fdividef(z, 1.f + __expf(-z)); }
+
+// One hidden 64 -> 64 layer: acc[nt][4] = bias + A . W^T, then SiLU and BF16
+// packing into the next A fragments an[kt][4].
+__device__ __forceinline__ void tc_layer(const unsigned (&a)[4][4], const __nv_bfloat16* __restrict__ W,
+                                         const float* __restrict__ bias, int g, int t, unsigned (&an)[4][4]) {
+  float acc[8][4];
+#pragma unroll
+  for (int nt = 0; nt < 8; ++nt) {
+    const float b0 = bias[8 * nt + 2 * t], b1 = bias[8 * nt + 2 * t + 1];
+    acc[nt][0] = b0;
+    acc[nt][1] = b1;
+    acc[nt][2] = b0;
+    acc[nt][3] = b1;
+  }
+#pragma unroll
+  for (int kt = 0; kt < 4; ++kt) {
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      const __nv_bfloat16* w = W + (8 * nt + g) * WSTR + 16 * kt + 2 * t;
+      const unsigned b0 = *reinterpret_cast<const unsigned*>(w);
+      const unsigned b1 = *reinterpret_cast<const unsigned*>(w + 8);
+      mma_bf16(acc[nt], a[kt], b0, b1);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    an[j][0] = pack_bf16(silu_fast(acc[2 * j][0]), silu_fast(acc[2 * j][1]));
+    an[j][1] = pack_bf16(silu_fast(acc[2 * j][2]), silu_fast(acc[2 * j][3]));
+    an[j][2] = pack_bf16(silu_fast(acc[2 * j + 1][0]), silu_fast(acc[2 * j + 1][1]));
+    an[j][3] = pack_bf16(silu_fast(acc[2 * j + 1][2]), silu_fast(acc[2 * j + 1][3]));
+  }
+}
+
+__global__ void __launch_bounds__(256) k_precond_learned_tc(
+    const float* __restrict__ P, int npw, int nb, int n_add, const cplx<double>* __restrict__ x, int64_t xk,
+    const cplx<double>* __restrict__ r, int64_t rk, const double* __restrict__ t_, const double* __restrict__ eig,
+    const int* __restrict__ sel, const unsigned char* __restrict__ tpa_only, cplx<double>* __restrict__ d,
+    int64_t dk) {
+  __shared__ __align__(16) __nv_bfloat16 sW2[HID * WSTR];
+  __shared__ __align__(16) __nv_bfloat16 sW3[HID * WSTR];
+  __shared__ float sW1[HID * NIN], sB1[HID], sB2[HID], sB3[HID], sW4[HID], sB4;
+  __shared__ double red[8];
+  __shared__ double sv[3];
+  for (int i = threadIdx.x; i < HID * HID; i += blockDim.x) {
+    const int n = i / HID, kx = i % HID;
+    sW2[n * WSTR + kx] = __float2bfloat16_rn(P[O_W2 + i]);
+    sW3[n * WSTR + kx] = __float2bfloat16_rn(P[O_W3 + i]);
+  }
+  for (int i = threadIdx.x; i < HID * NIN; i += blockDim.x) sW1[i] = bf(P[O_W1 + i]);
+  for (int i = threadIdx.x; i < HID; i += blockDim.x) {
+    sB1[i] = bf(P[O_B1 + i]);
+    sB2[i] = bf(P[O_B2 + i]);
+    sB3[i] = bf(P[O_B3 + i]);
+    sW4[i] = bf(P[O_W4 + i]);
+  }
+  if (threadIdx.x == 0) sB4 = bf(P[O_B4]);
+  const int k = blockIdx.x / n_add, s = blockIdx.x % n_add;
+  const int b = sel[(int64_t)k * n_add + s];
+  const bool plain = tpa_only && tpa_only[(int64_t)k * nb + b];
+  const cplx<double>* xr = x + k * xk + (int64_t)b * npw;
+  const cplx<double>* rr = r + k * rk + (int64_t)b * npw;
+  const double* tk = t_ + (int64_t)k * npw;
+  cplx<double>* dr = d + k * dk + (int64_t)s * npw;
+  double tb = 0.0, r2 = 0.0;
+  for (int gi = threadIdx.x; gi < npw; gi += blockDim.x) {
+    tb += tk[gi] * norm2(xr[gi]);
+    r2 += norm2(rr[gi]);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    tb += __shfl_xor_sync(0xffffffffu, tb, o);
+    r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = tb;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int w = 0; w < 8; ++w) a += red[w];
+    sv[0] = a;
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = r2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int w = 0; w < 8; ++w) a += red[w];
+    sv[1] = a;
+  }
+  __syncthreads();
+  const double tbv = sv[0], rrms = sqrt(sv[1] / npw), eps = eig[(int64_t)k * nb + b];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
+  double nn = 0.0;
+  for (int c0 = 0; c0 < npw; c0 += 128) {
+    const int base = c0 + 16 * warp;  // this warp's 16 plane waves
+    // features of sample (lane & 15) by lanes 0..15
+    float u[NIN] = {0.f, 0.f, 0.f, 0.f};
+    cplx<double> rv = mk<double>(0.0, 0.0);
+    double tg = 0.0;
+    {
+      const int gi = base + (lane & 15);
+      if (lane < 16 && gi < npw) {
+        rv = rr[gi];
+        tg = tk[gi];
+        if (!plain) features(tg, tbv, eps, sqrt(norm2(rv)), rrms, u);
+      }
+    }
+    float o_row0 = 0.f, o_row8 = 0.f;
+    if (!plain) {
+      float ua[NIN], ub[NIN];
+#pragma unroll
+      for (int q = 0; q < NIN; ++q) {
+        ua[q] = bf(__shfl_sync(0xffffffffu, u[q], g));
+        ub[q] = bf(__shfl_sync(0xffffffffu, u[q], g + 8));
+      }
+      // layer 1 straight into A fragments of layer 2
+      unsigned a1[4][4];
+#pragma unroll
+      for (int kt = 0; kt < 4; ++kt) {
+        float h[2][4];  // [row g / g+8][col 2t, 2t+1, 2t+8, 2t+9]
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) {
+          const int col = 16 * kt + 2 * tq + (cc & 1) + 8 * (cc >> 1);
+          float za = sB1[col], zb = sB1[col];
+#pragma unroll
+          for (int q = 0; q < NIN; ++q) {
+            za = fmaf(sW1[col * NIN + q], ua[q], za);
+            zb = fmaf(sW1[col * NIN + q], ub[q], zb);
+          }
+          h[0][cc] = silu_fast(za);
+          h[1][cc] = silu_fast(zb);
+        }
+        a1[kt][0] = pack_bf16(h[0][0], h[0][1]);
+        a1[kt][1] = pack_bf16(h[1][0], h[1][1]);
+        a1[kt][2] = pack_bf16(h[0][2], h[0][3]);
+        a1[kt][3] = pack_bf16(h[1][2], h[1][3]);
+      }
+      unsigned a2[4][4], a3[4][4];
+      tc_layer(a1, sW2, sB2, g, tq, a2);
+      tc_layer(a2, sW3, sB3, g, tq, a3);
+      // layer 4: unpack a3 (rows g, g+8; cols 16kt + 2t + {0,1,8,9}) and dot with W4
+      float pa = 0.f, pb = 0.f;
+#pragma unroll
+      for (int kt = 0; kt < 4; ++kt) {
+#pragma unroll
+        for (int reg = 0; reg < 4; ++reg) {
+          const __nv_bfloat162 v = *reinterpret_cast<const __nv_bfloat162*>(&a3[kt][reg]);
+          const int col = 16 * kt + 2 * tq + 8 * (reg >> 1);
+          const float p0 = __bfloat162float(v.x) * sW4[col] + __bfloat162float(v.y) * sW4[col + 1];
+          if (reg & 1) pb += p0;
+          else pa += p0;
+        }
+      }
+      pa += __shfl_xor_sync(0xffffffffu, pa, 1);
+      pa += __shfl_xor_sync(0xffffffffu, pa, 2);
+      pb += __shfl_xor_sync(0xffffffffu, pb, 1);
+      pb += __shfl_xor_sync(0xffffffffu, pb, 2);
+      o_row0 = pa + sB4;
+      o_row8 = pb + sB4;
+    }
+    // sample (lane & 15) needs the output of row (lane & 15): rows g come from
+    // quad g (lane 4g), rows g+8 from quad g too (second value)
+    const int srow = lane & 15;
+    const float o_a = __shfl_sync(0xffffffffu, o_row0, 4 * (srow & 7));
+    const float o_b = __shfl_sync(0xffffffffu, o_row8, 4 * (srow & 7));
+    const float o = srow < 8 ? o_a : o_b;
+    const int gi = base + srow;
+    if (lane < 16 && gi < npw) {
+      double c = tpa_coeff(tg, tbv);
+      if (!plain && (rv.x != 0.0 || rv.y != 0.0)) c *= (double)__expf(fminf(fmaxf(o, -3.f), 3.f));
+      const cplx<double> v = scale(rv, c);
+      dr[gi] = v;
+      nn += norm2(v);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) nn += __shfl_xor_sync(0xffffffffu, nn, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = nn;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int w = 0; w < 8; ++w) a += red[w];
+    sv[2] = sqrt(a);
+  }
+  __syncthreads();
+  if (sv[2] > 1e-300) {
+    const double inv = 1.0 / sv[2];
+    for (int gi = threadIdx.x; gi < npw; gi += blockDim.x) dr[gi] = scale(dr[gi], inv);
+  }
+}
+
 // tpa_only[k][b] |= rn[k][b] > ratio * rn_prev[k][b]; rn_prev = rn.
 __global__ void k_stall_update(const double* __restrict__ rn, double* __restrict__ rn_prev,
                                unsigned char* __restrict__ tpa_only, int n, double ratio) {
@@ -471,11 +684,10 @@ int gwb_precond_learned(const float* params, int32_t nk, int32_t nb, int32_t n_a
                         const int32_t* sel, const uint8_t* tpa_only, void* d, int64_t d_kstride, void* stream) {
   GWB_REQUIRE(params && nk > 0 && nb > 0 && n_add > 0 && n_add <= nb && npw > 0, "bad sizes");
   GWB_REQUIRE(x && r && t && eig && sel && d, "null pointer");
-  const size_t sm = NPARAM * sizeof(float);
-  GWB_CUDA_TRY(cudaFuncSetAttribute(k_precond_learned, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  k_precond_learned<<<nk * n_add, 256, sm, (cudaStream_t)stream>>>(params, npw, nb, n_add, (const cplx<double>*)x,
-                                                                  x_kstride, (const cplx<double>*)r, r_kstride, t,
-                                                                  eig, sel, tpa_only, (cplx<double>*)d, d_kstride);
+  k_precond_learned_tc<<<nk * n_add, 256, 0, (cudaStream_t)stream>>>(params, npw, nb, n_add,
+                                                                     (const cplx<double>*)x, x_kstride,
+                                                                     (const cplx<double>*)r, r_kstride, t, eig, sel,
+                                                                     tpa_only, (cplx<double>*)d, d_kstride);
   GWB_LAUNCH_CHECK();
   count_launches(1);
   return GWB_OK;

@@ -28,6 +28,10 @@ Modes:
                       the first failed certification - the reference's
                       fp32-expansion mode (``solvers/davidson.py:226-308,
                       581-687``).
+  ``mode="mixed"``    as fp32exp, but a round that shrinks the residual by less
+                      than 30 % counts as a float32 stall only once the
+                      residual is within 100x of the float32 floor (early
+                      rounds stagnate without any precision limit).
 ``precond`` is ``"teter"`` or an object with ``apply_into(...)`` (the learned
 preconditioner, ``gradwave_b200.learned``), which falls back to TPA per band.
 """
@@ -160,8 +164,8 @@ class _Solver:
     def __init__(self, h_apply, x0, t, mask, tol, max_iter, max_dim_factor, mode, precond, history_out):
         if not x0.is_cuda:
             raise RuntimeError("davidson_batched (B200 path) needs CUDA tensors: there is no CPU fallback")
-        if mode not in ("fp64", "fp32exp"):
-            raise ValueError(f"mode must be 'fp64' or 'fp32exp', got {mode!r}")
+        if mode not in ("fp64", "fp32exp", "mixed"):
+            raise ValueError(f"mode must be 'fp64', 'fp32exp' or 'mixed', got {mode!r}")
         self.h_apply = h_apply
         self.ham = getattr(h_apply, "__self__", None)
         if self.ham is not None and not hasattr(self.ham, "apply_into"):
@@ -177,7 +181,8 @@ class _Solver:
         if self.max_dim < self.nb:
             raise ValueError(f"basis of {self.max_dim} cannot hold {self.nb} bands")
         # a complex64 block is a low-precision draft: float32 applies throughout
-        self.fp32_exp = mode == "fp32exp" and x0.dtype == torch.complex128
+        self.fp32_exp = mode in ("fp32exp", "mixed") and x0.dtype == torch.complex128
+        self.mode = mode
         self.all_fp32 = x0.dtype == torch.complex64
         self.precond = precond
         self.history_out = history_out
@@ -403,7 +408,8 @@ class _Solver:
                 it -= 1
                 continue
             if self.fp32_exp:
-                stalled = it > 1 and rnmax > _FP32_CERT_STALL * prev_rnmax
+                gated = self.mode == "fp32exp" or rnmax < 100.0 * cert_floor
+                stalled = it > 1 and rnmax > _FP32_CERT_STALL * prev_rnmax and gated
                 prev_rnmax = rnmax
                 if rnmax < max(self.tol, cert_floor) or stalled:
                     with self.prof("certify"):
@@ -471,15 +477,15 @@ class _Solver:
         return BatchedDavidsonResult(eig.clone(), x, it, ws.rn.clone(), self.n_low, self.n_full, info)
 
 
-def _native_solve(ham, x0, t, mask, tol, max_iter, max_dim, mode, time_applies=False
+def _native_solve(ham, x0, t, mask, tol, max_iter, max_dim, mode, time_applies=False, model=None
                   ) -> BatchedDavidsonResult | None:
     """The whole solve inside libgwb.so (``gwb_davidson_solve``); None when the
     library reports a breakdown it does not repair (the host driver retries)."""
     import ctypes
     nk, nb, npw = (int(s) for s in x0.shape)
     dev = x0.device
-    p = _lib.DavidsonParams(nk, nb, npw, max_dim, int(max_iter), 1 if mode == "fp32exp" else 0, 0,
-                            1 if time_applies else 0, float(tol), float(t.max()))
+    p = _lib.DavidsonParams(nk, nb, npw, max_dim, int(max_iter), {"fp64": 0, "fp32exp": 1, "mixed": 2}[mode],
+                            0 if model is None else 1, 1 if time_applies else 0, float(tol), float(t.max()))
     nbytes = ctypes.c_size_t()
     _lib.call("gwb_davidson_workspace_bytes", ctypes.byref(p), ctypes.byref(nbytes))
     ws = ham._native_workspace(int(nbytes.value))
@@ -490,7 +496,8 @@ def _native_solve(ham, x0, t, mask, tol, max_iter, max_dim, mode, time_applies=F
     vec = torch.empty(nk, nb, npw, dtype=torch.complex128, device=dev)
     rn = torch.empty(nk, nb, dtype=torch.float64, device=dev)
     st = _lib.DavidsonStats()
-    status = _lib.load().gwb_davidson_solve(ham._h, ctypes.byref(p), None, x0c.data_ptr(), tc.data_ptr(),
+    status = _lib.load().gwb_davidson_solve(ham._h, ctypes.byref(p), None if model is None else model.data_ptr(),
+                                            x0c.data_ptr(), tc.data_ptr(),
                                             mk.data_ptr(), ws.data_ptr(), ws.numel(), eig.data_ptr(),
                                             vec.data_ptr(), rn.data_ptr(), ctypes.byref(st), _lib.stream_ptr(dev))
     if status == _lib.GWB_ERR_BREAKDOWN:
@@ -518,19 +525,21 @@ def davidson_batched(h_apply, x0, t, mask, tol: float = 1e-9, max_iter: int = 40
     runs the same steps kernel by kernel. ``GWB_NATIVE=0`` forces the host
     driver. ``sync_free`` is accepted for signature parity and ignored (every
     round reads four device scalars, like the reference's synchronous path)."""
-    if mode not in ("fp64", "fp32exp"):
-        raise ValueError(f"mode must be 'fp64' or 'fp32exp', got {mode!r}")
+    if mode not in ("fp64", "fp32exp", "mixed"):
+        raise ValueError(f"mode must be 'fp64', 'fp32exp' or 'mixed', got {mode!r}")
     with torch.no_grad():
         ham = getattr(h_apply, "__self__", None)
         max_dim = min(max_dim_factor * int(x0.shape[1]), int(mask.sum(dim=1).min()))
         native = (os.environ.get("GWB_NATIVE", "1") != "0" and ham is not None
                   and getattr(h_apply, "__func__", None) is getattr(type(ham), "apply", None)
                   and hasattr(ham, "_native_workspace") and x0.is_cuda and x0.dtype == torch.complex128
-                  and (precond is None or (isinstance(precond, str) and precond == "teter"))
+                  and (precond is None or (isinstance(precond, str) and precond == "teter")
+                       or hasattr(precond, "params"))
                   and history_out is None and int(x0.shape[1]) <= max_dim <= int(_lib.load().gwb_heev_max_dim()))
         if native:
             res = _native_solve(ham, x0, t, mask, tol, max_iter, max_dim, mode,
-                                time_applies=os.environ.get("GWB_TIME_APPLIES", "0") == "1")
+                                time_applies=os.environ.get("GWB_TIME_APPLIES", "0") == "1",
+                                model=getattr(precond, "params", None))
             if res is not None:
                 return res
         return _Solver(h_apply, x0, t, mask, tol, max_iter, max_dim_factor, mode, precond, history_out).run()

@@ -9,8 +9,10 @@ result keeps the reference's field order, and ``diagnostics`` carries the
 reference's keys (``solver``, ``max_dim_factor``, ``max_iter``,
 ``hit_max_iter``, ``n_apply_low``, ``n_apply_full``) plus this path's own.
 
-Registered here: ``"davidson"`` (the B200 Davidson, float64 applies) and
-``"davidson_mixed"`` (float32 expansion applies, float64 certification). To
+Registered here: ``"davidson"`` (the B200 Davidson, float64 applies, TPA),
+``"davidson_fp32exp"`` (the reference's float32-expansion mode) and
+``"davidson_mixed"`` (float32 expansion applies with float64 certification and
+the learned preconditioner when its weights are present). To
 serve the reference's SCF loop, register the adapter into the reference's own
 registry: ``gradwave.solvers.registry.register("davidson", davidson_adapter,
 overwrite=True)``.
@@ -60,25 +62,35 @@ def is_registered(name: str) -> bool:
     return name in _REGISTRY
 
 
-def _adapter(mode: str):
+def _adapter(mode: str, learned: bool = False):
     def davidson_adapter(apply_H, X0, precond, mask, *, tol, nbands=None, max_iter: int = 40,
                          max_dim_factor: int = 4, **kw) -> EigResult:
         from .davidson import davidson_batched
+        pc = kw.pop("preconditioner", None)
+        if pc is None:
+            pc = "teter"
+            if learned:
+                from . import learned as lp
+                if lp.available():
+                    pc = lp.LearnedPreconditioner.load(device=X0.device)
+        m = kw.pop("mode", mode)
         r = davidson_batched(apply_H, X0, precond, mask, tol=tol, max_iter=max_iter,
-                             max_dim_factor=max_dim_factor, mode=kw.pop("mode", mode),
-                             precond=kw.pop("preconditioner", "teter"))
+                             max_dim_factor=max_dim_factor, mode=m, precond=pc)
         diag = {"solver": "davidson", "max_dim_factor": max_dim_factor, "max_iter": max_iter,
                 "hit_max_iter": r.n_iter >= max_iter, "n_apply_low": r.n_apply_low,
-                "n_apply_full": r.n_apply_full, "mode": mode}
+                "n_apply_full": r.n_apply_full, "mode": m,
+                "preconditioner": "teter" if isinstance(pc, str) else "learned"}
         diag.update(r.info)
         return EigResult(r.eigenvalues, r.eigenvectors, r.n_iter, r.residual_norms, diag)
 
-    davidson_adapter.__name__ = f"davidson_adapter_{mode}"
+    davidson_adapter.__name__ = f"davidson_adapter_{mode}{'_learned' if learned else ''}"
     return davidson_adapter
 
 
 davidson_adapter = _adapter("fp64")
-davidson_mixed_adapter = _adapter("fp32exp")
+davidson_fp32exp_adapter = _adapter("fp32exp")
+davidson_mixed_adapter = _adapter("mixed", learned=True)
 
 register("davidson", davidson_adapter)
+register("davidson_fp32exp", davidson_fp32exp_adapter)
 register("davidson_mixed", davidson_mixed_adapter)

@@ -237,8 +237,9 @@ typedef struct {
   int32_t nk, nb, npw;   /* block (nk, nb, npw) with npw = npw_max of the handle */
   int32_t max_dim;       /* basis capacity: min(max_dim_factor * nb, min_k npw), <= gwb_heev_max_dim() */
   int32_t max_iter;
-  int32_t mode;          /* 0: float64 applies; 1: float32 expansion applies with float64 certification */
-  int32_t precond;       /* 0: Teter-Payne-Allan */
+  int32_t mode;          /* 0: float64 applies; 1: float32 expansion applies with float64 certification
+                            (the reference's stall rule); 2: as 1, stall rule only near the float32 floor */
+  int32_t precond;       /* 0: Teter-Payne-Allan; 1: learned (model = MLP parameters), TPA per-band fallback */
   int32_t flags;         /* bit 0: time every H apply with CUDA events (stats->apply_ms) */
   double tol;            /* residual-norm gate [eV] */
   double t_max;          /* largest kinetic energy of the batch (float32 residual-floor estimate) */
@@ -259,7 +260,8 @@ int gwb_davidson_workspace_bytes(const gwb_davidson_params* p, size_t* bytes);
  * from the start block x0 (complex128, device): eig_out (nk, nb) ascending,
  * vec_out (nk, nb, npw) orthonormal rows with padded slots 0, rn_out (nk, nb)
  * residual norms; stats (HOST) gets the counters. t (nk, npw) kinetic diagonal,
- * mask (nk, npw) uint8. model must be NULL for precond 0. Returns GWB_OK also
+ * mask (nk, npw) uint8. model: float32 network parameters for precond 1
+ * (gwb_mlp_param_count values), ignored for precond 0. Returns GWB_OK also
  * when max_iter is hit (stats->hit_max_iter = 1), like the reference.
  * Replaces gradwave solvers/davidson.py:528-774 (davidson_batched) and the
  * registry adapter core of solvers/registry.py:154-182. */

@@ -130,7 +130,7 @@ def test_registry_adapters_and_two_stage(cuda_device):
         registry.register("davidson", registry.davidson_adapter)
     with pytest.raises(ValueError, match="registered"):
         registry.get("nope")
-    for name in ("davidson", "davidson_mixed"):
+    for name in ("davidson", "davidson_fp32exp", "davidson_mixed"):
         r = registry.get(name)(h.apply, x0, bk.t, bk.mask, tol=1e-10, nbands=ci.nbands, max_iter=200)
         assert isinstance(r, registry.EigResult)
         assert np.abs(r.eigenvalues.cpu().numpy() - g["eigenvalues"]).max() < EIG_TOL_HA

@@ -26,7 +26,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_registry_contract_without_gpu():
     from gradwave_b200 import registry
-    assert {"davidson", "davidson_mixed"} <= set(registry.available())
+    assert {"davidson", "davidson_fp32exp", "davidson_mixed"} <= set(registry.available())
     with pytest.raises(ValueError):
         registry.register("davidson", registry.davidson_adapter)
     registry.register("davidson", registry.davidson_adapter, overwrite=True)

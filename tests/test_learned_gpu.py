@@ -150,3 +150,40 @@ def test_committed_network_on_heldout_cell(cuda_device):
         assert np.abs(r.eigenvalues.cpu().numpy() - g["eigenvalues"]).max() < 1e-9
     print(json.dumps({"learned_iters": rl.n_iter, "tpa_iters": rt.n_iter,
                       "learned_applies": rl.n_apply_full, "tpa_applies": rt.n_apply_full}))
+
+
+def test_tensor_core_inference_matches_reference_forward(cuda_device):
+    """The mma.sync inference path of gwb_precond_learned against features +
+    the CUDA-core forward + TPA, on random parameters."""
+    from gradwave_b200 import _lib, learned
+    rng = np.random.default_rng(21)
+    nk, nb, npw, n_add = 2, 4, 1000, 3
+    x = rng.standard_normal((nk, nb, npw)) + 1j * rng.standard_normal((nk, nb, npw))
+    r = (rng.standard_normal((nk, nb, npw)) + 1j * rng.standard_normal((nk, nb, npw))) * rng.uniform(0, 2, npw)
+    t = np.abs(rng.standard_normal((nk, npw))) * 60
+    eig = rng.standard_normal((nk, nb)) * 5
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(cuda_device)
+    X, R, Tt, E = T(x), T(r), T(t), T(eig)
+    sel = torch.tensor([[1, 0, 3], [2, 3, 0]], dtype=torch.int32, device=cuda_device)
+    p = learned.init_params(4)
+    p[-65:] = rng.standard_normal(65).astype(np.float32) * 0.2
+    P = torch.from_numpy(p).to(cuda_device)
+    s = _lib.stream_ptr(cuda_device)
+    D = torch.zeros_like(X)
+    _lib.call("gwb_precond_learned", P.data_ptr(), nk, nb, n_add, npw, X.data_ptr(), nb * npw, R.data_ptr(),
+              nb * npw, Tt.data_ptr(), E.data_ptr(), sel.data_ptr(), None, D.data_ptr(), nb * npw, s)
+    F = torch.empty(nk, n_add, npw, 4, dtype=torch.float32, device=cuda_device)
+    _lib.call("gwb_precond_features", nk, nb, n_add, npw, X.data_ptr(), nb * npw, R.data_ptr(), nb * npw,
+              Tt.data_ptr(), E.data_ptr(), sel.data_ptr(), F.data_ptr(), s)
+    o = learned.forward(P, F.reshape(-1, 4)).view(nk, n_add, npw).double().clamp(-3, 3)
+    sl = sel.long().cpu().numpy()
+    xs = np.take_along_axis(x, sl[..., None], 1)
+    rs = np.take_along_axis(r, sl[..., None], 1)
+    tb = np.einsum("kag,kg,kag->ka", xs.conj(), t, xs).real
+    xx = t[:, None, :] / tb[..., None]
+    pp = 27 + 18 * xx + 12 * xx ** 2 + 8 * xx ** 3
+    tpa = pp / (pp + 16 * xx ** 4)
+    ref = rs * tpa * np.exp(o.cpu().numpy())
+    ref /= np.linalg.norm(ref, axis=-1, keepdims=True)
+    got = D.cpu().numpy()[:, :n_add]
+    assert np.abs(got - ref).max() <= 2e-2 * np.abs(ref).max()
