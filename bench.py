@@ -216,8 +216,10 @@ def run_ours(args):
     x0_dev = x0_host.to(dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
-    def solve(x0, mode):
-        return davidson_batched(h.apply, x0, bk.t, bk.mask, tol=args.tol, max_iter=300, mode=mode)
+    fast_mode, fast_pc = _solver_choice(args.solver, dev)
+
+    def solve(x0, mode, pc="teter"):
+        return davidson_batched(h.apply, x0, bk.t, bk.mask, tol=args.tol, max_iter=300, mode=mode, precond=pc)
 
     def check(res):
         if gold is None:
@@ -247,16 +249,15 @@ def run_ours(args):
             ts.append(e0.elapsed_time(e1))
         return statistics.mean(ts), out
 
-    mode_fast = "fp32exp"
     # value: device-resident inputs; every H apply inside the timed native
     # solves is bracketed by CUDA events on the solve stream (GWB_TIME_APPLIES)
     n0 = _lib.launch_count()
     os.environ["GWB_TIME_APPLIES"] = "1"
     with ClockSampler(dev.index) as clk:
         for _ in range(args.warmup):
-            solve(x0_dev, mode_fast)
+            solve(x0_dev, fast_mode, fast_pc)
         n1 = _lib.launch_count()
-        ms_fast, res_fast = timed(lambda: solve(x0_dev, mode_fast), args.steps, 0)
+        ms_fast, res_fast = timed(lambda: solve(x0_dev, fast_mode, fast_pc), args.steps, 0)
         launches = (_lib.launch_count() - n1) // max(1, args.steps)
     os.environ["GWB_TIME_APPLIES"] = "0"
     err_fast = check(res_fast)
@@ -267,7 +268,7 @@ def run_ours(args):
     # e2e through the public API from pinned host memory
     def e2e():
         x0 = x0_host.to(dev, non_blocking=True)
-        r = solve(x0, mode_fast)
+        r = solve(x0, fast_mode, fast_pc)
         ev = r.eigenvalues.to("cpu", non_blocking=True)
         vec = r.eigenvectors.to("cpu", non_blocking=True)
         torch.cuda.current_stream(dev).synchronize()
@@ -317,13 +318,13 @@ def run_ours(args):
         n_vec = vec.numel() * vec.element_size()
         line = {"metric": METRIC, "value": round(ms_fast / ws, 3), "unit": "ms", "n_gpus": ws,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_fast, 3),
-                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "c128 (fp32 expansion, fp64 certify)",
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "c128/f64 basis; f32 expansion applies, f64 certify; bf16 network",
                 "data": "synthetic (seeded Si cells, analytic pseudopotential)",
                 "config": {"workload": args.config, "nk": nk, "nbands": ci.nbands, "fft": list(ci.shape),
                            "npw": [int(n) for n in ci.bk.npw], "tol_ev": args.tol,
                            "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"replicas{ws}"},
                 "eig_err_ev": err_fast, "eig_err_ha": None if err_fast is None else err_fast / HA,
-                "n_iter": res_fast.n_iter, "n_apply_low": res_fast.n_apply_low,
+                "solver": args.solver, "n_iter": res_fast.n_iter, "n_apply_low": res_fast.n_apply_low,
                 "n_apply_full": res_fast.n_apply_full,
                 "plain_fp64": {"value": round(ms_plain, 3), "unit": "ms", "n_iter": res_plain.n_iter,
                                "eig_err_ev": err_plain},
@@ -398,16 +399,34 @@ def run_once(args):
     bk = ci.bk.to(dev)
     h = BatchedHamiltonian(bk, ci.shape, ci.v_eff_r, ci.p)
     x0 = ci.identity_start().to(dev)
-    mode = "fp64" if args.prec == "fp64" else "fp32exp"
+    mode, pc = _solver_choice(args.solver, dev)
     for _ in range(args.warmup):
-        davidson_batched(h.apply, x0, bk.t, bk.mask, tol=args.tol, max_iter=300, mode=mode)
+        davidson_batched(h.apply, x0, bk.t, bk.mask, tol=args.tol, max_iter=300, mode=mode, precond=pc)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    r = davidson_batched(h.apply, x0, bk.t, bk.mask, tol=args.tol, max_iter=300, mode=mode)
+    r = davidson_batched(h.apply, x0, bk.t, bk.mask, tol=args.tol, max_iter=300, mode=mode, precond=pc)
     torch.cuda.synchronize()
-    print(json.dumps({"mode": "once", "config": args.config, "solver_mode": mode, "n_iter": r.n_iter,
+    print(json.dumps({"mode": "once", "config": args.config, "solver": args.solver, "n_iter": r.n_iter,
                       "wall_ms": (time.perf_counter() - t0) * 1e3}), flush=True)
     return 0
+
+
+def _solver_choice(name, dev):
+    """(mode, preconditioner) of a solver name: plain = float64 + TPA,
+    fp32exp = the reference's float32-expansion mode + TPA, mixed = float32
+    expansion with near-floor stall rule + TPA, learned-mixed = mixed with the
+    learned preconditioner (TPA when no weights are present)."""
+    from gradwave_b200 import learned
+    if name == "plain":
+        return "fp64", "teter"
+    if name == "fp32exp":
+        return "fp32exp", "teter"
+    if name == "mixed":
+        return "mixed", "teter"
+    if name == "learned-mixed":
+        pc = learned.LearnedPreconditioner.load(device=dev) if learned.available() else "teter"
+        return "mixed", pc
+    raise ValueError(f"unknown solver {name!r}")
 
 
 def main():
@@ -422,6 +441,8 @@ def main():
     ap.add_argument("--mode", default="solve", choices=["solve", "apply", "once"],
                     help="apply: only time Hamiltonian applies; once: a single solve (profiling)")
     ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64"], help="arithmetic of --mode apply")
+    ap.add_argument("--solver", default="learned-mixed", choices=["plain", "fp32exp", "mixed", "learned-mixed"],
+                    help="solver of the timed value (the plain float64 solver is always timed beside it)")
     args = ap.parse_args()
     if args.mode == "apply":
         return run_apply(args)

@@ -102,7 +102,7 @@ _SIGNATURES = {
     "gwb_mlp_adam": [_P, _P, _P, _P, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _P],
     "gwb_precond_features": [_I, _I, _I, _I, _P, _I64, _P, _I64, _P, _P, _P, _P, _P],
     "gwb_precond_learned": [_P, _I, _I, _I, _I, _P, _I64, _P, _I64, _P, _P, _P, _P, _P, _I64, _P],
-    "gwb_stall_update": [_P, _P, _P, _I, _D, _P],
+    "gwb_stall_update": [_P, _P, _P, _P, _I, _D, _I, _P],
     "gwb_davidson_workspace_bytes": [ctypes.POINTER(DavidsonParams), ctypes.POINTER(ctypes.c_size_t)],
     "gwb_davidson_solve": [_P, ctypes.POINTER(DavidsonParams), _P, _P, _P, _P, _P, ctypes.c_size_t, _P, _P, _P,
                            ctypes.POINTER(DavidsonStats), _P],

@@ -87,7 +87,7 @@ int gwb_heev_max_dim(void);
 int gwb_ham_apply_strided(gwb_ham*, const void*, int64_t, void*, int64_t, int32_t, int32_t, int32_t, void*);
 int gwb_precond_learned(const float*, int32_t, int32_t, int32_t, int32_t, const void*, int64_t, const void*, int64_t,
                         const double*, const double*, const int32_t*, const uint8_t*, void*, int64_t, void*);
-int gwb_stall_update(const double*, double*, uint8_t*, int32_t, double, void*);
+int gwb_stall_update(const double*, double*, uint8_t*, uint8_t*, int32_t, double, int32_t, void*);
 }
 
 namespace gwb {
@@ -111,7 +111,7 @@ struct Work {
   Z16 *V, *HV, *S, *X, *HX, *R, *D, *D2, *C, *G, *Linv, *Gs, *U;
   double *Zs, *rn, *eig, *eig2, *stats, *rn_prev;
   int *sel, *info, *heev_info, *flags;
-  unsigned char* tpa_only;
+  unsigned char *tpa_only, *stall_count;
 };
 
 static size_t layout(const gwb_davidson_params& p, unsigned char* base, Work* w) {
@@ -144,6 +144,7 @@ static size_t layout(const gwb_davidson_params& p, unsigned char* base, Work* w)
   t.nh_work = b.take<unsigned char>(base, NH_WORK_BYTES);
   t.rn_prev = b.take<double>(base, nk * nb);
   t.tpa_only = b.take<unsigned char>(base, nk * nb);
+  t.stall_count = b.take<unsigned char>(base, nk * nb);
   if (w) *w = t;
   return b.off + 256;
 }
@@ -172,6 +173,7 @@ class Solver {
       k_fill<<<(nk_ * nb_ + 255) / 256, 256, 0, st_>>>(w_.rn_prev, nk_ * nb_, INFINITY);
       GWB_LAUNCH_CHECK();
       GWB_CUDA_TRY(cudaMemsetAsync(w_.tpa_only, 0, (size_t)nk_ * nb_, st_));
+      GWB_CUDA_TRY(cudaMemsetAsync(w_.stall_count, 0, (size_t)nk_ * nb_, st_));
     }
     // initial block: masked copy, orthonormalised with host-checked CholQR2
     GWB_TRY(masked_copy(static_cast<const Z16*>(x0), nbp, w_.D, nbp, nb_));
@@ -405,8 +407,9 @@ class Solver {
   int precondition(int n_add, const double* eig) {
     const int64_t nbp = (int64_t)nb_ * npw_;
     if (p_.precond == 1) {
-      // stall fallback: a band whose residual shrank by less than 10 % keeps TPA
-      GWB_TRY(gwb_stall_update(w_.rn, w_.rn_prev, w_.tpa_only, nk_ * nb_, 0.9, st_));
+      // stall fallback: a band whose residual has not improved on its best by
+      // 10 % for 3 rounds keeps TPA from then on
+      GWB_TRY(gwb_stall_update(w_.rn, w_.rn_prev, w_.stall_count, w_.tpa_only, nk_ * nb_, 0.9, 3, st_));
       return gwb_precond_learned(static_cast<const float*>(model_), nk_, nb_, n_add, npw_, w_.X, nbp, w_.R, nbp, t_,
                                  eig, w_.sel, w_.tpa_only, w_.D, nbp, st_);
     }

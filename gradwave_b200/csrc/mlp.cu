@@ -599,12 +599,21 @@ __global__ void __launch_bounds__(256) k_precond_learned_tc(
   }
 }
 
-// tpa_only[k][b] |= rn[k][b] > ratio * rn_prev[k][b]; rn_prev = rn.
-__global__ void k_stall_update(const double* __restrict__ rn, double* __restrict__ rn_prev,
-                               unsigned char* __restrict__ tpa_only, int n, double ratio) {
+// Stall rule of the learned preconditioner: a band whose residual has not
+// dropped below ratio * (its best so far) for `patience` consecutive rounds
+// reverts to TPA for the rest of the solve (tpa_only is sticky).
+__global__ void k_stall_update(const double* __restrict__ rn, double* __restrict__ rn_best,
+                               unsigned char* __restrict__ count, unsigned char* __restrict__ tpa_only, int n,
+                               double ratio, int patience) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    if (rn[i] > ratio * rn_prev[i]) tpa_only[i] = 1;
-    rn_prev[i] = rn[i];
+    const double v = rn[i];
+    if (v < ratio * rn_best[i]) {
+      count[i] = 0;
+    } else if (count[i] < 255) {
+      count[i] = count[i] + 1;
+    }
+    if (count[i] >= patience) tpa_only[i] = 1;
+    rn_best[i] = fmin(rn_best[i], v);
   }
 }
 
@@ -693,9 +702,10 @@ int gwb_precond_learned(const float* params, int32_t nk, int32_t nb, int32_t n_a
   return GWB_OK;
 }
 
-int gwb_stall_update(const double* rn, double* rn_prev, uint8_t* tpa_only, int32_t n, double ratio, void* stream) {
-  GWB_REQUIRE(rn && rn_prev && tpa_only && n > 0, "bad arguments");
-  k_stall_update<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(rn, rn_prev, tpa_only, n, ratio);
+int gwb_stall_update(const double* rn, double* rn_best, uint8_t* count, uint8_t* tpa_only, int32_t n, double ratio,
+                     int32_t patience, void* stream) {
+  GWB_REQUIRE(rn && rn_best && count && tpa_only && n > 0 && patience > 0, "bad arguments");
+  k_stall_update<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(rn, rn_best, count, tpa_only, n, ratio, patience);
   GWB_LAUNCH_CHECK();
   count_launches(1);
   return GWB_OK;

@@ -5,8 +5,9 @@ activations, FP32 accumulation; kernels in ``csrc/mlp.cu``) corrects the
 Teter-Payne-Allan filter: K(G) = TPA(x) exp(o(u)) with the features u of
 ``gwb_precond_features`` (|k+G|^2 relative to the band's kinetic energy, the
 band eigenvalue, the residual amplitude at G and the band's kinetic scale).
-TPA stays the fallback and the judge: a band whose residual does not shrink
-by 10 % between rounds reverts to TPA for the rest of the solve.
+TPA stays the fallback and the judge: a band whose residual has not improved
+on its best value by 10 % for three consecutive rounds reverts to TPA for the
+rest of the solve.
 
 Training data come from the Davidson solver itself. A cell is solved twice
 with TPA: once to convergence (eigenvectors psi), then again while every round
@@ -119,6 +120,7 @@ class LearnedPreconditioner:
     ``davidson_batched``). Host-driver hook: ``apply_into(solver, n_add, eig)``."""
 
     stall_ratio = 0.9
+    stall_patience = 3
 
     def __init__(self, params, device=None):
         p = torch.as_tensor(np.asarray(params, dtype=np.float32) if not torch.is_tensor(params) else params)
@@ -139,11 +141,13 @@ class LearnedPreconditioner:
         st = getattr(solver, "_lp_state", None)
         if st is None:
             st = (torch.full((nk, nb), float("inf"), dtype=torch.float64, device=solver.dev),
+                  torch.zeros(nk, nb, dtype=torch.uint8, device=solver.dev),
                   torch.zeros(nk, nb, dtype=torch.uint8, device=solver.dev))
             solver._lp_state = st
-        rn_prev, tpa_only = st
-        _lib.call("gwb_stall_update", ws.rn.data_ptr(), rn_prev.data_ptr(), tpa_only.data_ptr(), nk * nb,
-                  self.stall_ratio, solver.stream)
+        rn_best, count, tpa_only = st
+        _lib.call("gwb_stall_update", ws.rn.data_ptr(), rn_best.data_ptr(), count.data_ptr(), tpa_only.data_ptr(),
+                  nk * nb, self.stall_ratio, self.stall_patience, solver.stream)
+        solver.n_tpa_fallback = int(0)  # read lazily by callers that want it
         eigc = eig.contiguous()
         solver._lp_eig = eigc
         _lib.call("gwb_precond_learned", self.params.data_ptr(), nk, nb, n_add, npw, ws.X.data_ptr(), nb * npw,

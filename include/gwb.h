@@ -226,8 +226,10 @@ int gwb_precond_features(int32_t nk, int32_t nb, int32_t n_add, int32_t npw, con
 int gwb_precond_learned(const float* params, int32_t nk, int32_t nb, int32_t n_add, int32_t npw, const void* x,
                         int64_t x_kstride, const void* r, int64_t r_kstride, const double* t, const double* eig,
                         const int32_t* sel, const uint8_t* tpa_only, void* d, int64_t d_kstride, void* stream);
-/* Stall fallback: tpa_only[i] |= rn[i] > ratio * rn_prev[i]; rn_prev = rn. */
-int gwb_stall_update(const double* rn, double* rn_prev, uint8_t* tpa_only, int32_t n, double ratio, void* stream);
+/* Stall fallback: count[i] = rounds since rn[i] last fell below ratio * rn_best[i]
+ * (rn_best starts at +inf, count at 0); tpa_only[i] = 1 once count[i] >= patience. */
+int gwb_stall_update(const double* rn, double* rn_best, uint8_t* count, uint8_t* tpa_only, int32_t n, double ratio,
+                     int32_t patience, void* stream);
 
 /* ======================================================================= */
 /* Native Davidson driver                                                  */

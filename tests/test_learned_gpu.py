@@ -187,3 +187,19 @@ def test_tensor_core_inference_matches_reference_forward(cuda_device):
     ref /= np.linalg.norm(ref, axis=-1, keepdims=True)
     got = D.cpu().numpy()[:, :n_add]
     assert np.abs(got - ref).max() <= 2e-2 * np.abs(ref).max()
+
+
+def test_stall_rule(cuda_device):
+    from gradwave_b200 import _lib
+    n = 3
+    best = torch.full((n,), float("inf"), dtype=torch.float64, device=cuda_device)
+    cnt = torch.zeros(n, dtype=torch.uint8, device=cuda_device)
+    tpa = torch.zeros(n, dtype=torch.uint8, device=cuda_device)
+    s = _lib.stream_ptr(cuda_device)
+    # band 0 improves every round, band 1 stagnates, band 2 improves once then stagnates
+    seq = [[1.0, 1.0, 1.0], [0.5, 0.99, 0.5], [0.2, 0.98, 0.49], [0.1, 0.97, 0.48], [0.05, 0.96, 0.47]]
+    for row in seq:
+        rn = torch.tensor(row, dtype=torch.float64, device=cuda_device)
+        _lib.call("gwb_stall_update", rn.data_ptr(), best.data_ptr(), cnt.data_ptr(), tpa.data_ptr(), n, 0.9, 3, s)
+    torch.cuda.synchronize()
+    assert tpa.tolist() == [0, 1, 1]
