@@ -7,6 +7,7 @@ missing or CUDA is unavailable, every compute entry raises.
 from __future__ import annotations
 
 import ctypes
+import struct
 import threading
 from pathlib import Path
 
@@ -94,6 +95,7 @@ _SIGNATURES = {
     "gwb_row_repair": [_I, _I, _I, _P, _I64, _P, _D, _P, _P],
     "gwb_heev_lowest": [_I, _I, _I, _P, _I, _I64, _P, _P, _P, _P, _P],
     "gwb_heev_max_dim": [],
+    "gwb_heev_ql_count": [_P],
     "gwb_heev_lowest_noalloc": [_I, _I, _I, _P, _I, _I64, _P, _P, _P, _P],
     "gwb_mlp_param_count": [],
     "gwb_mlp_forward": [_P, _I, _P, _P, _P],
@@ -138,6 +140,23 @@ def load() -> ctypes.CDLL:
 def launch_count() -> int:
     """Kernels launched by libgwb.so in this process (cuBLAS/torch not included)."""
     return int(load().gwb_launch_count())
+
+
+def heev_diagnostics() -> dict:
+    """Subspace-eigensolver diagnostics on the current device: matrices sent to
+    the QL fallback by reason, and the largest residual / |T| measured on the
+    bisection path."""
+    out = (ctypes.c_ulonglong * 5)()
+    check(load().gwb_heev_ql_count(out))
+    maxres = struct.unpack("<d", struct.pack("<Q", out[4]))[0]
+    return {"ql_pool": int(out[0]), "ql_nonfinite": int(out[1]), "ql_cholqr": int(out[2]),
+            "ql_residual": int(out[3]), "max_residual_rel": maxres}
+
+
+def heev_ql_count() -> int:
+    """Matrices the subspace eigensolver solved on its QL fallback (current device)."""
+    d = heev_diagnostics()
+    return d["ql_pool"] + d["ql_nonfinite"] + d["ql_cholqr"] + d["ql_residual"]
 
 
 def check(status: int) -> None:

@@ -178,12 +178,20 @@ int gwb_row_repair(int32_t nk, int32_t n, int32_t npw, void* D, int64_t d_kstrid
 /* Lowest nb eigenpairs of nk Hermitian m x m matrices S (leading dim lds,
  * both triangles filled), float64: eig (nk, nb) ascending, U (nk, m, nb)
  * row-major eigenvector columns; zscratch (nk, m*m) float64; info[k] = 1 when
- * the QL iteration limit was hit. m <= gwb_heev_max_dim(). Householder
- * tridiagonalisation + implicit QL + back-transform, one CTA per matrix.
+ * the QL iteration limit was hit. m <= gwb_heev_max_dim(). One CTA per
+ * matrix: Householder tridiagonalisation, Sturm-count multisection for the
+ * nb eigenvalues, inverse iteration + CholQR2 + Jacobi Rayleigh-Ritz for the
+ * vectors, residual-checked, with implicit QL as the fallback; back-transform.
  * Replaces torch.linalg.eigh in gradwave solvers/davidson.py:66-75,650. */
 int gwb_heev_lowest(int32_t nk, int32_t m, int32_t nb, const void* S, int32_t lds, int64_t s_kstride,
                     double* eig, void* U, double* zscratch, int32_t* info, void* stream);
 int gwb_heev_max_dim(void);
+/* Diagnostics of gwb_heev_lowest on the current device since load: out[0..3]
+ * matrices sent down the QL fallback by reason (pool too small for the
+ * bisection path, non-finite inverse iterate, CholQR breakdown, residual
+ * above 64 eps |T|), out[4] the bits of the largest residual / |T| the
+ * bisection path measured. No counterpart in the reference. */
+int gwb_heev_ql_count(unsigned long long* out);
 
 /* gwb_heev_lowest without any device allocation: the caller passes inputs and
  * outputs only, and the eigenvector scratch lives in a fixed 8 MiB device
