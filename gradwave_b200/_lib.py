@@ -95,6 +95,7 @@ _SIGNATURES = {
     "gwb_row_repair": [_I, _I, _I, _P, _I64, _P, _D, _P, _P],
     "gwb_heev_lowest": [_I, _I, _I, _P, _I, _I64, _P, _P, _P, _P, _P],
     "gwb_heev_max_dim": [],
+    "gwb_heev_scratch_doubles": [_I],
     "gwb_heev_ql_count": [_P],
     "gwb_heev_lowest_noalloc": [_I, _I, _I, _P, _I, _I64, _P, _P, _P, _P],
     "gwb_mlp_param_count": [],
@@ -111,7 +112,7 @@ _SIGNATURES = {
 }
 _RESTYPES = {"gwb_last_error": ctypes.c_char_p, "gwb_version": ctypes.c_char_p,
              "gwb_launch_count": ctypes.c_ulonglong,
-             "gwb_ham_scratch_bytes": ctypes.c_size_t}
+             "gwb_ham_scratch_bytes": ctypes.c_size_t, "gwb_heev_scratch_doubles": ctypes.c_int64}
 
 
 def declared_symbols() -> list[str]:

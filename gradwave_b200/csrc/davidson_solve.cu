@@ -132,7 +132,7 @@ static size_t layout(const gwb_davidson_params& p, unsigned char* base, Work* w)
   t.Linv = b.take<Z16>(base, nk * nb * nb);
   t.Gs = b.take<Z16>(base, nk * nb * nb);
   t.U = b.take<Z16>(base, nk * std::max(hm, nb) * nb);
-  t.Zs = b.take<double>(base, nk * hm * hm);
+  t.Zs = b.take<double>(base, nk * hm * (hm + 8));
   t.rn = b.take<double>(base, nk * nb);
   t.eig = b.take<double>(base, nk * nb);
   t.eig2 = b.take<double>(base, nk * nb);

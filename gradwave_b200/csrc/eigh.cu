@@ -1,36 +1,43 @@
 // Batched float64 Hermitian eigensolver for the Davidson subspace matrices
 // (replaces torch.linalg.eigh in gradwave solvers/davidson.py:66-75,650):
-// the lowest nb eigenpairs of each m x m matrix, ascending.
+// the lowest nb eigenpairs of each m x m matrix, ascending. Two kernels, one
+// CTA per matrix, everything in shared memory (m <= GWB_HEEV_MMAX):
 //
-// One CTA per matrix, the matrix in shared memory (m <= GWB_HEEV_MMAX):
+// k_heev_tridiag (512 threads)
 //   1. Householder tridiagonalisation with Hermitian reflectors
 //      P_j = I - w_j u_j u_j^H, A <- P_j A P_j (Golub & Van Loan, Matrix
-//      Computations, 4th ed., sec. 8.3.1, complex form), two block barriers
-//      per column: the u^H p reduction rides on the matrix-vector pass and the
-//      next column's norm on the rank-2 update. The complex subdiagonal is
-//      made real by a diagonal phase D (T = D T_r D^H); the reflectors are
-//      then packed into the front of the matrix storage and the rest of it
-//      becomes the working pool of the stages below.
-//   2. Eigenvalues lambda_0..lambda_{nb-1} of T_r by multisection on Sturm
+//      Computations, 4th ed., sec. 8.3.1, complex form) on the lower triangle,
+//      two block barriers per column. Reflectors, diagonal, complex
+//      subdiagonal and scales go to the caller's scratch.
+// k_heev_lowest (256 threads)
+//   The complex subdiagonal is made real by a diagonal phase D (T = D T_r D^H);
+//   the packed reflectors sit at the front of the shared memory and the rest
+//   is the working pool of:
+//   2. Eigenvalues lambda_0..lambda_{nb+3} of T_r by multisection on Sturm
 //      counts (8 lanes per eigenvalue, 9 sub-intervals per round). The count
 //      is the number of sign changes of the leading principal minors
 //      p_i = (d_i - x) p_{i-1} - e_{i-1}^2 p_{i-2}, rescaled by powers of two;
 //      the computed count is exact for T_r with each e_i^2 perturbed by a few
 //      ulps (Wilkinson, The Algebraic Eigenvalue Problem, ch. 5, secs. 37-40;
-//      Barth, Martin & Wilkinson, Numer. Math. 9 (1967) 386).
-//   3. Eigenvectors of T_r by two steps of inverse iteration per eigenvalue
-//      (one thread each; Gaussian elimination with partial pivoting of the
-//      tridiagonal T_r - lambda I, zero pivots lifted to eps |T|; seeded random
-//      start vectors, so the vectors of a degenerate cluster span it).
-//   4. CholQR2 of those vectors, then Rayleigh-Ritz: H = Z^T T_r Z, a cyclic
-//      Jacobi sweep on H (Golub & Van Loan sec. 8.5.2) that only rotates
-//      pairs with |H_pq| > 2 eps |T| (the clusters), eigenvalues diag(H).
-//   5. y = Q D Z q, one warp per eigenvector; each warp also measures the
-//      residual |T_r v - theta v|. If any step fails (non-finite iterate,
-//      Cholesky breakdown, residual above 64 eps |T|) or the pool is too small
-//      for stages 3-4, the CTA redoes stage 2-5 with implicit QL on T_r
-//      (Bowdler, Martin, Reinsch & Wilkinson, Numer. Math. 11 (1968), tql2),
-//      whose rotations one thread logs and every thread replays on Z.
+//      Barth, Martin & Wilkinson, Numer. Math. 9 (1967) 386). The wanted set
+//      grows past nb while the next eigenvalue belongs to the same cluster.
+//   3. Eigenvectors of T_r by three steps of inverse iteration (one thread per
+//      vector; Gaussian elimination with partial pivoting of T_r - shift I,
+//      factored once, zero pivots lifted to eps |T|; seeded random starts).
+//      Eigenvalues closer than 1e4 x the bisection width form a cluster that
+//      shares one shift just below it and is Gram-Schmidt orthonormalised
+//      after every step, so its vectors span its invariant subspace.
+//   4. Newton-Schulz orthonormalisation Z <- Z (3I - Z^T Z)/2, then
+//      Rayleigh-Ritz: H = Z^T T_r Z and a cyclic Jacobi sweep on H (Golub &
+//      Van Loan sec. 8.5.2) that rotates only pairs above eps |T| / 2 (the
+//      clusters); the Ritz values diag(H) are the eigenvalues.
+//   5. y = Q D Z q: each warp carries four eigenvectors through the
+//      reflectors and measures |T_r v - theta v|. If any step fails (non-finite
+//      iterate, orthonormalisation not converging, residual above 64 eps |T|)
+//      or the pool is too small for stages 3-4, the CTA redoes stages 2-5 with
+//      implicit QL on T_r (Bowdler, Martin, Reinsch & Wilkinson, Numer. Math.
+//      11 (1968), tql2), whose rotations one thread logs and every thread
+//      replays on Z.
 // Every loop is bounded: a QL iteration cap reports info = 1.
 #include <cmath>
 
@@ -63,7 +70,7 @@ __host__ __device__ inline size_t heev_h_doubles(int m) { return (size_t)m * (m 
 // float64 the bisection/inverse-iteration path wants in the pool.
 __host__ __device__ inline size_t heev_fast_need(int m, int nb) {
   const size_t ldz = (size_t)(m | 1);
-  const size_t a = 2 * (size_t)m * nb, b = 2 * (size_t)nb * nb;
+  const size_t a = 3 * (size_t)m * nb, b = 2 * (size_t)nb * nb;
   return nb * ldz + (a > b ? a : b);
 }
 // offset of reflector j in the packed layout (complex units): rows j+1..m-1
@@ -100,70 +107,280 @@ __device__ __forceinline__ double hash_pm1(unsigned long long x) {
 }
 
 // Number of eigenvalues of the real tridiagonal (d, e) below x: sign changes
-// of the leading principal minors, rescaled by 2^-+400 every fourth step (the
-// minors grow by at most |d_i - x| + e_i^2 per step).
+// of the leading principal minors,
+// rescaled by 2^-+400 after every fourth step (the minors grow by at most
+// |d_i - x| + e_i^2 per step).
+__device__ __forceinline__ void sturm_step(double di, double e2i, double x, double& p0, double& p1, int& cnt) {
+  constexpr double TINY = 0x1.0p-100;
+  double p2 = fma(di - x, p1, -e2i * p0);
+  if (p2 == 0.0) p2 = -TINY * p1;  // a zero minor takes the sign opposite to its predecessor
+  cnt += (p2 < 0.0) != (p1 < 0.0);
+  p0 = p1;
+  p1 = p2;
+}
+__device__ __forceinline__ void sturm_rescale(double& p0, double& p1) {
+  constexpr double BIG = 0x1.0p400, SMALL = 0x1.0p-400;
+  const double mx = fmax(fabs(p0), fabs(p1));
+  if (mx > BIG) {
+    p0 *= SMALL;
+    p1 *= SMALL;
+  } else if (mx < SMALL) {
+    p0 *= BIG;
+    p1 *= BIG;
+  }
+}
 __device__ __forceinline__ int sturm_count(const double* __restrict__ d, const double* __restrict__ e2, int m,
                                            double x) {
-  constexpr double BIG = 0x1.0p400, SMALL = 0x1.0p-400, TINY = 0x1.0p-100;
+  constexpr double TINY = 0x1.0p-100;
   double p0 = 1.0, p1 = d[0] - x;
   if (p1 == 0.0) p1 = -TINY;
   int cnt = p1 < 0.0;
-  for (int i = 1; i < m; ++i) {
-    double p2 = fma(d[i] - x, p1, -e2[i - 1] * p0);
-    if (p2 == 0.0) p2 = -TINY * p1;  // a zero minor takes the sign opposite to its predecessor
-    cnt += (p2 < 0.0) != (p1 < 0.0);
-    p0 = p1;
-    p1 = p2;
-    if ((i & 3) == 0) {
-      const double mx = fmax(fabs(p0), fabs(p1));
-      if (mx > BIG) {
-        p0 *= SMALL;
-        p1 *= SMALL;
-      } else if (mx < SMALL) {
-        p0 *= BIG;
-        p1 *= BIG;
-      }
+  int i = 1;
+  for (; i + 3 < m; i += 4) {
+    double dd[4], ee[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      dd[q] = d[i + q];
+      ee[q] = e2[i + q - 1];
     }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) sturm_step(dd[q], ee[q], x, p0, p1, cnt);
+    sturm_rescale(p0, p1);
   }
+  for (; i < m; ++i) sturm_step(d[i], e2[i - 1], x, p0, p1, cnt);
   return cnt;
 }
 
-// Reflectors applied to one eigenvector held by a warp: y <- Q y with
+// Reflectors applied to NV eigenvectors held by a warp (interleaved, so the
+// warp reductions of the NV dot products overlap): y <- Q y with
 // Q = P_0 ... P_{m-3}; Hc the packed reflectors, wv their scales.
-__device__ __forceinline__ void apply_reflectors(cplx<double> (&y)[PER], int m, int lane,
+template <int NV>
+__device__ __forceinline__ void apply_reflectors(cplx<double> (&y)[NV][PER], int m, int lane,
                                                  const cplx<double>* __restrict__ Hc, const double* __restrict__ wv) {
   for (int j = m - 3; j >= 0; --j) {
     const double w = wv[j];
     if (w == 0.0) continue;
     const cplx<double>* u = Hc + hoff(m, j) - (j + 1);  // u[r] for r > j
-    cplx<double> dot = mk<double>(0.0, 0.0);
+    cplx<double> uu[PER];
 #pragma unroll
     for (int t = 0; t < PER; ++t) {
       const int r = lane + 32 * t;
-      if (r > j && r < m) dot = dot + conj_mul(u[r], y[t]);
+      uu[t] = (r > j && r < m) ? u[r] : mk<double>(0.0, 0.0);
     }
-    for (int o = 16; o > 0; o >>= 1) {
-      dot.x += __shfl_xor_sync(0xffffffffu, dot.x, o);
-      dot.y += __shfl_xor_sync(0xffffffffu, dot.y, o);
-    }
-    dot = scale(dot, w);
+    const int t0 = (j + 1) >> 5;  // slots below t0 hold rows <= j only (warp-uniform)
+    cplx<double> dot[NV];
 #pragma unroll
-    for (int t = 0; t < PER; ++t) {
-      const int r = lane + 32 * t;
-      if (r > j && r < m) y[t] = y[t] - u[r] * dot;
+    for (int v = 0; v < NV; ++v) {
+      dot[v] = mk<double>(0.0, 0.0);
+#pragma unroll
+      for (int t = 0; t < PER; ++t)
+        if (t >= t0) dot[v] = dot[v] + conj_mul(uu[t], y[v][t]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        dot[v].x += __shfl_xor_sync(0xffffffffu, dot[v].x, o);
+        dot[v].y += __shfl_xor_sync(0xffffffffu, dot[v].y, o);
+      }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const cplx<double> dw = scale(dot[v], w);
+#pragma unroll
+      for (int t = 0; t < PER; ++t)
+        if (t >= t0) y[v][t] = y[v][t] - uu[t] * dw;
     }
   }
 }
 
-// S (nk, lds, lds) row-major Hermitian (both triangles filled), leading m x m.
-// eig (nk, nb) ascending; U (nk, m, nb) row-major eigenvector columns;
-// Zg scratch (nk, m, m) float64 (reflector staging, QL rotation log); info (nk).
-// extra: float64 of shared memory added to the pool beyond the matrix storage.
-__global__ void __launch_bounds__(HEEV_THREADS, 1)
-    k_heev_lowest(const cplx<double>* __restrict__ S, int lds, int64_t sk, int m, int nb, double* __restrict__ eig,
-                  cplx<double>* __restrict__ U, double* __restrict__ Zg, int* __restrict__ info, int extra) {
+// Per-matrix float64 scratch of the eigensolver: packed reflectors
+// (heev_h_doubles), then d (m), the complex subdiagonal (2m), the reflector
+// scales (m); the QL rotation log reuses the first m*m.
+__host__ __device__ inline size_t heev_scratch_doubles(int m) { return (size_t)m * (m + 8); }
+
+constexpr int TRI_THREADS = 512;
+constexpr int TRI_WARPS = TRI_THREADS / 32;
+
+// Stage 1 alone, 512 threads per matrix: Householder tridiagonalisation of the
+// lower triangle (the rank-2 update touches c <= r only; the matrix-vector
+// product reads A[r][c] for c <= r and conj(A[c][r]) above). The column the
+// next reflector is built from is copied to a contiguous buffer by the update
+// that finalises it. Output per matrix in Zg: reflector j (u_0 first, rows
+// j+1..m-1) at complex offset hoff(j), then d, the complex subdiagonal and the
+// reflector scales w_j (0 where a column needed no reflector).
+__global__ void __launch_bounds__(TRI_THREADS, 1)
+    k_heev_tridiag(const cplx<double>* __restrict__ S, int lds, int64_t sk, int m, double* __restrict__ Zg) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int lda = m + 1;  // padded row stride of A in shared memory
+  const int lda = m + 1;
+  cplx<double>* A = reinterpret_cast<cplx<double>*>(smem_raw);  // m*lda, lower triangle
+  cplx<double>* pv = A + m * lda;                                // m
+  cplx<double>* ucol = pv + m;                                   // 2m: raw column j below the diagonal, by parity
+  __shared__ double red[TRI_WARPS];
+  __shared__ double red1[TRI_WARPS];
+  __shared__ double red2[2][TRI_WARPS];
+  const int k = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const cplx<double>* Sk = S + k * sk;
+  double* Zk = Zg + (int64_t)k * heev_scratch_doubles(m);
+  double* o_d = Zk + heev_h_doubles(m);
+  double* o_ec = o_d + m;
+  double* o_wv = o_ec + 2 * m;
+
+  for (int r = warp; r < m; r += TRI_WARPS)
+    for (int c = lane; c <= r; c += 32) A[r * lda + c] = Sk[(int64_t)r * lds + c];
+  double v0 = 0.0;
+  for (int i = tid; i + 1 < m; i += TRI_THREADS) {
+    const cplx<double> a = Sk[(int64_t)(i + 1) * lds];
+    ucol[i] = a;
+    v0 += norm2(a);
+  }
+  v0 = warp_sum(v0);
+  if (lane == 0) red[warp] = v0;
+  __syncthreads();
+  double s2 = 0.0;
+#pragma unroll
+  for (int q = 0; q < TRI_WARPS; ++q) s2 += red[q];
+
+  for (int j = 0; j + 2 < m; ++j) {
+    const int r0 = j + 1, nr = m - r0, par = j & 1;
+    const cplx<double>* uc_ = ucol + par * m;  // uc_[i] = A[r0 + i][j], i < nr
+    cplx<double>* un_ = ucol + (par ^ 1) * m;  // next: A[r0 + 1 + i][r0], i < nr - 1
+    if (s2 == 0.0) {  // column already reduced: no reflector
+      if (tid == 0) {
+        o_d[j] = A[j * lda + j].x;
+        o_wv[j] = 0.0;
+        o_ec[2 * j] = 0.0;
+        o_ec[2 * j + 1] = 0.0;
+      }
+      double v = 0.0;
+      for (int i = tid; i + 1 < nr; i += TRI_THREADS) {
+        const cplx<double> a = A[(r0 + 1 + i) * lda + r0];
+        un_[i] = a;
+        v += norm2(a);
+      }
+      v = warp_sum(v);
+      if (lane == 0) red2[par][warp] = v;
+      __syncthreads();
+      s2 = 0.0;
+#pragma unroll
+      for (int q = 0; q < TRI_WARPS; ++q) s2 += red2[par][q];
+      continue;
+    }
+    const double sig = sqrt(s2);
+    const cplx<double> x0 = uc_[0];
+    const double a0 = sqrt(norm2(x0));
+    const cplx<double> phs = a0 > 0.0 ? scale(x0, 1.0 / a0) : mk<double>(1.0, 0.0);
+    const double w = 1.0 / (sig * (sig + a0));
+    const cplx<double> u0 = x0 + scale(phs, sig);
+    // p_r = w sum_c A[r][c] u_c, eight threads per row
+    constexpr int TPR = 8;
+    double kpart = 0.0;
+    for (int b0 = 0; b0 < nr * TPR; b0 += TRI_THREADS) {
+      const int bi = b0 + tid;
+      const int rr = bi / TPR, part = bi % TPR;
+      cplx<double> acc = mk<double>(0.0, 0.0);
+      if (rr < nr) {
+        const int r = r0 + rr;
+        for (int c = r0 + part; c < m; c += TPR) {
+          const cplx<double> uc = c == r0 ? u0 : uc_[c - r0];
+          const cplx<double> a = c <= r ? A[r * lda + c] : conj(A[c * lda + r]);
+          acc = acc + a * uc;
+        }
+      }
+#pragma unroll
+      for (int o = 1; o < TPR; o <<= 1) {
+        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+      }
+      if (rr < nr && part == 0) {
+        const cplx<double> p = scale(acc, w);
+        pv[rr] = p;
+        const cplx<double> ur = rr == 0 ? u0 : uc_[rr];
+        kpart += ur.x * p.x + ur.y * p.y;
+      }
+    }
+    kpart = warp_sum(kpart);
+    if (lane == 0) red1[warp] = kpart;
+    __syncthreads();  // pv, red1 complete
+    double kk = 0.0;
+#pragma unroll
+    for (int q = 0; q < TRI_WARPS; ++q) kk += red1[q];
+    kk *= 0.5 * w;
+    // lower triangle: A <- A - u q^H - q u^H with q = p - kk u; warps over rows,
+    // lanes over columns c <= r with u_c, q_c in registers
+    double s2p = 0.0;
+    {
+      cplx<double> ucs[PER], qcs[PER];
+#pragma unroll
+      for (int t = 0; t < PER; ++t) {
+        const int cc = lane + 32 * t;
+        ucs[t] = cc == 0 ? u0 : (cc < nr ? uc_[cc] : mk<double>(0.0, 0.0));
+        qcs[t] = cc < nr ? pv[cc] - scale(ucs[t], kk) : mk<double>(0.0, 0.0);
+      }
+      for (int rr = warp; rr < nr; rr += TRI_WARPS) {
+        const cplx<double> ur = rr == 0 ? u0 : uc_[rr];
+        const cplx<double> qr = pv[rr] - scale(ur, kk);
+        cplx<double>* arow = A + (r0 + rr) * lda + r0;
+#pragma unroll
+        for (int t = 0; t < PER; ++t) {
+          const int cc = lane + 32 * t;
+          if (cc <= rr) {
+            const cplx<double> an = arow[cc] - mul_conj(ur, qcs[t]) - mul_conj(qr, ucs[t]);
+            arow[cc] = an;
+            if (cc == 0 && rr > 0) {
+              s2p += norm2(an);
+              un_[rr - 1] = an;
+            }
+          }
+        }
+      }
+    }
+    // reflector j to the scratch (u_0 first), as doubles: the per-matrix base
+    // is only 8-byte aligned
+    {
+      const int o = hoff(m, j);
+      for (int i = tid; i < nr; i += TRI_THREADS) {
+        const cplx<double> u = i == 0 ? u0 : uc_[i];
+        Zk[2 * (o + i)] = u.x;
+        Zk[2 * (o + i) + 1] = u.y;
+      }
+    }
+    if (tid == 0) {
+      o_d[j] = A[j * lda + j].x;
+      o_wv[j] = w;
+      o_ec[2 * j] = -phs.x * sig;
+      o_ec[2 * j + 1] = -phs.y * sig;
+    }
+    s2p = warp_sum(s2p);
+    if (lane == 0) red2[par][warp] = s2p;
+    __syncthreads();  // update complete
+    s2 = 0.0;
+#pragma unroll
+    for (int q = 0; q < TRI_WARPS; ++q) s2 += red2[par][q];
+  }
+  if (tid == 0) {
+    if (m >= 2) {
+      o_d[m - 2] = A[(m - 2) * lda + m - 2].x;
+      const cplx<double> e = A[(m - 1) * lda + m - 2];
+      o_ec[2 * (m - 2)] = e.x;
+      o_ec[2 * (m - 2) + 1] = e.y;
+      o_wv[m - 2] = 0.0;
+    }
+    o_d[m - 1] = A[(m - 1) * lda + m - 1].x;
+    o_ec[2 * (m - 1)] = 0.0;
+    o_ec[2 * (m - 1) + 1] = 0.0;
+    o_wv[m - 1] = 0.0;
+  }
+}
+static size_t tri_smem(int m) { return ((size_t)m * (m + 1) + 3 * (size_t)m) * 16; }
+
+// Stages 2-5 on the output of k_heev_tridiag in Zg (nk, heev_scratch_doubles(m));
+// eig (nk, nb) ascending; U (nk, m, nb) row-major eigenvector columns; info
+// (nk). extra: float64 of shared memory added to the pool beyond the matrix
+// storage.
+__global__ void __launch_bounds__(HEEV_THREADS, 1)
+    k_heev_lowest(int m, int nb, double* __restrict__ eig, cplx<double>* __restrict__ U, double* __restrict__ Zg,
+                  int* __restrict__ info, int extra) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<double>* A = reinterpret_cast<cplx<double>*>(smem_raw);  // m*lda, later packed reflectors + pool
   double* Ad = reinterpret_cast<double*>(smem_raw);
   unsigned char* base = smem_raw + (heev_a_doubles(m) + (size_t)extra) * 8;
@@ -176,118 +393,30 @@ __global__ void __launch_bounds__(HEEV_THREADS, 1)
   double* e2 = wv + m;                                       // m  er^2
   double* lam = e2 + m;                                      // m  eigenvalues (ascending)
   int* order = reinterpret_cast<int*>(lam + m);              // m
-  __shared__ double red[HEEV_WARPS];
-  __shared__ double red1[HEEV_WARPS];
-  __shared__ double red2[2][HEEV_WARPS];
   __shared__ double s_rng[2][HEEV_WARPS];
   __shared__ int s_ctl[4];  // 0: QL log count, 2: QL done, 3: QL failed
   __shared__ int s_fail;  // reason + 1 of a bisection-path failure
   const int k = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const cplx<double>* Sk = S + k * sk;
-  double* Zglob = Zg + (int64_t)k * m * m;
+  double* Zglob = Zg + (int64_t)k * heev_scratch_doubles(m);
 
-  for (int i = tid; i < m * m; i += blockDim.x) A[(i / m) * lda + (i % m)] = Sk[(int64_t)(i / m) * lds + (i % m)];
+  // stage 1 output (k_heev_tridiag): packed reflectors into the front of the
+  // matrix storage, d, the complex subdiagonal and the reflector scales
+  cplx<double>* Hc = A;
+  {
+    const int hcount = m >= 3 ? hoff(m, m - 2) : 0;
+    const double* o_d = Zglob + heev_h_doubles(m);
+    const double* o_ec = o_d + m;
+    const double* o_wv = o_ec + 2 * m;
+    for (int i = tid; i < hcount; i += blockDim.x) Hc[i] = mk<double>(Zglob[2 * i], Zglob[2 * i + 1]);
+    for (int i = tid; i < m; i += blockDim.x) {
+      d[i] = o_d[i];
+      ec[i] = mk<double>(o_ec[2 * i], o_ec[2 * i + 1]);
+      wv[i] = o_wv[i];
+    }
+  }
   if (tid == 0) s_fail = 0;
   __syncthreads();
-
-  // ---- 1. tridiagonalisation ---------------------------------------------
-  double s2 = 0.0;
-  {
-    double v = 0.0;
-    for (int r = 1 + tid; r < m; r += blockDim.x) v += norm2(A[r * lda]);
-    s2 = blk_sum(v, red);
-  }
-  for (int j = 0; j + 2 < m; ++j) {
-    const int r0 = j + 1, nr = m - r0;
-    const int par = j & 1;
-    if (s2 == 0.0) {  // column already reduced: no reflector
-      if (tid == 0) {
-        d[j] = A[j * lda + j].x;
-        wv[j] = 0.0;
-        ec[j] = mk<double>(0.0, 0.0);
-      }
-      double v = 0.0;
-      for (int r = j + 2 + tid; r < m; r += blockDim.x) v += norm2(A[r * lda + j + 1]);
-      v = warp_sum(v);
-      if (lane == 0) red2[par][warp] = v;
-      __syncthreads();
-      s2 = 0.0;
-#pragma unroll
-      for (int w = 0; w < HEEV_WARPS; ++w) s2 += red2[par][w];
-      continue;
-    }
-    const double sig = sqrt(s2);
-    const cplx<double> x0 = A[r0 * lda + j];
-    const double a0 = sqrt(norm2(x0));
-    const cplx<double> phs = a0 > 0.0 ? scale(x0, 1.0 / a0) : mk<double>(1.0, 0.0);
-    const double w = 1.0 / (sig * (sig + a0));
-    const cplx<double> u0 = x0 + scale(phs, sig);  // u = column j below the diagonal, first entry u0
-    // p_r = w sum_c A[r][c] u_c = w sum_c conj(A[c][r]) u_c, TPR threads per row;
-    // the same pass accumulates Re(u^H p)
-    constexpr int TPR = 4;
-    double kpart = 0.0;
-    for (int b0 = 0; b0 < nr * TPR; b0 += blockDim.x) {
-      const int bi = b0 + tid;
-      const int rr = bi / TPR, part = bi % TPR;
-      cplx<double> acc = mk<double>(0.0, 0.0);
-      if (rr < nr) {
-        const int r = r0 + rr;
-        for (int c = r0 + part; c < m; c += TPR) {
-          const cplx<double> uc = c == r0 ? u0 : A[c * lda + j];
-          acc = acc + conj_mul(A[c * lda + r], uc);
-        }
-      }
-      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
-      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
-      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 2);
-      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 2);
-      if (rr < nr && part == 0) {
-        const cplx<double> p = scale(acc, w);
-        pv[rr] = p;
-        const cplx<double> ur = rr == 0 ? u0 : A[(r0 + rr) * lda + j];
-        kpart += ur.x * p.x + ur.y * p.y;
-      }
-    }
-    kpart = warp_sum(kpart);
-    if (lane == 0) red1[warp] = kpart;
-    __syncthreads();  // pv, red1 complete
-    double kk = 0.0;
-#pragma unroll
-    for (int q = 0; q < HEEV_WARPS; ++q) kk += red1[q];
-    kk *= 0.5 * w;
-    // A <- A - u q^H - q u^H with q = p - kk u; the norm of the next column
-    // (column r0, rows > r0) is summed from the updated entries
-    double s2p = 0.0;
-    for (int idx = tid; idx < nr * nr; idx += blockDim.x) {
-      const int rr = idx / nr, cc = idx - rr * nr;
-      const cplx<double> ur = rr == 0 ? u0 : A[(r0 + rr) * lda + j];
-      const cplx<double> uc = cc == 0 ? u0 : A[(r0 + cc) * lda + j];
-      const cplx<double> qr = pv[rr] - scale(ur, kk), qc = pv[cc] - scale(uc, kk);
-      cplx<double>& a = A[(r0 + rr) * lda + r0 + cc];
-      const cplx<double> an = a - mul_conj(ur, qc) - mul_conj(qr, uc);
-      a = an;
-      if (cc == 0 && rr > 0) s2p += norm2(an);
-    }
-    if (tid == 0) {  // nobody reads A[r0][j] in this phase (u0 is in registers)
-      d[j] = A[j * lda + j].x;
-      wv[j] = w;
-      ec[j] = scale(phs, -sig);
-      A[r0 * lda + j] = u0;
-    }
-    s2p = warp_sum(s2p);
-    if (lane == 0) red2[par][warp] = s2p;
-    __syncthreads();  // update complete
-    s2 = 0.0;
-#pragma unroll
-    for (int q = 0; q < HEEV_WARPS; ++q) s2 += red2[par][q];
-  }
   if (tid == 0) {
-    if (m >= 2) {
-      d[m - 2] = A[(m - 2) * lda + m - 2].x;
-      ec[m - 2] = A[(m - 1) * lda + m - 2];
-      if (m == 2) wv[0] = 0.0;
-    }
-    d[m - 1] = A[(m - 1) * lda + m - 1].x;
     // phases making the subdiagonal real: ph[j+1] = ph[j] e_j / |e_j|
     ph[0] = mk<double>(1.0, 0.0);
     for (int j = 0; j + 1 < m; ++j) {
@@ -297,22 +426,7 @@ __global__ void __launch_bounds__(HEEV_THREADS, 1)
     }
     er[m - 1] = 0.0;
   }
-  // pack the reflectors (column j, rows j+1..m-1, j <= m-3) at the front of
-  // the matrix storage, staged through the global scratch (as plain doubles:
-  // the per-matrix offset k*m*m is only 8-byte aligned for odd m)
-  double* stage = Zglob;
-  const int hcount = m >= 3 ? hoff(m, m - 2) : 0;
-  for (int idx = tid; idx < (m - 2) * (m - 1); idx += blockDim.x) {
-    const int j = idx / (m - 1), t = idx - j * (m - 1);
-    if (t < m - 1 - j) {
-      const cplx<double> v = A[(j + 1 + t) * lda + j];
-      stage[2 * (hoff(m, j) + t)] = v.x;
-      stage[2 * (hoff(m, j) + t) + 1] = v.y;
-    }
-  }
   __syncthreads();
-  cplx<double>* Hc = A;
-  for (int i = tid; i < hcount; i += blockDim.x) Hc[i] = mk<double>(stage[2 * i], stage[2 * i + 1]);
   for (int i = tid; i < m; i += blockDim.x) e2[i] = er[i] * er[i];
   __syncthreads();
   double* pool = Ad + heev_h_doubles(m);
@@ -349,18 +463,19 @@ __global__ void __launch_bounds__(HEEV_THREADS, 1)
   const int nbq = min(m, nb + HEEV_XB);
   const int ldz = m | 1;
   double* zT = pool;                  // nbq x ldz: vector a at zT[a*ldz + i]
-  double* fac = pool + nbq * ldz;     // 2 m B: 1/pivot, first superdiagonal of U
+  double* fac = pool + nbq * ldz;     // 3 m B: 1/pivot, first superdiagonal of U, multiplier
   double* Hm = fac;                   // nbq x nbq (after inverse iteration)
   double* Qm = fac + nbq * nbq;       // nbq x nbq
   double* shift = e2;                 // per-vector shift (e2 is free after the bisection)
   int* cl = order;                    // first index of each vector's cluster
-  int B = (pool_n - nbq * ldz) / (2 * m);
+  int B = (pool_n - nbq * ldz) / (3 * m);
   if (B > nbq) B = nbq;
   bool fast = B >= 1 && nbq * ldz + 2 * nbq * nbq <= pool_n;
   const double tol = 8.0 * EPS * tnorm;  // bisection interval width
   int nbx = nb;
   if (fast) {
-    // eigenvalue a by its 8-lane group; 9 sub-intervals per round
+    // eigenvalue a by its 8-lane group: 9 sub-intervals per round (one Sturm
+    // chain per lane: the count is bound by float64 issue, not latency)
     const int g = lane >> 3, gl = lane & 7;
     for (int a0 = 0; a0 < nbq; a0 += 4 * HEEV_WARPS) {
       const int a = a0 + warp * 4 + g;
@@ -369,11 +484,11 @@ __global__ void __launch_bounds__(HEEV_THREADS, 1)
       for (int round = 0; round < 40; ++round) {
         const bool done = !act || Uu - L <= tol;
         if (__all_sync(0xffffffffu, done)) break;
-        const double x = fma((Uu - L), (double)(gl + 1) * (1.0 / 9.0), L);
+        const double x = fma(Uu - L, (double)(gl + 1) * (1.0 / 9.0), L);
         const int cnt = sturm_count(d, e2, m, x);
         const unsigned bal = __ballot_sync(0xffffffffu, cnt > a);
         const unsigned gb = (bal >> (8 * g)) & 0xffu;
-        const int jj = gb ? __ffs(gb) - 1 : 8;
+        const int jj = gb ? __ffs(gb) - 1 : 8;  // first point with count > a
         const double xu = __shfl_sync(0xffffffffu, x, 8 * g + min(jj, 7));
         const double xl = __shfl_sync(0xffffffffu, x, 8 * g + max(jj - 1, 0));
         if (!done) {
@@ -413,60 +528,115 @@ __global__ void __launch_bounds__(HEEV_THREADS, 1)
     nbx = s_ctl[1];
 
     // inverse iteration, one thread per vector, B vectors at a time; three
-    // steps, the clusters orthonormalised after the first two
+    // steps, the clusters orthonormalised after each. The pivoted LU
+    // of T - shift I (1/pivot, first superdiagonal, multiplier; the swaps in
+    // two bit masks) is kept across the steps when every vector fits (B >= nbx).
     const double ptiny = EPS * tnorm;
+    const bool keep = B >= nbx;
+    unsigned long long sw0 = 0ull, sw1 = 0ull;
     for (int it = 0; it < 3; ++it) {
       for (int b0 = 0; b0 < nbx; b0 += B) {
         const int t = tid, a = b0 + t;
         if (t < B && a < nbx) {
           const double sg = shift[a];
-          double* z = zT + a * ldz;
-          double* iu = fac + t;          // iu[i * B]
-          double* u1 = fac + m * B + t;  // u1[i * B]
+          double* __restrict__ z = zT + a * ldz;
+          double* __restrict__ iu = fac + t;              // iu[i * B]
+          double* __restrict__ u1 = fac + m * B + t;      // u1[i * B]
+          double* __restrict__ lm = fac + 2 * m * B + t;  // lm[i * B]
           if (it == 0)
             for (int i = 0; i < m; ++i) z[i] = hash_pm1(((unsigned long long)(k * 131 + a) << 32) + i);
-          unsigned long long sw0 = 0ull, sw1 = 0ull;
-          double c0 = d[0] - sg, c1 = m > 1 ? er[0] : 0.0, rc = z[0];
-          for (int i = 0; i + 1 < m; ++i) {
-            const double ei = er[i], ai1 = d[i + 1] - sg, ei1 = er[i + 1], b1 = z[i + 1];
-            if (fabs(c0) >= ei || ei < ptiny) {  // no swap; a pivot below eps |T| is lifted to it
-              const double piv = fabs(c0) < ptiny ? ptiny : c0;
-              const double inv = 1.0 / piv, l = ei * inv;
-              iu[i * B] = inv;
-              u1[i * B] = c1;
-              z[i] = rc;
-              c0 = fma(-l, c1, ai1);
-              c1 = ei1;
-              rc = fma(-l, rc, b1);
-            } else {
-              const double inv = 1.0 / ei, l = c0 * inv;
-              iu[i * B] = inv;
-              u1[i * B] = ai1;
-              if (i < 64) sw0 |= 1ull << i; else sw1 |= 1ull << (i - 64);
-              z[i] = b1;
-              const double nc0 = fma(-l, ai1, c1);
-              c1 = -l * ei1;
-              c0 = nc0;
-              rc = fma(-l, b1, rc);
+          double rc = z[0];
+          if (it == 0 || !keep) {  // factor and transform the right-hand side
+            sw0 = sw1 = 0ull;
+            double c0 = d[0] - sg, c1 = m > 1 ? er[0] : 0.0;
+            double ei = 0.0, ai1 = 0.0, ei1 = 0.0, b1 = 0.0;
+            if (m > 1) {
+              ei = er[0];
+              ai1 = d[1] - sg;
+              ei1 = er[1];
+              b1 = z[1];
             }
-          }
-          {
+            for (int i = 0; i + 1 < m; ++i) {
+              double ei_n = 0.0, ai1_n = 0.0, ei1_n = 0.0, b1_n = 0.0;
+              if (i + 2 < m) {  // next step's operands, loaded ahead of this step's stores
+                ei_n = er[i + 1];
+                ai1_n = d[i + 2] - sg;
+                ei1_n = er[i + 2];
+                b1_n = z[i + 2];
+              }
+              if (fabs(c0) >= ei || ei < ptiny) {  // no swap; a pivot below eps |T| is lifted to it
+                const double piv = fabs(c0) < ptiny ? ptiny : c0;
+                const double inv = 1.0 / piv, l = ei * inv;
+                iu[i * B] = inv;
+                u1[i * B] = c1;
+                lm[i * B] = l;
+                z[i] = rc;
+                c0 = fma(-l, c1, ai1);
+                c1 = ei1;
+                rc = fma(-l, rc, b1);
+              } else {
+                const double inv = 1.0 / ei, l = c0 * inv;
+                iu[i * B] = inv;
+                u1[i * B] = ai1;
+                lm[i * B] = l;
+                if (i < 64) sw0 |= 1ull << i; else sw1 |= 1ull << (i - 64);
+                z[i] = b1;
+                const double nc0 = fma(-l, ai1, c1);
+                c1 = -l * ei1;
+                c0 = nc0;
+                rc = fma(-l, b1, rc);
+              }
+              ei = ei_n;
+              ai1 = ai1_n;
+              ei1 = ei1_n;
+              b1 = b1_n;
+            }
             const double piv = fabs(c0) < ptiny ? ptiny : c0;
             iu[(m - 1) * B] = 1.0 / piv;
-            z[m - 1] = rc;
+          } else {  // factors kept: transform the right-hand side only
+            double b1 = m > 1 ? z[1] : 0.0;
+            for (int i = 0; i + 1 < m; ++i) {
+              const double b1_n = i + 2 < m ? z[i + 2] : 0.0;
+              const double l = lm[i * B];
+              const bool sw = i < 64 ? (sw0 >> i) & 1ull : (sw1 >> (i - 64)) & 1ull;
+              if (!sw) {
+                z[i] = rc;
+                rc = fma(-l, rc, b1);
+              } else {
+                z[i] = b1;
+                rc = fma(-l, b1, rc);
+              }
+              b1 = b1_n;
+            }
           }
-          double zn1 = z[m - 1] * iu[(m - 1) * B], zn2 = 0.0;
+          // back substitution with U (1/pivot, first superdiagonal, second
+          // superdiagonal e_{i+1} where rows were swapped)
+          double zn1 = rc * iu[(m - 1) * B], zn2 = 0.0;
           z[m - 1] = zn1;
-          for (int i = m - 2; i >= 0; --i) {
-            const bool s = i < 64 ? (sw0 >> i) & 1ull : (sw1 >> (i - 64)) & 1ull;
-            const double u2 = s ? er[i + 1] : 0.0;
-            const double zi = (z[i] - u1[i * B] * zn1 - u2 * zn2) * iu[i * B];
-            z[i] = zi;
-            zn2 = zn1;
-            zn1 = zi;
+          double nrm = zn1 * zn1;
+          if (m > 1) {
+            double yi = z[m - 2], u1i = u1[(m - 2) * B], iui = iu[(m - 2) * B], e_i1 = er[m - 1];
+            for (int i = m - 2; i >= 0; --i) {
+              double yn = 0.0, u1n = 0.0, iun = 0.0, en = 0.0;
+              if (i > 0) {
+                yn = z[i - 1];
+                u1n = u1[(i - 1) * B];
+                iun = iu[(i - 1) * B];
+                en = er[i];
+              }
+              const bool sw = i < 64 ? (sw0 >> i) & 1ull : (sw1 >> (i - 64)) & 1ull;
+              const double u2 = sw ? e_i1 : 0.0;
+              const double zi = fma(-u2, zn2, fma(-u1i, zn1, yi)) * iui;
+              z[i] = zi;
+              nrm = fma(zi, zi, nrm);
+              zn2 = zn1;
+              zn1 = zi;
+              yi = yn;
+              u1i = u1n;
+              iui = iun;
+              e_i1 = en;
+            }
           }
-          double nrm = 0.0;
-          for (int i = 0; i < m; ++i) nrm = fma(z[i], z[i], nrm);
           if (!(nrm > 0.0 && nrm < 1e300)) {
             s_fail = 2;
           } else {
@@ -476,7 +646,7 @@ __global__ void __launch_bounds__(HEEV_THREADS, 1)
         }
         __syncthreads();
       }
-      if (s_fail || it == 2) break;
+      if (s_fail) break;
       // modified Gram-Schmidt inside each cluster, one warp per cluster
       for (int a = warp; a < nbx; a += HEEV_WARPS) {
         if (cl[a] != a || a + 1 >= nbx || cl[a + 1] != a) continue;
@@ -510,107 +680,104 @@ __global__ void __launch_bounds__(HEEV_THREADS, 1)
     fast = !s_fail;
   }
   if (fast) {
-    // CholQR2: Z <- Z R^{-1} with Z^T Z = R^T R, twice
-    const int npair = nbx * (nbx + 1) / 2;
-    for (int pass = 0; pass < 2 && fast; ++pass) {
-      for (int pr = warp; pr < npair; pr += HEEV_WARPS) {
-        int a = 0, rem = pr;
-        while (rem >= nbx - a) {
-          rem -= nbx - a;
-          ++a;
+    // Orthonormalisation: the vectors of distinct clusters are orthogonal to
+    // the inverse-iteration accuracy and each cluster is Gram-Schmidt
+    // orthonormal, so G = Z^T Z = I + E with E tiny; Newton-Schulz steps
+    // Z <- Z (3I - G)/2 square the deviation (|E| -> 3|E|^2/4) until it is at
+    // round-off. A deviation above 1/4 means the inverse iteration failed.
+    bool polish = false;
+    for (int pass = 0; pass < 5; ++pass) {
+      double dev = 0.0;
+      for (int a = warp; a < nbx; a += HEEV_WARPS) {
+        const double* za = zT + a * ldz;
+        double acc[PER];
+#pragma unroll
+        for (int t = 0; t < PER; ++t) acc[t] = 0.0;
+        for (int i = 0; i < m; ++i) {
+          const double zai = za[i];
+#pragma unroll
+          for (int t = 0; t < PER; ++t) {
+            const int b = lane + 32 * t;
+            if (b >= a && b < nbx) acc[t] = fma(zai, zT[b * ldz + i], acc[t]);
+          }
         }
-        const int b = a + rem;
-        double s = 0.0;
-        for (int i = lane; i < m; i += 32) s = fma(zT[a * ldz + i], zT[b * ldz + i], s);
-        s = warp_sum(s);
-        if (lane == 0) Hm[a * nbx + b] = s;
-      }
-      __syncthreads();
-      if (warp == 0) {  // upper Cholesky factor R in place
-        for (int j = 0; j < nbx; ++j) {
-          const double piv = Hm[j * nbx + j];
-          if (!(piv > 1e-20)) {  // columns are unit vectors: a pivot this small is a collapse
-            if (lane == 0) s_fail = 3;
-            break;
+#pragma unroll
+        for (int t = 0; t < PER; ++t) {
+          const int b = lane + 32 * t;
+          if (b >= a && b < nbx) {
+            Hm[a * nbx + b] = acc[t];
+            Hm[b * nbx + a] = acc[t];
+            dev = fmax(dev, fabs(acc[t] - (a == b ? 1.0 : 0.0)));
           }
-          const double rj = sqrt(piv), ri = 1.0 / rj;
-          __syncwarp();
-          for (int c = j + 1 + lane; c < nbx; c += 32) Hm[j * nbx + c] *= ri;
-          if (lane == 0) Hm[j * nbx + j] = rj;
-          __syncwarp();
-          const int rem = nbx - 1 - j;
-          for (int q = lane; q < rem * rem; q += 32) {
-            const int r = j + 1 + q / rem, c = j + 1 + q % rem;
-            if (c >= r) Hm[r * nbx + c] -= Hm[j * nbx + r] * Hm[j * nbx + c];
-          }
-          __syncwarp();
         }
       }
+      for (int o = 16; o > 0; o >>= 1) dev = fmax(dev, __shfl_xor_sync(0xffffffffu, dev, o));
+      if (lane == 0) s_rng[pass & 1][warp] = dev;
       __syncthreads();
-      if (s_fail) {
+      dev = 0.0;
+#pragma unroll
+      for (int q = 0; q < HEEV_WARPS; ++q) dev = fmax(dev, s_rng[pass & 1][q]);
+      if (dev <= 32.0 * EPS && polish) break;  // round-off level of an m-term dot product
+      if (dev <= 32.0 * EPS) polish = true;      // one more step takes the error to round-off
+      if (!(dev < 0.25) || pass == 4) {
         fast = false;
+        if (tid == 0) s_fail = 3;
         break;
       }
-      // row i of Z: w R = z_i by forward substitution over the columns, one warp per row
+      // Z <- Z (1.5 I - 0.5 G): warp per row i, lanes over columns b, in place
       for (int i = warp; i < m; i += HEEV_WARPS) {
-        double v[PER];
+        double o[PER];
 #pragma unroll
-        for (int t = 0; t < PER; ++t) {
-          const int b = lane + 32 * t;
-          v[t] = b < nbx ? zT[b * ldz + i] : 0.0;
-        }
+        for (int t = 0; t < PER; ++t) o[t] = 0.0;
+        for (int a = 0; a < nbx; ++a) {
+          const double za = zT[a * ldz + i];
 #pragma unroll
-        for (int ta = 0; ta < PER; ++ta) {
-          for (int al = 0; al < 32; ++al) {
-            const int a = 32 * ta + al;
-            if (a >= nbx) break;
-            double wa = __shfl_sync(0xffffffffu, v[ta], al) / Hm[a * nbx + a];
-            if (lane == al) v[ta] = wa;
-#pragma unroll
-            for (int t = ta; t < PER; ++t) {
-              const int b = lane + 32 * t;
-              if (b > a && b < nbx) v[t] = fma(-wa, Hm[a * nbx + b], v[t]);
-            }
+          for (int t = 0; t < PER; ++t) {
+            const int b = lane + 32 * t;
+            if (b < nbx) o[t] = fma(za, (a == b ? 1.5 : 0.0) - 0.5 * Hm[a * nbx + b], o[t]);
           }
         }
+        __syncwarp();
 #pragma unroll
         for (int t = 0; t < PER; ++t) {
           const int b = lane + 32 * t;
-          if (b < nbx) zT[b * ldz + i] = v[t];
+          if (b < nbx) zT[b * ldz + i] = o[t];
         }
       }
       __syncthreads();
     }
   }
   if (fast) {
-    // H = Z^T T Z (full), Q = I
-    const int npair = nbx * (nbx + 1) / 2;
-    for (int pr = warp; pr < npair; pr += HEEV_WARPS) {
-      int a = 0, rem = pr;
-      while (rem >= nbx - a) {
-        rem -= nbx - a;
-        ++a;
-      }
-      const int b = a + rem;
+    // H = Z^T T Z (full): warp per row a, lanes over columns b >= a
+    for (int a = warp; a < nbx; a += HEEV_WARPS) {
       const double* za = zT + a * ldz;
-      const double* zb = zT + b * ldz;
-      double s = 0.0;
-      for (int i = lane; i < m; i += 32) {
-        double tz = d[i] * zb[i];
-        if (i > 0) tz = fma(er[i - 1], zb[i - 1], tz);
-        if (i + 1 < m) tz = fma(er[i], zb[i + 1], tz);
-        s = fma(za[i], tz, s);
+      double acc[PER];
+#pragma unroll
+      for (int t = 0; t < PER; ++t) acc[t] = 0.0;
+      for (int i = 0; i < m; ++i) {
+        double tz = d[i] * za[i];
+        if (i > 0) tz = fma(er[i - 1], za[i - 1], tz);
+        if (i + 1 < m) tz = fma(er[i], za[i + 1], tz);
+#pragma unroll
+        for (int t = 0; t < PER; ++t) {
+          const int b = lane + 32 * t;
+          if (b >= a && b < nbx) acc[t] = fma(tz, zT[b * ldz + i], acc[t]);
+        }
       }
-      s = warp_sum(s);
-      if (lane == 0) {
-        Hm[a * nbx + b] = s;
-        Hm[b * nbx + a] = s;
+#pragma unroll
+      for (int t = 0; t < PER; ++t) {
+        const int b = lane + 32 * t;
+        if (b >= a && b < nbx) {
+          Hm[a * nbx + b] = acc[t];
+          Hm[b * nbx + a] = acc[t];
+        }
       }
     }
+    __syncthreads();
     for (int i = tid; i < nbx * nbx; i += blockDim.x) Qm[i] = (i / nbx == i % nbx) ? 1.0 : 0.0;
     __syncthreads();
     if (warp == 0) {  // cyclic Jacobi on the pairs above threshold
-      const double thr = 2.0 * EPS * tnorm;
+      const double thr = 0.5 * EPS * tnorm;  // below this a rotation only moves round-off
       for (int sweep = 0; sweep < 12; ++sweep) {
         int nrot = 0;
         for (int p = 0; p + 1 < nbx; ++p) {
@@ -663,58 +830,75 @@ __global__ void __launch_bounds__(HEEV_THREADS, 1)
       }
     }
     __syncthreads();
-    // eigenvectors: v = Z Q[:, src], residual |T v - theta v|, y = Q_H D v
+    // eigenvectors: v = Z Q[:, src], residual |T v - theta v|, y = Q_H D v;
+    // each warp carries VPW vectors through the reflectors together
+    constexpr int VPW = 4;
     cplx<double>* Uk = U + (int64_t)k * m * nb;
     const double rtol = 64.0 * EPS * tnorm;
-    for (int ra = warp; ra < nb; ra += HEEV_WARPS) {
-      const int src = order[ra];
-      const double th = Hm[src * nbx + src];
-      double v[PER];
+    for (int rb = 0; rb < nb; rb += HEEV_WARPS * VPW) {
+      cplx<double> y[VPW][PER];
+      double ths[VPW];
 #pragma unroll
-      for (int t = 0; t < PER; ++t) v[t] = 0.0;
-      for (int b = 0; b < nbx; ++b) {
-        const double qb = Qm[b * nbx + src];
-        if (qb == 0.0) continue;
+      for (int sv = 0; sv < VPW; ++sv) {
+        const int ra = rb + warp + HEEV_WARPS * sv;
+        ths[sv] = 0.0;
+#pragma unroll
+        for (int t = 0; t < PER; ++t) y[sv][t] = mk<double>(0.0, 0.0);
+        if (ra >= nb) continue;  // warp-uniform
+        const int src = order[ra];
+        const double th = Hm[src * nbx + src];
+        ths[sv] = th;
+        double v[PER];
+#pragma unroll
+        for (int t = 0; t < PER; ++t) v[t] = 0.0;
+        for (int b = 0; b < nbx; ++b) {
+          const double qb = Qm[b * nbx + src];
+          if (qb == 0.0) continue;
+#pragma unroll
+          for (int t = 0; t < PER; ++t) {
+            const int i = lane + 32 * t;
+            if (i < m) v[t] = fma(zT[b * ldz + i], qb, v[t]);
+          }
+        }
+        double res = 0.0;
 #pragma unroll
         for (int t = 0; t < PER; ++t) {
           const int i = lane + 32 * t;
-          if (i < m) v[t] = fma(zT[b * ldz + i], qb, v[t]);
+          const double up = __shfl_up_sync(0xffffffffu, v[t], 1);
+          const double wrapu = __shfl_sync(0xffffffffu, t > 0 ? v[t > 0 ? t - 1 : 0] : 0.0, 31);
+          const double dn = __shfl_down_sync(0xffffffffu, v[t], 1);
+          const double wrapd = __shfl_sync(0xffffffffu, t + 1 < PER ? v[t + 1 < PER ? t + 1 : t] : 0.0, 0);
+          const double vm = lane > 0 ? up : wrapu, vp = lane < 31 ? dn : wrapd;
+          if (i < m) {
+            double tv = (d[i] - th) * v[t];
+            if (i > 0) tv = fma(er[i - 1], vm, tv);
+            if (i + 1 < m) tv = fma(er[i], vp, tv);
+            res = fma(tv, tv, res);
+          }
+        }
+        res = warp_sum(res);
+        if (lane == 0) atomicMax(&g_heev_maxres, (unsigned long long)__double_as_longlong(sqrt(res) / tnorm));
+        if (!(res <= rtol * rtol)) {
+          if (lane == 0) s_fail = 4;
+        }
+#pragma unroll
+        for (int t = 0; t < PER; ++t) {
+          const int r = lane + 32 * t;
+          y[sv][t] = r < m ? scale(ph[r], v[t]) : mk<double>(0.0, 0.0);
         }
       }
-      double res = 0.0;
+      apply_reflectors<VPW>(y, m, lane, Hc, wv);
 #pragma unroll
-      for (int t = 0; t < PER; ++t) {
-        const int i = lane + 32 * t;
-        const double up = __shfl_up_sync(0xffffffffu, v[t], 1);
-        const double wrapu = __shfl_sync(0xffffffffu, t > 0 ? v[t > 0 ? t - 1 : 0] : 0.0, 31);
-        const double dn = __shfl_down_sync(0xffffffffu, v[t], 1);
-        const double wrapd = __shfl_sync(0xffffffffu, t + 1 < PER ? v[t + 1 < PER ? t + 1 : t] : 0.0, 0);
-        const double vm = lane > 0 ? up : wrapu, vp = lane < 31 ? dn : wrapd;
-        if (i < m) {
-          double tv = (d[i] - th) * v[t];
-          if (i > 0) tv = fma(er[i - 1], vm, tv);
-          if (i + 1 < m) tv = fma(er[i], vp, tv);
-          res = fma(tv, tv, res);
+      for (int sv = 0; sv < VPW; ++sv) {
+        const int ra = rb + warp + HEEV_WARPS * sv;
+        if (ra >= nb) continue;
+#pragma unroll
+        for (int t = 0; t < PER; ++t) {
+          const int r = lane + 32 * t;
+          if (r < m) Uk[(int64_t)r * nb + ra] = y[sv][t];
         }
+        if (lane == 0) eig[(int64_t)k * nb + ra] = ths[sv];
       }
-      res = warp_sum(res);
-      if (lane == 0) atomicMax(&g_heev_maxres, (unsigned long long)__double_as_longlong(sqrt(res) / tnorm));
-      if (!(res <= rtol * rtol)) {
-        if (lane == 0) s_fail = 4;
-      }
-      cplx<double> y[PER];
-#pragma unroll
-      for (int t = 0; t < PER; ++t) {
-        const int r = lane + 32 * t;
-        y[t] = r < m ? scale(ph[r], v[t]) : mk<double>(0.0, 0.0);
-      }
-      apply_reflectors(y, m, lane, Hc, wv);
-#pragma unroll
-      for (int t = 0; t < PER; ++t) {
-        const int r = lane + 32 * t;
-        if (r < m) Uk[(int64_t)r * nb + ra] = y[t];
-      }
-      if (lane == 0) eig[(int64_t)k * nb + ra] = th;
     }
     __syncthreads();
     if (!s_fail) {
@@ -740,7 +924,7 @@ __global__ void __launch_bounds__(HEEV_THREADS, 1)
     // header {-(mm+2), ilo} followed by its rotations {c, s} (i = mm-1 .. ilo);
     // then every thread replays the log on its rows of Z. The d/e recurrence
     // never reads Z, so batches need only two barriers each.
-    // plain doubles: the per-matrix offset k*m*m is only 8-byte aligned for odd m
+    // plain doubles: the per-matrix offset k*m*(m+8) is only 8-byte aligned for odd m
     double* lg = Zglob;
     const int cap = (m * m) / 2;  // entries of two doubles
     int l = 0, iter = 0;          // scalar QL state, used by thread 0 only
@@ -876,17 +1060,17 @@ __global__ void __launch_bounds__(HEEV_THREADS, 1)
   cplx<double>* Uk = U + (int64_t)k * m * nb;
   for (int a = warp; a < nb; a += HEEV_WARPS) {
     const int src = order[a];
-    cplx<double> y[PER];
+    cplx<double> y[1][PER];
 #pragma unroll
     for (int t = 0; t < PER; ++t) {
       const int r = lane + 32 * t;
-      y[t] = r < m ? scale(ph[r], Z[(int64_t)src * m + r]) : mk<double>(0.0, 0.0);
+      y[0][t] = r < m ? scale(ph[r], Z[(int64_t)src * m + r]) : mk<double>(0.0, 0.0);
     }
-    apply_reflectors(y, m, lane, Hc, wv);
+    apply_reflectors<1>(y, m, lane, Hc, wv);
 #pragma unroll
     for (int t = 0; t < PER; ++t) {
       const int r = lane + 32 * t;
-      if (r < m) Uk[(int64_t)r * nb + a] = y[t];
+      if (r < m) Uk[(int64_t)r * nb + a] = y[0][t];
     }
   }
 }
@@ -905,16 +1089,19 @@ static int heev_extra(int m, int nb) {
 }
 size_t heev_smem(int m, int nb) { return heev_a_doubles(m) * 8 + (size_t)heev_extra(m, nb) * 8 + heev_base_bytes(m); }
 
-// One launch of the eigensolver with scratch z (nk * m * m float64).
+// The eigensolver on nk matrices with scratch z (nk * heev_scratch_doubles(m)
+// float64): stage 1, then stages 2-5.
 static int launch_heev(int nk, int m, int nb, const void* S, int lds, int64_t sk, double* eig, void* U,
                        double* z, int* info, cudaStream_t st) {
+  const size_t sm1 = tri_smem(m);
+  GWB_CUDA_TRY(cudaFuncSetAttribute(k_heev_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+  k_heev_tridiag<<<nk, TRI_THREADS, sm1, st>>>((const cplx<double>*)S, lds, sk, m, z);
   const int extra = heev_extra(m, nb);
   const size_t sm = heev_smem(m, nb);
   GWB_CUDA_TRY(cudaFuncSetAttribute(k_heev_lowest, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  k_heev_lowest<<<nk, HEEV_THREADS, sm, st>>>((const cplx<double>*)S, lds, sk, m, nb, eig, (cplx<double>*)U, z,
-                                              info, extra);
+  k_heev_lowest<<<nk, HEEV_THREADS, sm, st>>>(m, nb, eig, (cplx<double>*)U, z, info, extra);
   GWB_LAUNCH_CHECK();
-  count_launches(1);
+  count_launches(2);
   return GWB_OK;
 }
 
@@ -931,6 +1118,8 @@ extern "C" int gwb_heev_lowest(int32_t nk, int32_t m, int32_t nb, const void* S,
 }
 
 extern "C" int gwb_heev_max_dim(void) { return GWB_HEEV_MMAX; }
+
+extern "C" int64_t gwb_heev_scratch_doubles(int32_t m) { return m > 0 ? (int64_t)heev_scratch_doubles(m) : 0; }
 
 // Diagnostics of the bisection path on the current device since load:
 // out[0..3] matrices sent to QL by reason (pool too small, non-finite inverse
@@ -957,7 +1146,7 @@ extern "C" int gwb_heev_ql_count(unsigned long long* out) {
 // Limits and sharing:
 //   * the array holds GWB_HEEV_NOALLOC_DOUBLES float64 (8 MiB); every GPU that
 //     loads libgwb.so holds it until the process exits;
-//   * a call needs nk * m * m float64 of it; larger problems are rejected with
+//   * a call needs nk * m * (m + 8) float64 of it; larger problems are rejected with
 //     GWB_ERR_ARG (use gwb_heev_lowest with caller-provided scratch);
 //   * every call on a device uses the same array and leaves its last contents
 //     there; the kernel writes every element of Z it reads (identity fill), so
@@ -983,8 +1172,8 @@ extern "C" int gwb_heev_lowest_noalloc(int32_t nk, int32_t m, int32_t nb, const 
   GWB_REQUIRE(nk > 0 && m > 0 && nb > 0 && nb <= m && lds >= m, "bad sizes");
   GWB_REQUIRE(m <= GWB_HEEV_MMAX, "m exceeds the shared-memory eigensolver limit (112)");
   GWB_REQUIRE(S && eig && U && info, "null pointer");
-  if ((int64_t)nk * m * m > (int64_t)GWB_HEEV_NOALLOC_DOUBLES) {
-    set_error("gwb_heev_lowest_noalloc: nk*m*m = " + std::to_string((int64_t)nk * m * m) +
+  if ((int64_t)nk * (int64_t)heev_scratch_doubles(m) > (int64_t)GWB_HEEV_NOALLOC_DOUBLES) {
+    set_error("gwb_heev_lowest_noalloc: nk*m*(m+8) = " + std::to_string((int64_t)nk * (int64_t)heev_scratch_doubles(m)) +
               " float64 of scratch exceeds the fixed " + std::to_string(GWB_HEEV_NOALLOC_DOUBLES) +
               " (8 MiB); call gwb_heev_lowest with caller-provided scratch");
     return GWB_ERR_ARG;

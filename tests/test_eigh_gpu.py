@@ -23,7 +23,7 @@ def _run(S: np.ndarray, nb: int):
     St = torch.from_numpy(S).to(dev)
     eig = torch.zeros(nk, nb, dtype=torch.float64, device=dev)
     U = torch.zeros(nk, m, nb, dtype=torch.complex128, device=dev)
-    Z = torch.zeros(nk, m * m, dtype=torch.float64, device=dev)
+    Z = torch.zeros(nk, _lib.load().gwb_heev_scratch_doubles(m), dtype=torch.float64, device=dev)
     info = torch.full((nk,), -1, dtype=torch.int32, device=dev)
     _lib.call("gwb_heev_lowest", nk, m, nb, St.data_ptr(), m, m * m, eig.data_ptr(), U.data_ptr(),
               Z.data_ptr(), info.data_ptr(), _lib.stream_ptr(dev))

@@ -47,7 +47,7 @@ def test_noalloc_matches_allocating_entry_twice(cuda_device):
                 torch.full((nk,), -1, dtype=torch.int32, device=cuda_device))
 
     eig_ref, U_ref, info_ref = outputs()
-    Z = torch.zeros(nk, m * m, dtype=torch.float64, device=cuda_device)
+    Z = torch.zeros(nk, _lib.load().gwb_heev_scratch_doubles(m), dtype=torch.float64, device=cuda_device)
     _lib.call("gwb_heev_lowest", nk, m, nb, S.data_ptr(), m, m * m, eig_ref.data_ptr(), U_ref.data_ptr(),
               Z.data_ptr(), info_ref.data_ptr(), st)
     scale = float(torch.linalg.eigvalsh(S).abs().max())
@@ -67,7 +67,7 @@ def test_noalloc_matches_allocating_entry_twice(cuda_device):
 
 def test_noalloc_rejects_oversized_request(cuda_device):
     from gradwave_b200 import _lib
-    nk, m, nb = 200, 96, 8          # 200 * 96 * 96 = 1.84M float64 > the fixed 1M
+    nk, m, nb = 200, 96, 8          # 200 * 96 * 104 = 2.0M float64 > the fixed 1M
     dummy = torch.zeros(1, dtype=torch.complex128, device=cuda_device)
     with pytest.raises(_lib.GwbError) as err:
         _lib.call("gwb_heev_lowest_noalloc", nk, m, nb, dummy.data_ptr(), m, m * m, dummy.data_ptr(),
