@@ -68,6 +68,7 @@ _P = ctypes.c_void_p
 _I = ctypes.c_int32
 _I64 = ctypes.c_int64
 _D = ctypes.c_double
+_SZ = ctypes.c_size_t
 
 # name -> argtypes (every function returns int status unless listed in _RESTYPES)
 _SIGNATURES = {
@@ -104,7 +105,8 @@ _SIGNATURES = {
     "gwb_mlp_backward": [_P, _I, _P, _P, _P, _P],
     "gwb_mlp_adam": [_P, _P, _P, _P, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _P],
     "gwb_precond_features": [_I, _I, _I, _I, _P, _I64, _P, _I64, _P, _P, _P, _P, _P],
-    "gwb_precond_learned": [_P, _I, _I, _I, _I, _P, _I64, _P, _I64, _P, _P, _P, _P, _P, _I64, _P],
+    "gwb_precond_learned": [_P, _I, _I, _I, _I, _P, _I64, _P, _I64, _P, _P, _P, _P, _P, _I64, _P, _SZ, _P],
+    "gwb_precond_learned_work_bytes": [_I, _I, _I],
     "gwb_stall_update": [_P, _P, _P, _P, _I, _D, _I, _P],
     "gwb_davidson_workspace_bytes": [ctypes.POINTER(DavidsonParams), ctypes.POINTER(ctypes.c_size_t)],
     "gwb_davidson_solve": [_P, ctypes.POINTER(DavidsonParams), _P, _P, _P, _P, _P, ctypes.c_size_t, _P, _P, _P,
@@ -112,7 +114,8 @@ _SIGNATURES = {
 }
 _RESTYPES = {"gwb_last_error": ctypes.c_char_p, "gwb_version": ctypes.c_char_p,
              "gwb_launch_count": ctypes.c_ulonglong,
-             "gwb_ham_scratch_bytes": ctypes.c_size_t, "gwb_heev_scratch_doubles": ctypes.c_int64}
+             "gwb_ham_scratch_bytes": ctypes.c_size_t, "gwb_heev_scratch_doubles": ctypes.c_int64,
+             "gwb_precond_learned_work_bytes": ctypes.c_int64}
 
 
 def declared_symbols() -> list[str]:

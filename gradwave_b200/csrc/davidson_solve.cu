@@ -85,8 +85,10 @@ int gwb_heev_lowest(int32_t, int32_t, int32_t, const void*, int32_t, int64_t, do
                     void*);
 int gwb_heev_max_dim(void);
 int gwb_ham_apply_strided(gwb_ham*, const void*, int64_t, void*, int64_t, int32_t, int32_t, int32_t, void*);
+int64_t gwb_precond_learned_work_bytes(int32_t, int32_t, int32_t);
 int gwb_precond_learned(const float*, int32_t, int32_t, int32_t, int32_t, const void*, int64_t, const void*, int64_t,
-                        const double*, const double*, const int32_t*, const uint8_t*, void*, int64_t, void*);
+                        const double*, const double*, const int32_t*, const uint8_t*, void*, int64_t, void*, size_t,
+                        void*);
 int gwb_stall_update(const double*, double*, uint8_t*, uint8_t*, int32_t, double, int32_t, void*);
 }
 
@@ -112,6 +114,8 @@ struct Work {
   double *Zs, *rn, *eig, *eig2, *stats, *rn_prev;
   int *sel, *info, *heev_info, *flags;
   unsigned char *tpa_only, *stall_count;
+  unsigned char* pl_work;
+  size_t pl_work_bytes;
 };
 
 static size_t layout(const gwb_davidson_params& p, unsigned char* base, Work* w) {
@@ -145,6 +149,8 @@ static size_t layout(const gwb_davidson_params& p, unsigned char* base, Work* w)
   t.rn_prev = b.take<double>(base, nk * nb);
   t.tpa_only = b.take<unsigned char>(base, nk * nb);
   t.stall_count = b.take<unsigned char>(base, nk * nb);
+  t.pl_work_bytes = (size_t)gwb_precond_learned_work_bytes((int32_t)nk, (int32_t)nb, (int32_t)npw);
+  t.pl_work = b.take<unsigned char>(base, t.pl_work_bytes);
   if (w) *w = t;
   return b.off + 256;
 }
@@ -411,7 +417,7 @@ class Solver {
       // 10 % for 3 rounds keeps TPA from then on
       GWB_TRY(gwb_stall_update(w_.rn, w_.rn_prev, w_.stall_count, w_.tpa_only, nk_ * nb_, 0.9, 3, st_));
       return gwb_precond_learned(static_cast<const float*>(model_), nk_, nb_, n_add, npw_, w_.X, nbp, w_.R, nbp, t_,
-                                 eig, w_.sel, w_.tpa_only, w_.D, nbp, st_);
+                                 eig, w_.sel, w_.tpa_only, w_.D, nbp, w_.pl_work, w_.pl_work_bytes, st_);
     }
     return gwb_precond_teter(nk_, nb_, n_add, npw_, w_.X, nbp, w_.R, nbp, t_, w_.sel, w_.D, nbp, st_);
   }

@@ -24,9 +24,10 @@
 //   3. Eigenvectors of T_r by three steps of inverse iteration (one thread per
 //      vector; Gaussian elimination with partial pivoting of T_r - shift I,
 //      factored once, zero pivots lifted to eps |T|; seeded random starts).
-//      Eigenvalues closer than 1e4 x the bisection width form a cluster that
-//      shares one shift just below it and is Gram-Schmidt orthonormalised
-//      after every step, so its vectors span its invariant subspace.
+//      Each vector is shifted by its own eigenvalue; eigenvalues closer than
+//      1e6 x the bisection width form a cluster that is Gram-Schmidt
+//      orthonormalised after every step, so its vectors span its invariant
+//      subspace even where the shifts coincide.
 //   4. Newton-Schulz orthonormalisation Z <- Z (3I - Z^T Z)/2, then
 //      Rayleigh-Ritz: H = Z^T T_r Z and a cyclic Jacobi sweep on H (Golub &
 //      Van Loan sec. 8.5.2) that rotates only pairs above eps |T| / 2 (the
@@ -503,12 +504,13 @@ __global__ void __launch_bounds__(HEEV_THREADS, 1)
       if (act && gl == 0) lam[a] = 0.5 * (L + Uu);
     }
     __syncthreads();
-    // clusters: runs of eigenvalues less than 1e4 * tol apart. An isolated
-    // eigenvalue is its own shift; a cluster [lo, hi] shares the shift
-    // lo - (hi - lo) - 16 tol, where every member is amplified within a factor
-    // of two of the others, and its block is re-orthonormalised between steps
+    // clusters: runs of eigenvalues less than 1e6 * tol apart (degenerate
+    // bands of an unconverged subspace split by ~1e-9 |T|). Every vector is
+    // shifted by its own eigenvalue, so it converges away from everything
+    // outside its cluster; each cluster is Gram-Schmidt orthonormalised after
+    // every step, so near-equal shifts cannot make its vectors collapse.
     if (tid == 0) {
-      const double gap = 1e4 * tol;
+      const double gap = 1e6 * tol;
       int n = nb;
       while (n < nbq && lam[n] - lam[n - 1] <= gap) ++n;
       s_ctl[1] = n;
@@ -516,10 +518,9 @@ __global__ void __launch_bounds__(HEEV_THREADS, 1)
       while (a < n) {
         int b = a + 1;
         while (b < n && lam[b] - lam[b - 1] <= gap) ++b;
-        const double sh = b - a == 1 ? lam[a] : lam[a] - (lam[b - 1] - lam[a]) - 16.0 * tol;
         for (int c = a; c < b; ++c) {
           cl[c] = a;
-          shift[c] = sh;
+          shift[c] = lam[c];
         }
         a = b;
       }
@@ -528,7 +529,7 @@ __global__ void __launch_bounds__(HEEV_THREADS, 1)
     nbx = s_ctl[1];
 
     // inverse iteration, one thread per vector, B vectors at a time; three
-    // steps, the clusters orthonormalised after each. The pivoted LU
+    // steps, each cluster orthonormalised after every step. The pivoted LU
     // of T - shift I (1/pivot, first superdiagonal, multiplier; the swaps in
     // two bit masks) is kept across the steps when every vector fits (B >= nbx).
     const double ptiny = EPS * tnorm;
@@ -686,7 +687,7 @@ __global__ void __launch_bounds__(HEEV_THREADS, 1)
     // Z <- Z (3I - G)/2 square the deviation (|E| -> 3|E|^2/4) until it is at
     // round-off. A deviation above 1/4 means the inverse iteration failed.
     bool polish = false;
-    for (int pass = 0; pass < 5; ++pass) {
+    for (int pass = 0; pass < 8; ++pass) {
       double dev = 0.0;
       for (int a = warp; a < nbx; a += HEEV_WARPS) {
         const double* za = zT + a * ldz;
@@ -719,7 +720,7 @@ __global__ void __launch_bounds__(HEEV_THREADS, 1)
       for (int q = 0; q < HEEV_WARPS; ++q) dev = fmax(dev, s_rng[pass & 1][q]);
       if (dev <= 32.0 * EPS && polish) break;  // round-off level of an m-term dot product
       if (dev <= 32.0 * EPS) polish = true;      // one more step takes the error to round-off
-      if (!(dev < 0.25) || pass == 4) {
+      if (!(dev < 0.25) || pass == 7) {
         fast = false;
         if (tid == 0) s_fail = 3;
         break;

@@ -312,82 +312,6 @@ __global__ void __launch_bounds__(256) k_features(int npw, int nb, int n_add, co
   }
 }
 
-// The learned preconditioner step: like k_precond_teter, with the TPA
-// coefficient corrected by the network; bands flagged in tpa_only (the stall
-// fallback) keep plain TPA.
-__global__ void __launch_bounds__(256) k_precond_learned(const float* __restrict__ P, int npw, int nb, int n_add,
-                                                         const cplx<double>* __restrict__ x, int64_t xk,
-                                                         const cplx<double>* __restrict__ r, int64_t rk,
-                                                         const double* __restrict__ t, const double* __restrict__ eig,
-                                                         const int* __restrict__ sel,
-                                                         const unsigned char* __restrict__ tpa_only,
-                                                         cplx<double>* __restrict__ d, int64_t dk) {
-  extern __shared__ float sp[];
-  __shared__ double red[8];
-  __shared__ double sv[3];
-  load_params(P, sp);
-  const int k = blockIdx.x / n_add, s = blockIdx.x % n_add;
-  const int b = sel[(int64_t)k * n_add + s];
-  const bool plain = tpa_only && tpa_only[(int64_t)k * nb + b];
-  const cplx<double>* xr = x + k * xk + (int64_t)b * npw;
-  const cplx<double>* rr = r + k * rk + (int64_t)b * npw;
-  const double* tk = t + (int64_t)k * npw;
-  cplx<double>* dr = d + k * dk + (int64_t)s * npw;
-  double tb = 0.0, r2 = 0.0;
-  for (int g = threadIdx.x; g < npw; g += blockDim.x) {
-    tb += tk[g] * norm2(xr[g]);
-    r2 += norm2(rr[g]);
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    tb += __shfl_xor_sync(0xffffffffu, tb, o);
-    r2 += __shfl_xor_sync(0xffffffffu, r2, o);
-  }
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = tb;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double a = 0.0;
-    for (int w = 0; w < 8; ++w) a += red[w];
-    sv[0] = a;
-  }
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = r2;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double a = 0.0;
-    for (int w = 0; w < 8; ++w) a += red[w];
-    sv[1] = a;
-  }
-  __syncthreads();
-  const double tbv = sv[0], rrms = sqrt(sv[1] / npw), eps = eig[(int64_t)k * nb + b];
-  double nn = 0.0;
-  for (int g = threadIdx.x; g < npw; g += blockDim.x) {
-    const cplx<double> rv = rr[g];
-    double c = tpa_coeff(tk[g], tbv);
-    if (!plain && (rv.x != 0.0 || rv.y != 0.0)) {
-      float u[NIN];
-      features(tk[g], tbv, eps, sqrt(norm2(rv)), rrms, u);
-      const float o = fminf(fmaxf(forward_one(sp, u), -3.f), 3.f);
-      c *= (double)expf(o);
-    }
-    const cplx<double> v = scale(rv, c);
-    dr[g] = v;
-    nn += norm2(v);
-  }
-  for (int o = 16; o > 0; o >>= 1) nn += __shfl_xor_sync(0xffffffffu, nn, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = nn;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double a = 0.0;
-    for (int w = 0; w < 8; ++w) a += red[w];
-    sv[2] = sqrt(a);
-  }
-  __syncthreads();
-  if (sv[2] > 1e-300) {
-    const double inv = 1.0 / sv[2];
-    for (int g = threadIdx.x; g < npw; g += blockDim.x) dr[g] = scale(dr[g], inv);
-  }
-}
-
 // ---------------------------------------------------------------------------
 // Tensor-core inference (mma.sync m16n8k16, BF16 in, FP32 accumulate). A warp
 // evaluates 16 plane waves at a time: layer 1 (4 -> 64) on the CUDA cores
@@ -410,7 +334,18 @@ __device__ __forceinline__ void mma_bf16(float* d, const unsigned* a, unsigned b
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-__device__ __forceinline__ float silu_fast(float z) { return __fdividef(z, 1.f + __expf(-z)); }
+// SiLU as h + h tanh(h), h = z/2: one SFU op (tanh.approx.f32, |rel. err| < 2^-10.9)
+// per activation instead of an exponential and a reciprocal; well inside the
+// BF16 rounding the activations get next.
+__device__ __forceinline__ float tanh_approx(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float silu_fast(float z) {
+  const float h = 0.5f * z;
+  return fmaf(h, tanh_approx(h), h);
+}
 
 // One hidden 64 -> 64 layer: acc[nt][4] = bias + A . W^T, then SiLU and BF16
 // packing into the next A fragments an[kt][4].
@@ -444,36 +379,19 @@ __device__ __forceinline__ void tc_layer(const unsigned (&a)[4][4], const __nv_b
   }
 }
 
-__global__ void __launch_bounds__(256) k_precond_learned_tc(
-    const float* __restrict__ P, int npw, int nb, int n_add, const cplx<double>* __restrict__ x, int64_t xk,
-    const cplx<double>* __restrict__ r, int64_t rk, const double* __restrict__ t_, const double* __restrict__ eig,
-    const int* __restrict__ sel, const unsigned char* __restrict__ tpa_only, cplx<double>* __restrict__ d,
-    int64_t dk) {
-  __shared__ __align__(16) __nv_bfloat16 sW2[HID * WSTR];
-  __shared__ __align__(16) __nv_bfloat16 sW3[HID * WSTR];
-  __shared__ float sW1[HID * NIN], sB1[HID], sB2[HID], sB3[HID], sW4[HID], sB4;
-  __shared__ double red[8];
-  __shared__ double sv[3];
-  for (int i = threadIdx.x; i < HID * HID; i += blockDim.x) {
-    const int n = i / HID, kx = i % HID;
-    sW2[n * WSTR + kx] = __float2bfloat16_rn(P[O_W2 + i]);
-    sW3[n * WSTR + kx] = __float2bfloat16_rn(P[O_W3 + i]);
-  }
-  for (int i = threadIdx.x; i < HID * NIN; i += blockDim.x) sW1[i] = bf(P[O_W1 + i]);
-  for (int i = threadIdx.x; i < HID; i += blockDim.x) {
-    sB1[i] = bf(P[O_B1 + i]);
-    sB2[i] = bf(P[O_B2 + i]);
-    sB3[i] = bf(P[O_B3 + i]);
-    sW4[i] = bf(P[O_W4 + i]);
-  }
-  if (threadIdx.x == 0) sB4 = bf(P[O_B4]);
+// Per selected row (k, s): tb = sum_G t_G |x_G|^2 (the band's kinetic energy)
+// and the rms residual amplitude, float64 in a fixed order.
+__global__ void __launch_bounds__(256) k_precond_row_stats(int npw, int nb, int n_add,
+                                                           const cplx<double>* __restrict__ x, int64_t xk,
+                                                           const cplx<double>* __restrict__ r, int64_t rk,
+                                                           const double* __restrict__ t_, const int* __restrict__ sel,
+                                                           double* __restrict__ stats) {
+  __shared__ double red[2][8];
   const int k = blockIdx.x / n_add, s = blockIdx.x % n_add;
   const int b = sel[(int64_t)k * n_add + s];
-  const bool plain = tpa_only && tpa_only[(int64_t)k * nb + b];
   const cplx<double>* xr = x + k * xk + (int64_t)b * npw;
   const cplx<double>* rr = r + k * rk + (int64_t)b * npw;
   const double* tk = t_ + (int64_t)k * npw;
-  cplx<double>* dr = d + k * dk + (int64_t)s * npw;
   double tb = 0.0, r2 = 0.0;
   for (int gi = threadIdx.x; gi < npw; gi += blockDim.x) {
     tb += tk[gi] * norm2(xr[gi]);
@@ -483,34 +401,72 @@ __global__ void __launch_bounds__(256) k_precond_learned_tc(
     tb += __shfl_xor_sync(0xffffffffu, tb, o);
     r2 += __shfl_xor_sync(0xffffffffu, r2, o);
   }
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = tb;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double a = 0.0;
-    for (int w = 0; w < 8; ++w) a += red[w];
-    sv[0] = a;
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = tb;
+    red[1][threadIdx.x >> 5] = r2;
   }
   __syncthreads();
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = r2;
-  __syncthreads();
   if (threadIdx.x == 0) {
-    double a = 0.0;
-    for (int w = 0; w < 8; ++w) a += red[w];
-    sv[1] = a;
+    double a = 0.0, c = 0.0;
+    for (int w = 0; w < 8; ++w) {
+      a += red[0][w];
+      c += red[1][w];
+    }
+    stats[2 * blockIdx.x] = a;
+    stats[2 * blockIdx.x + 1] = sqrt(c / npw);
+  }
+}
+
+constexpr int PL_CHUNK = 512;   // plane waves per CTA of the inference kernel
+constexpr int PL_THREADS = 128;
+
+// Learned preconditioner on one chunk of one selected row: grid (chunks, rows),
+// four warps, each evaluating 16 plane waves at a time with the network on
+// the tensor cores; d = r * TPA * exp(clamp(o, +-3)) unnormalised, and the
+// chunk's sum of |d|^2 into partial[row * chunks + chunk].
+__global__ void __launch_bounds__(PL_THREADS) k_precond_learned_tc(
+    const float* __restrict__ P, int npw, int nb, int n_add, const cplx<double>* __restrict__ r, int64_t rk,
+    const double* __restrict__ t_, const double* __restrict__ eig, const int* __restrict__ sel,
+    const unsigned char* __restrict__ tpa_only, const double* __restrict__ stats, cplx<double>* __restrict__ d,
+    int64_t dk, double* __restrict__ partial) {
+  __shared__ __align__(16) __nv_bfloat16 sW2[HID * WSTR];
+  __shared__ __align__(16) __nv_bfloat16 sW3[HID * WSTR];
+  __shared__ float sW1[HID * NIN], sB1[HID], sB2[HID], sB3[HID], sW4[HID], sB4;
+  __shared__ double red[PL_THREADS / 32];
+  const int row = blockIdx.y, k = row / n_add, s = row % n_add;
+  const int b = sel[(int64_t)k * n_add + s];
+  const bool plain = tpa_only && tpa_only[(int64_t)k * nb + b];
+  if (!plain) {
+    for (int i = threadIdx.x; i < HID * HID; i += blockDim.x) {
+      const int n = i / HID, kx = i % HID;
+      sW2[n * WSTR + kx] = __float2bfloat16_rn(P[O_W2 + i]);
+      sW3[n * WSTR + kx] = __float2bfloat16_rn(P[O_W3 + i]);
+    }
+    for (int i = threadIdx.x; i < HID * NIN; i += blockDim.x) sW1[i] = bf(P[O_W1 + i]);
+    for (int i = threadIdx.x; i < HID; i += blockDim.x) {
+      sB1[i] = bf(P[O_B1 + i]);
+      sB2[i] = bf(P[O_B2 + i]);
+      sB3[i] = bf(P[O_B3 + i]);
+      sW4[i] = bf(P[O_W4 + i]);
+    }
+    if (threadIdx.x == 0) sB4 = bf(P[O_B4]);
   }
   __syncthreads();
-  const double tbv = sv[0], rrms = sqrt(sv[1] / npw), eps = eig[(int64_t)k * nb + b];
+  const cplx<double>* rr = r + k * rk + (int64_t)b * npw;
+  const double* tk = t_ + (int64_t)k * npw;
+  cplx<double>* dr = d + k * dk + (int64_t)s * npw;
+  const double tbv = stats[2 * row], rrms = stats[2 * row + 1], eps = eig[(int64_t)k * nb + b];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
+  const int c_begin = blockIdx.x * PL_CHUNK, c_end = min(npw, c_begin + PL_CHUNK);
   double nn = 0.0;
-  for (int c0 = 0; c0 < npw; c0 += 128) {
-    const int base = c0 + 16 * warp;  // this warp's 16 plane waves
+  for (int base = c_begin + 16 * warp; base < c_end; base += 16 * (PL_THREADS / 32)) {
     // features of sample (lane & 15) by lanes 0..15
     float u[NIN] = {0.f, 0.f, 0.f, 0.f};
     cplx<double> rv = mk<double>(0.0, 0.0);
     double tg = 0.0;
     {
       const int gi = base + (lane & 15);
-      if (lane < 16 && gi < npw) {
+      if (lane < 16 && gi < c_end) {
         rv = rr[gi];
         tg = tk[gi];
         if (!plain) features(tg, tbv, eps, sqrt(norm2(rv)), rrms, u);
@@ -576,7 +532,7 @@ __global__ void __launch_bounds__(256) k_precond_learned_tc(
     const float o_b = __shfl_sync(0xffffffffu, o_row8, 4 * (srow & 7));
     const float o = srow < 8 ? o_a : o_b;
     const int gi = base + srow;
-    if (lane < 16 && gi < npw) {
+    if (lane < 16 && gi < c_end) {
       double c = tpa_coeff(tg, tbv);
       if (!plain && (rv.x != 0.0 || rv.y != 0.0)) c *= (double)__expf(fminf(fmaxf(o, -3.f), 3.f));
       const cplx<double> v = scale(rv, c);
@@ -585,18 +541,25 @@ __global__ void __launch_bounds__(256) k_precond_learned_tc(
     }
   }
   for (int o = 16; o > 0; o >>= 1) nn += __shfl_xor_sync(0xffffffffu, nn, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = nn;
+  if (lane == 0) red[warp] = nn;
   __syncthreads();
   if (threadIdx.x == 0) {
     double a = 0.0;
-    for (int w = 0; w < 8; ++w) a += red[w];
-    sv[2] = sqrt(a);
+    for (int w = 0; w < PL_THREADS / 32; ++w) a += red[w];
+    partial[(int64_t)row * gridDim.x + blockIdx.x] = a;
   }
-  __syncthreads();
-  if (sv[2] > 1e-300) {
-    const double inv = 1.0 / sv[2];
-    for (int gi = threadIdx.x; gi < npw; gi += blockDim.x) dr[gi] = scale(dr[gi], inv);
-  }
+}
+
+// d row <- d row / |d row|, the norm summed from the chunk partials in order.
+__global__ void k_precond_normalize(int npw, int n_add, int chunks, const double* __restrict__ partial,
+                                    cplx<double>* __restrict__ d, int64_t dk) {
+  const int row = blockIdx.x, k = row / n_add, s = row % n_add;
+  double a = 0.0;
+  for (int c = 0; c < chunks; ++c) a += partial[(int64_t)row * chunks + c];
+  if (!(a > 0.0)) return;
+  const double inv = 1.0 / sqrt(a);
+  cplx<double>* dr = d + k * dk + (int64_t)s * npw;
+  for (int gi = threadIdx.x; gi < npw; gi += blockDim.x) dr[gi] = scale(dr[gi], inv);
 }
 
 // Stall rule of the learned preconditioner: a band whose residual has not
@@ -688,17 +651,32 @@ int gwb_precond_features(int32_t nk, int32_t nb, int32_t n_add, int32_t npw, con
   return GWB_OK;
 }
 
+int64_t gwb_precond_learned_work_bytes(int32_t nk, int32_t n_add, int32_t npw) {
+  if (nk <= 0 || n_add <= 0 || npw <= 0) return 0;
+  const int64_t rows = (int64_t)nk * n_add, chunks = (npw + PL_CHUNK - 1) / PL_CHUNK;
+  return rows * (2 + chunks) * (int64_t)sizeof(double);
+}
+
 int gwb_precond_learned(const float* params, int32_t nk, int32_t nb, int32_t n_add, int32_t npw, const void* x,
                         int64_t x_kstride, const void* r, int64_t r_kstride, const double* t, const double* eig,
-                        const int32_t* sel, const uint8_t* tpa_only, void* d, int64_t d_kstride, void* stream) {
+                        const int32_t* sel, const uint8_t* tpa_only, void* d, int64_t d_kstride, void* work,
+                        size_t work_bytes, void* stream) {
   GWB_REQUIRE(params && nk > 0 && nb > 0 && n_add > 0 && n_add <= nb && npw > 0, "bad sizes");
-  GWB_REQUIRE(x && r && t && eig && sel && d, "null pointer");
-  k_precond_learned_tc<<<nk * n_add, 256, 0, (cudaStream_t)stream>>>(params, npw, nb, n_add,
-                                                                     (const cplx<double>*)x, x_kstride,
-                                                                     (const cplx<double>*)r, r_kstride, t, eig, sel,
-                                                                     tpa_only, (cplx<double>*)d, d_kstride);
+  GWB_REQUIRE(x && r && t && eig && sel && d && work, "null pointer");
+  GWB_REQUIRE((int64_t)work_bytes >= gwb_precond_learned_work_bytes(nk, n_add, npw),
+              "work smaller than gwb_precond_learned_work_bytes");
+  const int rows = nk * n_add, chunks = (npw + PL_CHUNK - 1) / PL_CHUNK;
+  double* stats = static_cast<double*>(work);
+  double* partial = stats + 2 * (int64_t)rows;
+  const cudaStream_t st = (cudaStream_t)stream;
+  k_precond_row_stats<<<rows, 256, 0, st>>>(npw, nb, n_add, (const cplx<double>*)x, x_kstride,
+                                            (const cplx<double>*)r, r_kstride, t, sel, stats);
+  k_precond_learned_tc<<<dim3(chunks, rows), PL_THREADS, 0, st>>>(params, npw, nb, n_add, (const cplx<double>*)r,
+                                                                  r_kstride, t, eig, sel, tpa_only, stats,
+                                                                  (cplx<double>*)d, d_kstride, partial);
+  k_precond_normalize<<<rows, 256, 0, st>>>(npw, n_add, chunks, partial, (cplx<double>*)d, d_kstride);
   GWB_LAUNCH_CHECK();
-  count_launches(1);
+  count_launches(3);
   return GWB_OK;
 }
 

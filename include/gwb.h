@@ -233,10 +233,14 @@ int gwb_precond_features(int32_t nk, int32_t nb, int32_t n_add, int32_t npw, con
                          const void* r, int64_t r_kstride, const double* t, const double* eig, const int32_t* sel,
                          float* feats, void* stream);
 /* As gwb_precond_teter with the coefficient TPA * exp(clamp(network, -3, 3));
- * bands with tpa_only[k][b] != 0 (uint8 (nk, nb), may be NULL) keep TPA. */
+ * bands with tpa_only[k][b] != 0 (uint8 (nk, nb), may be NULL) keep TPA.
+ * work: device scratch of gwb_precond_learned_work_bytes(nk, n_add, npw) bytes
+ * (per-row statistics and per-chunk partial norms, 8-byte aligned). */
+int64_t gwb_precond_learned_work_bytes(int32_t nk, int32_t n_add, int32_t npw);
 int gwb_precond_learned(const float* params, int32_t nk, int32_t nb, int32_t n_add, int32_t npw, const void* x,
                         int64_t x_kstride, const void* r, int64_t r_kstride, const double* t, const double* eig,
-                        const int32_t* sel, const uint8_t* tpa_only, void* d, int64_t d_kstride, void* stream);
+                        const int32_t* sel, const uint8_t* tpa_only, void* d, int64_t d_kstride, void* work,
+                        size_t work_bytes, void* stream);
 /* Stall fallback: count[i] = rounds since rn[i] last fell below ratio * rn_best[i]
  * (rn_best starts at +inf, count at 0); tpa_only[i] = 1 once count[i] >= patience. */
 int gwb_stall_update(const double* rn, double* rn_best, uint8_t* count, uint8_t* tpa_only, int32_t n, double ratio,

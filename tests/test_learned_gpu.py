@@ -90,8 +90,10 @@ def test_zero_output_layer_is_tpa(cuda_device):
     _lib.call("gwb_precond_teter", nk, nb, n_add, npw, X.data_ptr(), nb * npw, R.data_ptr(), nb * npw,
               Tt.data_ptr(), sel.data_ptr(), D1.data_ptr(), nb * npw, s)
     P = torch.from_numpy(learned.init_params(0)).to(cuda_device)
+    W = torch.empty(_lib.load().gwb_precond_learned_work_bytes(nk, n_add, npw), dtype=torch.uint8, device=cuda_device)
     _lib.call("gwb_precond_learned", P.data_ptr(), nk, nb, n_add, npw, X.data_ptr(), nb * npw, R.data_ptr(),
-              nb * npw, Tt.data_ptr(), E.data_ptr(), sel.data_ptr(), None, D2.data_ptr(), nb * npw, s)
+              nb * npw, Tt.data_ptr(), E.data_ptr(), sel.data_ptr(), None, D2.data_ptr(), nb * npw, W.data_ptr(),
+              W.numel(), s)
     assert float((D1 - D2).abs().max()) < 1e-13
 
 
@@ -170,8 +172,10 @@ def test_tensor_core_inference_matches_reference_forward(cuda_device):
     P = torch.from_numpy(p).to(cuda_device)
     s = _lib.stream_ptr(cuda_device)
     D = torch.zeros_like(X)
+    W = torch.empty(_lib.load().gwb_precond_learned_work_bytes(nk, n_add, npw), dtype=torch.uint8, device=cuda_device)
     _lib.call("gwb_precond_learned", P.data_ptr(), nk, nb, n_add, npw, X.data_ptr(), nb * npw, R.data_ptr(),
-              nb * npw, Tt.data_ptr(), E.data_ptr(), sel.data_ptr(), None, D.data_ptr(), nb * npw, s)
+              nb * npw, Tt.data_ptr(), E.data_ptr(), sel.data_ptr(), None, D.data_ptr(), nb * npw, W.data_ptr(),
+              W.numel(), s)
     F = torch.empty(nk, n_add, npw, 4, dtype=torch.float32, device=cuda_device)
     _lib.call("gwb_precond_features", nk, nb, n_add, npw, X.data_ptr(), nb * npw, R.data_ptr(), nb * npw,
               Tt.data_ptr(), E.data_ptr(), sel.data_ptr(), F.data_ptr(), s)
