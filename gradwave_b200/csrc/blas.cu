@@ -77,57 +77,95 @@ extern "C" int gwb_zgemm(int opA, int opB, int64_t M, int64_t N, int64_t K, doub
 // A (M x K), B (N x K) row-major and M, N small (the subspace, projection and
 // Gram products of the Davidson step: M, N <= a few hundred, K = npw). cuBLAS
 // tiles such shapes into a few dozen CTAs; here K is split into slices so the
-// grid fills the GPU, each CTA accumulates a 32 x 32 output tile of one slice
-// (2 x 2 outputs per thread, float64), and a second kernel sums the slices in
-// a fixed order (deterministic).
+// grid fills the GPU, each CTA accumulates a TM x TN output tile of one slice
+// (2 x 2 outputs per thread, float64; TM, TN in {8, 16, 24, 32} chosen from M
+// and N so narrow blocks are not padded to 32), staging 16-column K steps of A
+// and B through double-buffered shared memory with cp.async (the next step
+// loads while this one multiplies), and a second kernel sums the slices in a
+// fixed order (deterministic).
 namespace gwb {
 
-constexpr int NH_T = 32, NH_K = 16;
+constexpr int NH_K = 16;
 
-__global__ void __launch_bounds__(256) k_zgemm_nh_part(int M, int N, int K, int kslice,
-                                                       const cplx<double>* __restrict__ A, int64_t lda, int64_t sA,
-                                                       const cplx<double>* __restrict__ B, int64_t ldb, int64_t sB,
-                                                       cplx<double>* __restrict__ part, int batch) {
-  __shared__ cplx<double> sa[NH_T][NH_K + 1];
-  __shared__ cplx<double> sb[NH_T][NH_K + 1];
-  const int tilesN = (N + NH_T - 1) / NH_T;
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc, bool valid) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
+  const int n = valid ? 16 : 0;  // 0: zero-fill, nothing read
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(gsrc), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+template <int TM, int TN>
+__global__ void __launch_bounds__(TM * TN / 4) k_zgemm_nh_part(int M, int N, int K, int kslice,
+                                                             const cplx<double>* __restrict__ A, int64_t lda,
+                                                             int64_t sA, const cplx<double>* __restrict__ B,
+                                                             int64_t ldb, int64_t sB, cplx<double>* __restrict__ part,
+                                                             int batch) {
+  constexpr int NT = TM * TN / 4;  // threads: (TM/2) x (TN/2)
+  constexpr int HM = TM / 2, HN = TN / 2;
+  __shared__ __align__(16) cplx<double> sa[2][TM][NH_K + 1];
+  __shared__ __align__(16) cplx<double> sb[2][TN][NH_K + 1];
+  const int tilesN = (N + TN - 1) / TN;
   const int ti = blockIdx.x / tilesN, tj = blockIdx.x % tilesN;
   const int s = blockIdx.y, b = blockIdx.z;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int tx = threadIdx.x % HN, ty = threadIdx.x / HN;
   const cplx<double>* Ab = A + b * sA;
   const cplx<double>* Bb = B + b * sB;
   const int g0 = s * kslice, g1 = min(K, g0 + kslice);
+  const int nsteps = (g1 - g0 + NH_K - 1) / NH_K;
+
+  auto load = [&](int step, int buf) {
+    const int gb = g0 + step * NH_K;
+    for (int idx = threadIdx.x; idx < (TM + TN) * NH_K; idx += NT) {
+      const int r = idx / NH_K, kk = idx % NH_K, g = gb + kk;
+      if (r < TM) {
+        const int ia = ti * TM + r;
+        const bool ok = ia < M && g < g1;
+        cp_async16(&sa[buf][r][kk], ok ? (const void*)(Ab + (int64_t)ia * lda + g) : (const void*)Ab, ok);
+      } else {
+        const int jb = tj * TN + (r - TM);
+        const bool ok = jb < N && g < g1;
+        cp_async16(&sb[buf][r - TM][kk], ok ? (const void*)(Bb + (int64_t)jb * ldb + g) : (const void*)Bb, ok);
+      }
+    }
+    cp_async_commit();
+  };
+
   cplx<double> acc[2][2];
 #pragma unroll
   for (int a = 0; a < 2; ++a)
 #pragma unroll
     for (int c = 0; c < 2; ++c) acc[a][c] = mk<double>(0.0, 0.0);
-  for (int gb = g0; gb < g1; gb += NH_K) {
-    for (int idx = threadIdx.x; idx < NH_T * NH_K; idx += 256) {
-      const int r = idx / NH_K, kk = idx % NH_K;
-      const int g = gb + kk;
-      const int ia = ti * NH_T + r, jb = tj * NH_T + r;
-      sa[r][kk] = (ia < M && g < g1) ? Ab[(int64_t)ia * lda + g] : mk<double>(0.0, 0.0);
-      sb[r][kk] = (jb < N && g < g1) ? Bb[(int64_t)jb * ldb + g] : mk<double>(0.0, 0.0);
+  if (nsteps > 0) load(0, 0);
+  for (int st = 0; st < nsteps; ++st) {
+    const int buf = st & 1;
+    if (st + 1 < nsteps) {
+      load(st + 1, buf ^ 1);
+      cp_async_wait<1>();  // this step's group has landed; the next may still fly
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
 #pragma unroll
     for (int kk = 0; kk < NH_K; ++kk) {
-      const cplx<double> a0 = sa[ty][kk], a1 = sa[ty + 16][kk];
-      const cplx<double> b0 = sb[tx][kk], b1 = sb[tx + 16][kk];
+      const cplx<double> a0 = sa[buf][ty][kk], a1 = sa[buf][ty + HM][kk];
+      const cplx<double> b0 = sb[buf][tx][kk], b1 = sb[buf][tx + HN][kk];
       acc[0][0] = acc[0][0] + mul_conj(a0, b0);
       acc[0][1] = acc[0][1] + mul_conj(a0, b1);
       acc[1][0] = acc[1][0] + mul_conj(a1, b0);
       acc[1][1] = acc[1][1] + mul_conj(a1, b1);
     }
-    __syncthreads();
+    __syncthreads();  // buf is refilled by the load two steps on
   }
   cplx<double>* P = part + ((int64_t)s * batch + b) * M * N;
 #pragma unroll
   for (int a = 0; a < 2; ++a)
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
-      const int i = ti * NH_T + ty + 16 * a, j = tj * NH_T + tx + 16 * c;
+      const int i = ti * TM + ty + HM * a, j = tj * TN + tx + HN * c;
       if (i < M && j < N) P[(int64_t)i * N + j] = acc[a][c];
     }
 }
@@ -160,22 +198,36 @@ extern "C" int gwb_zgemm_nh(int64_t M, int64_t N, int64_t K, double alpha_re, do
   if (M == 0 || N == 0 || batch == 0) return GWB_OK;
   GWB_REQUIRE(A && B && C && work, "null pointer");
   GWB_REQUIRE(M * N * batch * 16 <= (int64_t)work_bytes, "work smaller than one M*N*batch slice");
-  const int tiles = (int)(((M + NH_T - 1) / NH_T) * ((N + NH_T - 1) / NH_T));
+  // tile edges: multiples of 8 up to 32 covering M and N
+  const int TM = (int)std::min<int64_t>(32, (M + 7) / 8 * 8), TN = (int)std::min<int64_t>(32, (N + 7) / 8 * 8);
+  const int tiles = (int)(((M + TM - 1) / TM) * ((N + TN - 1) / TN));
   const int64_t slice_bytes = M * N * batch * 16;
-  int64_t want = (4 * 148 + (int64_t)tiles * batch - 1) / ((int64_t)tiles * batch);
+  const int threads = TM * TN / 4;
+  // enough CTAs for ~4 x 148 x (256 / threads) tiles in flight
+  const int64_t target = 4 * 148 * (256 / threads);
+  int64_t want = (target + (int64_t)tiles * batch - 1) / ((int64_t)tiles * batch);
   want = std::min<int64_t>(want, std::max<int64_t>(1, K / 128));
   want = std::min<int64_t>(want, (int64_t)work_bytes / slice_bytes);
   const int nslice = (int)std::max<int64_t>(1, want);
   const int kslice = (int)(((K + nslice - 1) / nslice + NH_K - 1) / NH_K * NH_K);
   const int ns = (int)((K + kslice - 1) / kslice);
   dim3 g1(tiles, ns, (unsigned)batch);
-  k_zgemm_nh_part<<<g1, 256, 0, (cudaStream_t)stream>>>((int)M, (int)N, (int)K, kslice, (const cplx<double>*)A, lda,
-                                                        strideA, (const cplx<double>*)B, ldb, strideB,
-                                                        (cplx<double>*)work, (int)batch);
+  cudaStream_t st = (cudaStream_t)stream;
+  const cplx<double>* Ap = (const cplx<double>*)A;
+  const cplx<double>* Bp = (const cplx<double>*)B;
+  cplx<double>* Wp = (cplx<double>*)work;
+#define GWB_NH_CASE(tm, tn)                                                                                      \
+  if (TM == tm && TN == tn)                                                                                      \
+    k_zgemm_nh_part<tm, tn><<<g1, tm * tn / 4, 0, st>>>((int)M, (int)N, (int)K, kslice, Ap, lda, strideA, Bp, ldb, \
+                                                        strideB, Wp, (int)batch);
+#define GWB_NH_ROW(tm) GWB_NH_CASE(tm, 8) GWB_NH_CASE(tm, 16) GWB_NH_CASE(tm, 24) GWB_NH_CASE(tm, 32)
+  GWB_NH_ROW(8) GWB_NH_ROW(16) GWB_NH_ROW(24) GWB_NH_ROW(32)
+#undef GWB_NH_ROW
+#undef GWB_NH_CASE
   const int64_t total = M * N * batch;
   const int blocks = (int)std::min<int64_t>((total + 255) / 256, 4096);
-  k_zgemm_nh_reduce<<<blocks, 256, 0, (cudaStream_t)stream>>>((int)M, (int)N, ns, (int)batch,
-                                                              (const cplx<double>*)work, mk<double>(alpha_re, alpha_im),
+  k_zgemm_nh_reduce<<<blocks, 256, 0, st>>>((int)M, (int)N, ns, (int)batch,
+                                            (const cplx<double>*)work, mk<double>(alpha_re, alpha_im),
                                                               mk<double>(beta_re, beta_im), (cplx<double>*)C, ldc,
                                                               strideC);
   GWB_LAUNCH_CHECK();
