@@ -221,12 +221,15 @@ __global__ void __launch_bounds__(256, (C1 && C2) ? 3 : 1) k_plane_forward(
 // Nonlocal term. Tiles: TB bands x TP projectors, G slices of TG.
 constexpr int NL_TB = 16, NL_TP = 32, NL_TG = 32;
 
-// K4: part[s][k][b][p] = sum_{g in slice s} conj(P[k][p][g]) c[k][b][g]
+// K4: part[s][k][b][p] = sum_{g in slice s} conj(P[k][p][g]) c[k][b][g].
+// The next step's tiles are loaded into registers while this step multiplies
+// out of shared memory (one barrier pair per step).
 template <typename T, typename SIO>
 __global__ void __launch_bounds__(256) k_becp_partial(const SIO* __restrict__ c,
                                                       const cplx<T>* __restrict__ P,
                                                       cplx<T>* __restrict__ part, int nk, int nb,
                                                       int nproj, int npw_max, int gslice, int64_t ck) {
+  constexpr int LC = NL_TB * NL_TG / 256, LP = NL_TP * NL_TG / 256;  // elements per thread per step
   __shared__ cplx<T> sc[NL_TB][NL_TG + 1];
   __shared__ cplx<T> sp[NL_TP][NL_TG + 1];
   const int pt = blockIdx.x, bt = blockIdx.y;
@@ -235,18 +238,35 @@ __global__ void __launch_bounds__(256) k_becp_partial(const SIO* __restrict__ c,
   const int lb = tid / 16, lp = tid % 16;  // each thread: band lb, projectors lp and lp+16
   cplx<T> acc0 = mk<T>(0, 0), acc1 = mk<T>(0, 0);
   const int g_begin = s * gslice, g_end = min(npw_max, g_begin + gslice);
-  for (int gb = g_begin; gb < g_end; gb += NL_TG) {
-    for (int i = tid; i < NL_TB * NL_TG; i += blockDim.x) {
-      const int bb = i / NL_TG, gg = i % NL_TG;
+  cplx<T> rc[LC], rp[LP];
+  auto fetch = [&](int gb) {
+#pragma unroll
+    for (int q = 0; q < LC; ++q) {
+      const int i = tid + 256 * q, bb = i / NL_TG, gg = i % NL_TG;
       const int b = bt * NL_TB + bb, gi = gb + gg;
-      sc[bb][gg] = (b < nb && gi < g_end) ? ld<T>(c, (size_t)k * ck + (size_t)b * npw_max + gi) : mk<T>(0, 0);
+      rc[q] = (b < nb && gi < g_end) ? ld<T>(c, (size_t)k * ck + (size_t)b * npw_max + gi) : mk<T>(0, 0);
     }
-    for (int i = tid; i < NL_TP * NL_TG; i += blockDim.x) {
-      const int pp = i / NL_TG, gg = i % NL_TG;
+#pragma unroll
+    for (int q = 0; q < LP; ++q) {
+      const int i = tid + 256 * q, pp = i / NL_TG, gg = i % NL_TG;
       const int p = pt * NL_TP + pp, gi = gb + gg;
-      sp[pp][gg] = (p < nproj && gi < g_end) ? P[((size_t)k * nproj + p) * npw_max + gi] : mk<T>(0, 0);
+      rp[q] = (p < nproj && gi < g_end) ? P[((size_t)k * nproj + p) * npw_max + gi] : mk<T>(0, 0);
+    }
+  };
+  if (g_begin < g_end) fetch(g_begin);
+  for (int gb = g_begin; gb < g_end; gb += NL_TG) {
+#pragma unroll
+    for (int q = 0; q < LC; ++q) {
+      const int i = tid + 256 * q;
+      sc[i / NL_TG][i % NL_TG] = rc[q];
+    }
+#pragma unroll
+    for (int q = 0; q < LP; ++q) {
+      const int i = tid + 256 * q;
+      sp[i / NL_TG][i % NL_TG] = rp[q];
     }
     __syncthreads();
+    if (gb + NL_TG < g_end) fetch(gb + NL_TG);
 #pragma unroll 8
     for (int gg = 0; gg < NL_TG; ++gg) {
       const cplx<T> cv = sc[lb][gg];
@@ -264,17 +284,29 @@ __global__ void __launch_bounds__(256) k_becp_partial(const SIO* __restrict__ c,
   }
 }
 
-// K5: bd[k][b][q] = sum_p (sum_s part[s][k][b][p]) D[p][q]
+// K5: bd[k][b][q] = sum_p (sum_s part[s][k][b][p]) D[p][q]. The slice sums
+// are split over the threads (projector p, slice group) and combined in a
+// fixed order (deterministic).
 template <typename T>
-__global__ void k_becp_reduce_d(const cplx<T>* __restrict__ part, const T* __restrict__ D,
-                                cplx<T>* __restrict__ bd, int nk, int nb, int nproj, int nslice) {
+__global__ void __launch_bounds__(128) k_becp_reduce_d(const cplx<T>* __restrict__ part, const T* __restrict__ D,
+                                                       cplx<T>* __restrict__ bd, int nk, int nb, int nproj,
+                                                       int nslice) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* becp = reinterpret_cast<cplx<T>*>(smem_raw);  // nproj
-  const int kb = blockIdx.x;  // k*nb + b
+  cplx<T>* grp = becp + nproj;                            // nproj * ngrp partial sums
+  const int kb = blockIdx.x;                               // k*nb + b
   const size_t stride = (size_t)nk * nb * nproj;
+  const int ngrp = max(1, (int)blockDim.x / nproj);
+  for (int idx = threadIdx.x; idx < nproj * ngrp; idx += blockDim.x) {
+    const int p = idx % nproj, gq = idx / nproj;
+    cplx<T> a = mk<T>(0, 0);
+    for (int s = gq; s < nslice; s += ngrp) a = a + part[s * stride + (size_t)kb * nproj + p];
+    grp[gq * nproj + p] = a;
+  }
+  __syncthreads();
   for (int p = threadIdx.x; p < nproj; p += blockDim.x) {
     cplx<T> a = mk<T>(0, 0);
-    for (int s = 0; s < nslice; ++s) a = a + part[s * stride + (size_t)kb * nproj + p];
+    for (int gq = 0; gq < ngrp; ++gq) a = a + grp[gq * nproj + p];
     becp[p] = a;
   }
   __syncthreads();
@@ -298,8 +330,12 @@ __global__ void __launch_bounds__(256) k_nl_add(const cplx<T>* __restrict__ bd,
   const int tid = threadIdx.x;
   const int lg = tid % TGO, lb0 = tid / TGO;  // 4 band groups x 64 g; each thread 4 bands
   cplx<T> acc[4];
+  const int gi_o = gt * TGO + lg;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) acc[i] = mk<T>(0, 0);
+  for (int i = 0; i < 4; ++i) {  // the output rows first: their loads overlap the tile staging below
+    const int b = bt * NL_TB + lb0 * 4 + i;
+    acc[i] = (gi_o < npw_max && b < nb) ? ld<T>(out, (size_t)k * ok + (size_t)b * npw_max + gi_o) : mk<T>(0, 0);
+  }
   for (int q0 = 0; q0 < nproj; q0 += TQ) {
     for (int i = tid; i < NL_TB * TQ; i += blockDim.x) {
       const int bb = i / TQ, qq = i % TQ;
@@ -320,15 +356,11 @@ __global__ void __launch_bounds__(256) k_nl_add(const cplx<T>* __restrict__ bd,
     }
     __syncthreads();
   }
-  const int gi = gt * TGO + lg;
-  if (gi < npw_max) {
+  if (gi_o < npw_max) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int b = bt * NL_TB + lb0 * 4 + i;
-      if (b < nb) {
-        const size_t o = (size_t)k * ok + (size_t)b * npw_max + gi;
-        st(out, o, ld<T>(out, o) + acc[i]);
-      }
+      if (b < nb) st(out, (size_t)k * ok + (size_t)b * npw_max + gi_o, acc[i]);
     }
   }
 }
@@ -443,8 +475,9 @@ static int apply_impl(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t ok
     const T* D = dbl ? (const T*)h->d_d64 : (const T*)h->d_d32;
     dim3 g4((h->nproj + NL_TP - 1) / NL_TP, (nb + NL_TB - 1) / NL_TB, h->nk * nsl);
     k_becp_partial<T, SIO><<<g4, 256, 0, st>>>(c, P, (cplx<T>*)h->d_part, h->nk, nb, h->nproj, h->npw_max, gslice, ck);
-    k_becp_reduce_d<T><<<h->nk * nb, 128, h->nproj * es, st>>>((const cplx<T>*)h->d_part, D, (cplx<T>*)h->d_bd,
-                                                            h->nk, nb, h->nproj, nsl);
+    const int ngrp = std::max(1, 128 / h->nproj);
+    k_becp_reduce_d<T><<<h->nk * nb, 128, (size_t)h->nproj * (1 + ngrp) * es, st>>>(
+        (const cplx<T>*)h->d_part, D, (cplx<T>*)h->d_bd, h->nk, nb, h->nproj, nsl);
     dim3 g6((h->npw_max + 63) / 64, (nb + NL_TB - 1) / NL_TB, h->nk);
     k_nl_add<T, SIO><<<g6, 256, 0, st>>>((const cplx<T>*)h->d_bd, P, out, h->nk, nb, h->nproj, h->npw_max, ok);
     GWB_LAUNCH_CHECK();
