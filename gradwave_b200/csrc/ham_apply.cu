@@ -36,6 +36,7 @@
 
 #include "common.cuh"
 #include "fft.cuh"
+#include "rdft.cuh"
 
 namespace gwb {
 
@@ -179,6 +180,163 @@ __global__ void __launch_bounds__(256, C0 ? 3 : 1) k_pencil_vloc(FftGeom g, cplx
     const int j0 = i / n2, i2 = i - j0 * n2;
     const int r = rowmap(j0, g.M[0], L0, n0);
     base[(size_t)j0 * n1 * n2 + i2] = S[r * n2 + i2];
+  }
+}
+
+// K2 with the whole axis-0 transform in registers (cubic box, N0 <= 48): one
+// thread per pencil (i1, i2) of one (band, k); the occupied planes are loaded
+// (coalesced over i2), inverse DFT, x v(r)/N, forward DFT, occupied planes
+// stored back. No shared memory, no barriers; the plane stride is a constant,
+// so every load and store is one base register plus an immediate offset.
+template <typename T, int N0>
+__global__ void __launch_bounds__(128) k_pencil_vloc_reg(FftGeom g, cplx<T>* __restrict__ W, const T* __restrict__ v,
+                                                         int nbc) {
+  constexpr int PLANE = N0 * N0;
+  const int L0 = g.L[0], M0 = g.M[0];
+  const int bl = blockIdx.y, k = blockIdx.z;
+  const int pidx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pidx >= PLANE) return;
+  cplx<T>* base = W + ((size_t)k * nbc + bl) * L0 * (size_t)PLANE + pidx;
+  // occupied rows: 0..M0 hold planes 0..M0; rows N0-(L0-M0-1)..N0-1 hold the
+  // wrapped planes M0+1..L0-1, i.e. plane r - (N0 - L0)
+  const int hi0 = N0 - (L0 - M0 - 1);
+  cplx<T>* wrap = base - (ptrdiff_t)(N0 - L0) * PLANE;
+  cplx<T> x[N0];
+  rdft_detail::StaticFor<0, N0>::run([&](auto rc) {
+    constexpr int r = decltype(rc)::value;
+    x[r] = r <= M0 ? base[r * PLANE] : (r >= hi0 ? wrap[r * PLANE] : mk<T>(0, 0));
+  });
+  rdft<N0, +1>(x);
+  const T* vp = v + pidx;
+  rdft_detail::StaticFor<0, N0>::run([&](auto rc) {
+    constexpr int r = decltype(rc)::value;
+    x[r] = scale(x[r], vp[r * PLANE]);
+  });
+  rdft<N0, -1>(x);
+  rdft_detail::StaticFor<0, N0>::run([&](auto rc) {
+    constexpr int r = decltype(rc)::value;
+    if (r <= M0) base[r * PLANE] = x[r];
+    else if (r >= hi0) wrap[r * PLANE] = x[r];
+  });
+}
+
+// K1 and K3 with whole transforms in registers (cubic box, N <= 48): a CTA
+// takes PLR planes of one (band, k), N threads per plane, the planes in shared
+// memory with rows padded to N + 1. K1: sphere scatter, one thread per
+// occupied row runs the axis-2 inverse DFT, then one thread per column the
+// axis-1 inverse DFT and writes the column (coalesced over i2) to W. K3: one
+// thread per column loads it from W and runs the axis-1 forward DFT, one
+// thread per occupied row the axis-2 forward DFT, then the sphere gather + t c.
+// Two barriers after the staging, instead of two per radix pass.
+constexpr int PLR = 4;  // planes per CTA
+
+template <int N>
+__device__ __forceinline__ int occ_row(int rr, int M, int L) {  // memory row of occupied row rr
+  return rr <= M ? rr : rr + N - L;
+}
+
+template <typename T, typename SIO, int N>
+__global__ void __launch_bounds__(PLR * N) k_plane_inverse_reg(FftGeom g, const int* __restrict__ plane_ptr,
+                                                              const int* __restrict__ plane_g,
+                                                              const int* __restrict__ plane_pos,
+                                                              const SIO* __restrict__ c, cplx<T>* __restrict__ W,
+                                                              int64_t ck, int b0, int nbc, int npw_max) {
+  constexpr int LDS = N + 1, PS = N * LDS;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* S = reinterpret_cast<cplx<T>*>(smem_raw);  // [PLR][N][LDS]
+  const int L0 = g.L[0], L1 = g.L[1], M1 = g.M[1];
+  const int jb = blockIdx.x * PLR, bl = blockIdx.y, k = blockIdx.z;
+  const int np = min(PLR, L0 - jb);
+  for (int i = threadIdx.x; i < PLR * PS; i += blockDim.x) S[i] = mk<T>(0, 0);
+  __syncthreads();
+  const size_t crow = (size_t)k * ck + (size_t)(b0 + bl) * npw_max;
+  const int* pp = plane_ptr + k * L0 + jb;
+  const int e0 = pp[0], e1 = pp[np];
+  for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    int q = 0;
+#pragma unroll
+    for (int qq = 1; qq < PLR; ++qq) q += (qq < np && e >= pp[qq]) ? 1 : 0;
+    const int pos = plane_pos[e], i1 = pos / N, i2 = pos - i1 * N;
+    S[q * PS + i1 * LDS + i2] = ld<T>(c, crow + plane_g[e]);
+  }
+  __syncthreads();
+  const int p = threadIdx.x / N, lane = threadIdx.x - p * N;
+  if (p < np && lane < L1) {  // axis 2 (rows), occupied rows only
+    cplx<T>* row = S + p * PS + occ_row<N>(lane, M1, L1) * LDS;
+    cplx<T> x[N];
+    rdft_detail::StaticFor<0, N>::run([&](auto qc) { x[decltype(qc)::value] = row[decltype(qc)::value]; });
+    rdft<N, +1>(x);
+    rdft_detail::StaticFor<0, N>::run([&](auto qc) { row[decltype(qc)::value] = x[decltype(qc)::value]; });
+  }
+  __syncthreads();
+  if (p < np) {  // axis 1 (columns): the whole column out to W
+    const cplx<T>* col = S + p * PS + lane;
+    cplx<T> x[N];
+    rdft_detail::StaticFor<0, N>::run([&](auto rc) {
+      constexpr int r = decltype(rc)::value;
+      x[r] = col[r * LDS];
+    });
+    rdft<N, +1>(x);
+    cplx<T>* dst = W + (((size_t)k * nbc + bl) * L0 + jb + p) * (size_t)(N * N) + lane;
+    rdft_detail::StaticFor<0, N>::run([&](auto rc) {
+      constexpr int r = decltype(rc)::value;
+      dst[r * N] = x[r];
+    });
+  }
+}
+
+template <typename T, typename SIO, int N>
+__global__ void __launch_bounds__(PLR * N) k_plane_forward_reg(
+    FftGeom g, const int* __restrict__ plane_ptr, const int* __restrict__ plane_g, const int* __restrict__ plane_pos,
+    const int* __restrict__ npw, const SIO* __restrict__ c, SIO* __restrict__ out, const cplx<T>* __restrict__ W,
+    const T* __restrict__ t, int64_t ck, int64_t ok, int b0, int nbc, int npw_max) {
+  constexpr int LDS = N + 1, PS = N * LDS;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* S = reinterpret_cast<cplx<T>*>(smem_raw);  // [PLR][N][LDS]
+  const int L0 = g.L[0], L1 = g.L[1], M1 = g.M[1];
+  const int jb = blockIdx.x * PLR, bl = blockIdx.y, k = blockIdx.z;
+  const int np = min(PLR, L0 - jb);
+  const int p = threadIdx.x / N, lane = threadIdx.x - p * N;
+  const int hi1 = N - (L1 - M1 - 1);
+  if (p < np) {  // axis 1 (columns) forward; keep the occupied rows
+    const cplx<T>* src = W + (((size_t)k * nbc + bl) * L0 + jb + p) * (size_t)(N * N) + lane;
+    cplx<T> x[N];
+    rdft_detail::StaticFor<0, N>::run([&](auto rc) {
+      constexpr int r = decltype(rc)::value;
+      x[r] = src[r * N];
+    });
+    rdft<N, -1>(x);
+    cplx<T>* col = S + p * PS + lane;
+    rdft_detail::StaticFor<0, N>::run([&](auto rc) {
+      constexpr int r = decltype(rc)::value;
+      if (r <= M1 || r >= hi1) col[r * LDS] = x[r];
+    });
+  }
+  __syncthreads();
+  if (p < np && lane < L1) {  // axis 2 (rows) forward, occupied rows only
+    cplx<T>* row = S + p * PS + occ_row<N>(lane, M1, L1) * LDS;
+    cplx<T> x[N];
+    rdft_detail::StaticFor<0, N>::run([&](auto qc) { x[decltype(qc)::value] = row[decltype(qc)::value]; });
+    rdft<N, -1>(x);
+    rdft_detail::StaticFor<0, N>::run([&](auto qc) { row[decltype(qc)::value] = x[decltype(qc)::value]; });
+  }
+  __syncthreads();
+  const size_t crow = (size_t)k * ck + (size_t)(b0 + bl) * npw_max;
+  const size_t orow = (size_t)k * ok + (size_t)(b0 + bl) * npw_max;
+  const T* tk = t + (size_t)k * npw_max;
+  const int* pp = plane_ptr + k * L0 + jb;
+  const int e0 = pp[0], e1 = pp[np];
+  for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    int q = 0;
+#pragma unroll
+    for (int qq = 1; qq < PLR; ++qq) q += (qq < np && e >= pp[qq]) ? 1 : 0;
+    const int pos = plane_pos[e], i1 = pos / N, i2 = pos - i1 * N;
+    const int gi = plane_g[e];
+    const cplx<T> cv = ld<T>(c, crow + gi);
+    st(out, orow + gi, S[q * PS + i1 * LDS + i2] + scale(cv, tk[gi]));
+  }
+  if (jb == 0) {
+    for (int gi = npw[k] + threadIdx.x; gi < npw_max; gi += blockDim.x) st(out, orow + gi, mk<T>(0, 0));
   }
 }
 
@@ -423,15 +581,40 @@ static int local_chunks(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t 
   GWB_CUDA_TRY(cudaFuncSetAttribute(k_plane_forward<T, SIO, C, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA));
   GWB_CUDA_TRY(cudaFuncSetAttribute(k_pencil_vloc<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
   cplx<T>* W = (cplx<T>*)h->d_W;
+  const bool cubic = g.n[0] == g.n[1] && g.n[1] == g.n[2];
+  const int nreg = (cubic && g.n[0] == 36 && C == kCode36) ? 36 : ((cubic && g.n[0] == 24 && C == kCode24) ? 24 : 0);
+  const size_t smR = (size_t)PLR * nreg * (nreg + 1) * sizeof(cplx<T>);
+  if (nreg == 36) {
+    GWB_CUDA_TRY(cudaFuncSetAttribute(k_plane_inverse_reg<T, SIO, 36>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smR));
+    GWB_CUDA_TRY(cudaFuncSetAttribute(k_plane_forward_reg<T, SIO, 36>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smR));
+  } else if (nreg == 24) {
+    GWB_CUDA_TRY(cudaFuncSetAttribute(k_plane_inverse_reg<T, SIO, 24>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smR));
+    GWB_CUDA_TRY(cudaFuncSetAttribute(k_plane_forward_reg<T, SIO, 24>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smR));
+  }
   for (int b0 = 0; b0 < nb; b0 += nbc) {
     const int cb = std::min(nbc, nb - b0);
-    dim3 gA(g.L[0], cb, h->nk), gB(g.n[1], cb, h->nk);
-    k_plane_inverse<T, SIO, C, C><<<gA, 256, smA, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos, c, W,
-                                                       tw1, tw2, ck, b0, cb, h->npw_max);
-    k_pencil_vloc<T, C><<<gB, 256, smB, st>>>(g, W, v, tw0, cb);
-    k_plane_forward<T, SIO, C, C><<<gA, 256, smA, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos,
-                                                       h->d_npw, c, out, W, t, tw1, tw2, ck, ok, b0, cb,
-                                                       h->npw_max);
+    dim3 gA(g.L[0], cb, h->nk), gB(g.n[1], cb, h->nk), gP((g.L[0] + PLR - 1) / PLR, cb, h->nk);
+    dim3 gR((g.n[1] * g.n[2] + 127) / 128, cb, h->nk);
+    if (nreg == 36) {
+      k_plane_inverse_reg<T, SIO, 36><<<gP, PLR * 36, smR, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos, c,
+                                                                 W, ck, b0, cb, h->npw_max);
+      k_pencil_vloc_reg<T, 36><<<gR, 128, 0, st>>>(g, W, v, cb);
+      k_plane_forward_reg<T, SIO, 36><<<gP, PLR * 36, smR, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos,
+                                                                 h->d_npw, c, out, W, t, ck, ok, b0, cb, h->npw_max);
+    } else if (nreg == 24) {
+      k_plane_inverse_reg<T, SIO, 24><<<gP, PLR * 24, smR, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos, c,
+                                                                 W, ck, b0, cb, h->npw_max);
+      k_pencil_vloc_reg<T, 24><<<gR, 128, 0, st>>>(g, W, v, cb);
+      k_plane_forward_reg<T, SIO, 24><<<gP, PLR * 24, smR, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos,
+                                                                 h->d_npw, c, out, W, t, ck, ok, b0, cb, h->npw_max);
+    } else {
+      k_plane_inverse<T, SIO, C, C><<<gA, 256, smA, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos, c, W,
+                                                         tw1, tw2, ck, b0, cb, h->npw_max);
+      k_pencil_vloc<T, C><<<gB, 256, smB, st>>>(g, W, v, tw0, cb);
+      k_plane_forward<T, SIO, C, C><<<gA, 256, smA, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos,
+                                                         h->d_npw, c, out, W, t, tw1, tw2, ck, ok, b0, cb,
+                                                         h->npw_max);
+    }
     GWB_LAUNCH_CHECK();
     count_launches(3);
   }
