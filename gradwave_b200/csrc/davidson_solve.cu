@@ -84,6 +84,7 @@ int gwb_row_repair(int32_t, int32_t, int32_t, void*, int64_t, const uint8_t*, do
 int gwb_heev_lowest(int32_t, int32_t, int32_t, const void*, int32_t, int64_t, double*, void*, double*, int32_t*,
                     void*);
 int gwb_heev_max_dim(void);
+int64_t gwb_heev_scratch_doubles(int32_t);
 int gwb_ham_apply_strided(gwb_ham*, const void*, int64_t, void*, int64_t, int32_t, int32_t, int32_t, void*);
 int64_t gwb_precond_learned_work_bytes(int32_t, int32_t, int32_t);
 int gwb_precond_learned(const float*, int32_t, int32_t, int32_t, int32_t, const void*, int64_t, const void*, int64_t,
@@ -136,7 +137,7 @@ static size_t layout(const gwb_davidson_params& p, unsigned char* base, Work* w)
   t.Linv = b.take<Z16>(base, nk * nb * nb);
   t.Gs = b.take<Z16>(base, nk * nb * nb);
   t.U = b.take<Z16>(base, nk * std::max(hm, nb) * nb);
-  t.Zs = b.take<double>(base, nk * hm * (hm + 8));
+  t.Zs = b.take<double>(base, nk * (size_t)gwb_heev_scratch_doubles((int32_t)hm));
   t.rn = b.take<double>(base, nk * nb);
   t.eig = b.take<double>(base, nk * nb);
   t.eig2 = b.take<double>(base, nk * nb);

@@ -195,9 +195,16 @@ __device__ __forceinline__ void apply_reflectors(cplx<double> (&y)[NV][PER], int
 }
 
 // Per-matrix float64 scratch of the eigensolver: packed reflectors
-// (heev_h_doubles), then d (m), the complex subdiagonal (2m), the reflector
-// scales (m); the QL rotation log reuses the first m*m.
-__host__ __device__ inline size_t heev_scratch_doubles(int m) { return (size_t)m * (m + 8); }
+// (heev_h_doubles), d (m), the complex subdiagonal (2m), the reflector scales
+// (m), the phases D (2m), a flag (1: the back-transform kernel builds the
+// eigenvectors; 0: the QL path already wrote them) and, from m (m + 8) on,
+// the wanted eigenvectors of T_r (nb columns of m). The QL rotation log
+// reuses the first m*m.
+__host__ __device__ inline size_t heev_scratch_doubles(int m) { return (size_t)m * (2 * m + 8); }
+__host__ __device__ inline size_t heev_off_d(int m) { return (size_t)m * (m > 0 ? m - 1 : 0); }
+__host__ __device__ inline size_t heev_off_ph(int m) { return heev_off_d(m) + 4 * (size_t)m; }
+__host__ __device__ inline size_t heev_off_flag(int m) { return heev_off_ph(m) + 2 * (size_t)m; }
+__host__ __device__ inline size_t heev_off_v(int m) { return (size_t)m * (m + 8); }
 
 constexpr int TRI_THREADS = 512;
 constexpr int TRI_WARPS = TRI_THREADS / 32;
@@ -831,85 +838,72 @@ __global__ void __launch_bounds__(HEEV_THREADS, 1)
       }
     }
     __syncthreads();
-    // eigenvectors: v = Z Q[:, src], residual |T v - theta v|, y = Q_H D v;
-    // each warp carries VPW vectors through the reflectors together
-    constexpr int VPW = 4;
-    cplx<double>* Uk = U + (int64_t)k * m * nb;
+    // eigenvectors of T_r: v = Z Q[:, src] into the scratch (k_heev_backtransform
+    // applies D and the reflectors), with the residual |T v - theta v| checked
+    double* Vk = Zglob + heev_off_v(m);
     const double rtol = 64.0 * EPS * tnorm;
-    for (int rb = 0; rb < nb; rb += HEEV_WARPS * VPW) {
-      cplx<double> y[VPW][PER];
-      double ths[VPW];
+    for (int ra = warp; ra < nb; ra += HEEV_WARPS) {
+      const int src = order[ra];
+      const double th = Hm[src * nbx + src];
+      double v[PER];
 #pragma unroll
-      for (int sv = 0; sv < VPW; ++sv) {
-        const int ra = rb + warp + HEEV_WARPS * sv;
-        ths[sv] = 0.0;
-#pragma unroll
-        for (int t = 0; t < PER; ++t) y[sv][t] = mk<double>(0.0, 0.0);
-        if (ra >= nb) continue;  // warp-uniform
-        const int src = order[ra];
-        const double th = Hm[src * nbx + src];
-        ths[sv] = th;
-        double v[PER];
-#pragma unroll
-        for (int t = 0; t < PER; ++t) v[t] = 0.0;
-        for (int b = 0; b < nbx; ++b) {
-          const double qb = Qm[b * nbx + src];
-          if (qb == 0.0) continue;
-#pragma unroll
-          for (int t = 0; t < PER; ++t) {
-            const int i = lane + 32 * t;
-            if (i < m) v[t] = fma(zT[b * ldz + i], qb, v[t]);
-          }
-        }
-        double res = 0.0;
+      for (int t = 0; t < PER; ++t) v[t] = 0.0;
+      for (int b = 0; b < nbx; ++b) {
+        const double qb = Qm[b * nbx + src];
+        if (qb == 0.0) continue;
 #pragma unroll
         for (int t = 0; t < PER; ++t) {
           const int i = lane + 32 * t;
-          const double up = __shfl_up_sync(0xffffffffu, v[t], 1);
-          const double wrapu = __shfl_sync(0xffffffffu, t > 0 ? v[t > 0 ? t - 1 : 0] : 0.0, 31);
-          const double dn = __shfl_down_sync(0xffffffffu, v[t], 1);
-          const double wrapd = __shfl_sync(0xffffffffu, t + 1 < PER ? v[t + 1 < PER ? t + 1 : t] : 0.0, 0);
-          const double vm = lane > 0 ? up : wrapu, vp = lane < 31 ? dn : wrapd;
-          if (i < m) {
-            double tv = (d[i] - th) * v[t];
-            if (i > 0) tv = fma(er[i - 1], vm, tv);
-            if (i + 1 < m) tv = fma(er[i], vp, tv);
-            res = fma(tv, tv, res);
-          }
-        }
-        res = warp_sum(res);
-        if (lane == 0) atomicMax(&g_heev_maxres, (unsigned long long)__double_as_longlong(sqrt(res) / tnorm));
-        if (!(res <= rtol * rtol)) {
-          if (lane == 0) s_fail = 4;
-        }
-#pragma unroll
-        for (int t = 0; t < PER; ++t) {
-          const int r = lane + 32 * t;
-          y[sv][t] = r < m ? scale(ph[r], v[t]) : mk<double>(0.0, 0.0);
+          if (i < m) v[t] = fma(zT[b * ldz + i], qb, v[t]);
         }
       }
-      apply_reflectors<VPW>(y, m, lane, Hc, wv);
+      double res = 0.0;
 #pragma unroll
-      for (int sv = 0; sv < VPW; ++sv) {
-        const int ra = rb + warp + HEEV_WARPS * sv;
-        if (ra >= nb) continue;
-#pragma unroll
-        for (int t = 0; t < PER; ++t) {
-          const int r = lane + 32 * t;
-          if (r < m) Uk[(int64_t)r * nb + ra] = y[sv][t];
+      for (int t = 0; t < PER; ++t) {
+        const int i = lane + 32 * t;
+        const double up = __shfl_up_sync(0xffffffffu, v[t], 1);
+        const double wrapu = __shfl_sync(0xffffffffu, t > 0 ? v[t > 0 ? t - 1 : 0] : 0.0, 31);
+        const double dn = __shfl_down_sync(0xffffffffu, v[t], 1);
+        const double wrapd = __shfl_sync(0xffffffffu, t + 1 < PER ? v[t + 1 < PER ? t + 1 : t] : 0.0, 0);
+        const double vm = lane > 0 ? up : wrapu, vp = lane < 31 ? dn : wrapd;
+        if (i < m) {
+          double tv = (d[i] - th) * v[t];
+          if (i > 0) tv = fma(er[i - 1], vm, tv);
+          if (i + 1 < m) tv = fma(er[i], vp, tv);
+          res = fma(tv, tv, res);
         }
-        if (lane == 0) eig[(int64_t)k * nb + ra] = ths[sv];
       }
+      res = warp_sum(res);
+      if (lane == 0) atomicMax(&g_heev_maxres, (unsigned long long)__double_as_longlong(sqrt(res) / tnorm));
+      if (!(res <= rtol * rtol)) {
+        if (lane == 0) s_fail = 4;
+      }
+#pragma unroll
+      for (int t = 0; t < PER; ++t) {
+        const int i = lane + 32 * t;
+        if (i < m) Vk[(int64_t)ra * m + i] = v[t];
+      }
+      if (lane == 0) eig[(int64_t)k * nb + ra] = th;
     }
     __syncthreads();
     if (!s_fail) {
-      if (tid == 0) info[k] = 0;
+      for (int i = tid; i < m; i += blockDim.x) {
+        Zglob[heev_off_ph(m) + 2 * i] = ph[i].x;
+        Zglob[heev_off_ph(m) + 2 * i + 1] = ph[i].y;
+      }
+      if (tid == 0) {
+        Zglob[heev_off_flag(m)] = 1.0;
+        info[k] = 0;
+      }
       return;
     }
   }
 
   // ---- QL path: implicit QL on (d, er), Z in the pool -----------------------
-  if (tid == 0) atomicAdd(&g_heev_ql[s_fail > 0 ? s_fail - 1 : 0], 1ull);
+  if (tid == 0) {
+    atomicAdd(&g_heev_ql[s_fail > 0 ? s_fail - 1 : 0], 1ull);
+    Zglob[heev_off_flag(m)] = 0.0;  // the eigenvectors are written here, not by the back-transform kernel
+  }
   double* Z = pool;  // Z(row r, col i) at Z[i*m + r]; pool_n >= m*m
   double* dq = lam;  // the QL recurrence works on copies of d and er
   double* eq = e2;
@@ -925,7 +919,7 @@ __global__ void __launch_bounds__(HEEV_THREADS, 1)
     // header {-(mm+2), ilo} followed by its rotations {c, s} (i = mm-1 .. ilo);
     // then every thread replays the log on its rows of Z. The d/e recurrence
     // never reads Z, so batches need only two barriers each.
-    // plain doubles: the per-matrix offset k*m*(m+8) is only 8-byte aligned for odd m
+    // plain doubles: the per-matrix offset k*m*(2m+8) is only 8-byte aligned for odd m
     double* lg = Zglob;
     const int cap = (m * m) / 2;  // entries of two doubles
     int l = 0, iter = 0;          // scalar QL state, used by thread 0 only
@@ -1076,6 +1070,61 @@ __global__ void __launch_bounds__(HEEV_THREADS, 1)
   }
 }
 
+// Stage 5 on many SMs: y = Q_H D v for the eigenvectors v of T_r that
+// k_heev_lowest left in the scratch. Grid (k, groups of BT_WARPS * BT_NV
+// vectors); the CTA stages the packed reflectors in shared memory, and each
+// warp carries BT_NV vectors through them. Matrices the QL path solved (flag
+// 0) are skipped: their eigenvectors are already in U.
+constexpr int BT_WARPS = 4, BT_NV = 2;
+
+__global__ void __launch_bounds__(BT_WARPS * 32) k_heev_backtransform(int m, int nb, const double* __restrict__ Zg,
+                                                                      cplx<double>* __restrict__ U) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int k = blockIdx.x;
+  const double* Zk = Zg + (int64_t)k * heev_scratch_doubles(m);
+  if (Zk[heev_off_flag(m)] == 0.0) return;
+  const int hcount = m >= 3 ? hoff(m, m - 2) : 0;
+  cplx<double>* Hc = reinterpret_cast<cplx<double>*>(smem_raw);
+  cplx<double>* phs = Hc + hcount;
+  double* wvs = reinterpret_cast<double*>(phs + m);
+  for (int i = threadIdx.x; i < hcount; i += blockDim.x) Hc[i] = mk<double>(Zk[2 * i], Zk[2 * i + 1]);
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    phs[i] = mk<double>(Zk[heev_off_ph(m) + 2 * i], Zk[heev_off_ph(m) + 2 * i + 1]);
+    wvs[i] = Zk[heev_off_d(m) + 3 * (size_t)m + i];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int a0 = (blockIdx.y * BT_WARPS + warp) * BT_NV;
+  if (a0 >= nb) return;  // warp-uniform; no barrier follows
+  const double* Vk = Zk + heev_off_v(m);
+  cplx<double> y[BT_NV][PER];
+#pragma unroll
+  for (int sv = 0; sv < BT_NV; ++sv) {
+    const int ra = a0 + sv;
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+      const int r = lane + 32 * t;
+      y[sv][t] = (ra < nb && r < m) ? scale(phs[r], Vk[(int64_t)ra * m + r]) : mk<double>(0.0, 0.0);
+    }
+  }
+  apply_reflectors<BT_NV>(y, m, lane, Hc, wvs);
+  cplx<double>* Uk = U + (int64_t)k * m * nb;
+#pragma unroll
+  for (int sv = 0; sv < BT_NV; ++sv) {
+    const int ra = a0 + sv;
+    if (ra >= nb) continue;
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+      const int r = lane + 32 * t;
+      if (r < m) Uk[(int64_t)r * nb + ra] = y[sv][t];
+    }
+  }
+}
+static size_t bt_smem(int m) {
+  const size_t hcount = m >= 3 ? (size_t)((m - 2) * (m - 1) - (m - 2) * (m - 3) / 2) : 0;
+  return hcount * 16 + (size_t)m * 16 + (size_t)m * 8;
+}
+
 // Shared memory: matrix storage + extra pool + per-matrix vectors, within the
 // 227 KB opt-in limit; the extra pool lets stages 3-4 hold every vector at once.
 static int heev_extra(int m, int nb) {
@@ -1101,8 +1150,12 @@ static int launch_heev(int nk, int m, int nb, const void* S, int lds, int64_t sk
   const size_t sm = heev_smem(m, nb);
   GWB_CUDA_TRY(cudaFuncSetAttribute(k_heev_lowest, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   k_heev_lowest<<<nk, HEEV_THREADS, sm, st>>>(m, nb, eig, (cplx<double>*)U, z, info, extra);
+  const size_t sm3 = bt_smem(m);
+  GWB_CUDA_TRY(cudaFuncSetAttribute(k_heev_backtransform, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3));
+  dim3 g3(nk, (nb + BT_WARPS * BT_NV - 1) / (BT_WARPS * BT_NV));
+  k_heev_backtransform<<<g3, BT_WARPS * 32, sm3, st>>>(m, nb, z, (cplx<double>*)U);
   GWB_LAUNCH_CHECK();
-  count_launches(2);
+  count_launches(3);
   return GWB_OK;
 }
 
@@ -1147,7 +1200,7 @@ extern "C" int gwb_heev_ql_count(unsigned long long* out) {
 // Limits and sharing:
 //   * the array holds GWB_HEEV_NOALLOC_DOUBLES float64 (8 MiB); every GPU that
 //     loads libgwb.so holds it until the process exits;
-//   * a call needs nk * m * (m + 8) float64 of it; larger problems are rejected with
+//   * a call needs nk * m * (2m + 8) float64 of it; larger problems are rejected with
 //     GWB_ERR_ARG (use gwb_heev_lowest with caller-provided scratch);
 //   * every call on a device uses the same array and leaves its last contents
 //     there; the kernel writes every element of Z it reads (identity fill), so
@@ -1174,7 +1227,7 @@ extern "C" int gwb_heev_lowest_noalloc(int32_t nk, int32_t m, int32_t nb, const 
   GWB_REQUIRE(m <= GWB_HEEV_MMAX, "m exceeds the shared-memory eigensolver limit (112)");
   GWB_REQUIRE(S && eig && U && info, "null pointer");
   if ((int64_t)nk * (int64_t)heev_scratch_doubles(m) > (int64_t)GWB_HEEV_NOALLOC_DOUBLES) {
-    set_error("gwb_heev_lowest_noalloc: nk*m*(m+8) = " + std::to_string((int64_t)nk * (int64_t)heev_scratch_doubles(m)) +
+    set_error("gwb_heev_lowest_noalloc: nk*m*(2m+8) = " + std::to_string((int64_t)nk * (int64_t)heev_scratch_doubles(m)) +
               " float64 of scratch exceeds the fixed " + std::to_string(GWB_HEEV_NOALLOC_DOUBLES) +
               " (8 MiB); call gwb_heev_lowest with caller-provided scratch");
     return GWB_ERR_ARG;

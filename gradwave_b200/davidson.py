@@ -156,7 +156,7 @@ class _Workspace:
         self.eig = torch.zeros(nk, nb, dtype=torch.float64, device=dev)
         hm = min(max_dim, heev_max)
         self.U = torch.zeros(nk, max(hm, nb), nb, **c)
-        self.Z = torch.zeros(nk, hm * (hm + 8), dtype=torch.float64, device=dev)
+        self.Z = torch.zeros(nk, int(_lib.load().gwb_heev_scratch_doubles(hm)), dtype=torch.float64, device=dev)
         self.Gs = torch.zeros(nk, nb, nb, **c)
 
 

@@ -187,7 +187,7 @@ int gwb_row_repair(int32_t nk, int32_t n, int32_t npw, void* D, int64_t d_kstrid
 int gwb_heev_lowest(int32_t nk, int32_t m, int32_t nb, const void* S, int32_t lds, int64_t s_kstride,
                     double* eig, void* U, double* zscratch, int32_t* info, void* stream);
 int gwb_heev_max_dim(void);
-/* Scratch float64 per matrix that gwb_heev_lowest needs: m * (m + 8). */
+/* Scratch float64 per matrix that gwb_heev_lowest needs: m * (2m + 8). */
 int64_t gwb_heev_scratch_doubles(int32_t m);
 /* Diagnostics of gwb_heev_lowest on the current device since load: out[0..3]
  * matrices sent down the QL fallback by reason (pool too small for the
@@ -201,7 +201,7 @@ int gwb_heev_ql_count(unsigned long long* out);
  * array inside the library (held on every GPU that loads it). For callers
  * whose device memory belongs to a pool allocator or a fixed budget and who
  * therefore cannot call cudaMalloc. No counterpart in the reference.
- * Limits: nk*m*(m+8) <= 1048576 (else GWB_ERR_ARG); calls share the array, so
+ * Limits: nk*m*(2m+8) <= 1048576 (else GWB_ERR_ARG); calls share the array, so
  * calls whose kernels may overlap on the GPU race and must be ordered; the
  * first call on a device looks up the array's address and should come before
  * any stream capture. */

@@ -67,7 +67,7 @@ def test_noalloc_matches_allocating_entry_twice(cuda_device):
 
 def test_noalloc_rejects_oversized_request(cuda_device):
     from gradwave_b200 import _lib
-    nk, m, nb = 200, 96, 8          # 200 * 96 * 104 = 2.0M float64 > the fixed 1M
+    nk, m, nb = 200, 96, 8          # 200 * 96 * 200 = 3.8M float64 > the fixed 1M
     dummy = torch.zeros(1, dtype=torch.complex128, device=cuda_device)
     with pytest.raises(_lib.GwbError) as err:
         _lib.call("gwb_heev_lowest_noalloc", nk, m, nb, dummy.data_ptr(), m, m * m, dummy.data_ptr(),
