@@ -8,7 +8,6 @@
 #include <cublas_v2.h>
 
 #include <algorithm>
-#include <mutex>
 #include <string>
 #include <unordered_map>
 
@@ -16,13 +15,14 @@
 
 namespace gwb {
 
-static std::mutex g_blas_mu;
-static std::unordered_map<int, cublasHandle_t> g_blas;
+// One cuBLAS handle per (host thread, device): a handle's stream is set before
+// every call, so threads that drive solves on different streams at the same
+// time must not share one.
+static thread_local std::unordered_map<int, cublasHandle_t> g_blas;
 
 static int blas_handle(cublasHandle_t* out) {
   int dev = 0;
   GWB_CUDA_TRY(cudaGetDevice(&dev));
-  std::lock_guard<std::mutex> lk(g_blas_mu);
   auto it = g_blas.find(dev);
   if (it == g_blas.end()) {
     cublasHandle_t h;

@@ -4,7 +4,10 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <mutex>
+#include <set>
 #include <string>
+#include <utility>
 
 #include "../../include/gwb.h"
 
@@ -79,6 +82,34 @@ template <typename S, typename T> __device__ __forceinline__ void st(S* p, size_
 void set_error(const std::string& msg);
 // Tally of kernels this library launched (gwb_launch_count).
 void count_launches(int n);
+
+// Raise a kernel's dynamic shared-memory cap to the device's opt-in maximum
+// (less its static shared memory), once per (kernel, device). The cap is a
+// process-wide attribute of the kernel: setting it to each launch's own size
+// would let a thread launching a larger size race a thread setting a smaller
+// one (concurrent solves on separate streams). Every caller sets the same
+// value, so there is no such race.
+template <typename F>
+inline cudaError_t allow_smem(F* func) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  const auto key = std::make_pair(reinterpret_cast<const void*>(func), dev);
+  if (done.count(key)) return cudaSuccess;
+  int optin = 0;
+  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  cudaFuncAttributes fa;
+  e = cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(func));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(reinterpret_cast<const void*>(func), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           optin - (int)fa.sharedSizeBytes);
+  if (e == cudaSuccess) done.insert(key);
+  return e;
+}
 
 }  // namespace gwb
 

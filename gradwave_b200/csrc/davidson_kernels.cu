@@ -391,7 +391,7 @@ int gwb_chol_inv(int32_t nk, int32_t n, void* G, int32_t ldg, int64_t g_kstride,
   GWB_REQUIRE(G && Linv && info, "null pointer");
   if (n <= CHOL_SMEM_MAX) {
     const size_t sm = (size_t)2 * n * n * sizeof(cplx<double>);
-    GWB_CUDA_TRY(cudaFuncSetAttribute(k_chol_inv_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    GWB_CUDA_TRY(allow_smem(k_chol_inv_smem));
     k_chol_inv_smem<<<nk, 256, sm, (cudaStream_t)stream>>>((cplx<double>*)G, n, ldg, g_kstride,
                                                           (cplx<double>*)Linv, linv_kstride, info, flag);
   } else {

@@ -1144,14 +1144,14 @@ size_t heev_smem(int m, int nb) { return heev_a_doubles(m) * 8 + (size_t)heev_ex
 static int launch_heev(int nk, int m, int nb, const void* S, int lds, int64_t sk, double* eig, void* U,
                        double* z, int* info, cudaStream_t st) {
   const size_t sm1 = tri_smem(m);
-  GWB_CUDA_TRY(cudaFuncSetAttribute(k_heev_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+  GWB_CUDA_TRY(allow_smem(k_heev_tridiag));
   k_heev_tridiag<<<nk, TRI_THREADS, sm1, st>>>((const cplx<double>*)S, lds, sk, m, z);
   const int extra = heev_extra(m, nb);
   const size_t sm = heev_smem(m, nb);
-  GWB_CUDA_TRY(cudaFuncSetAttribute(k_heev_lowest, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  GWB_CUDA_TRY(allow_smem(k_heev_lowest));
   k_heev_lowest<<<nk, HEEV_THREADS, sm, st>>>(m, nb, eig, (cplx<double>*)U, z, info, extra);
   const size_t sm3 = bt_smem(m);
-  GWB_CUDA_TRY(cudaFuncSetAttribute(k_heev_backtransform, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3));
+  GWB_CUDA_TRY(allow_smem(k_heev_backtransform));
   dim3 g3(nk, (nb + BT_WARPS * BT_NV - 1) / (BT_WARPS * BT_NV));
   k_heev_backtransform<<<g3, BT_WARPS * 32, sm3, st>>>(m, nb, z, (cplx<double>*)U);
   GWB_LAUNCH_CHECK();

@@ -577,19 +577,19 @@ static int local_chunks(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t 
   const cplx<T>* tw2 = dbl ? (const cplx<T>*)h->d_tw64[2] : (const cplx<T>*)h->d_tw32[2];
   const T* v = dbl ? (const T*)h->d_v64 : (const T*)h->d_v32;
   const T* t = dbl ? (const T*)h->d_t64 : (const T*)h->d_t32;
-  GWB_CUDA_TRY(cudaFuncSetAttribute(k_plane_inverse<T, SIO, C, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA));
-  GWB_CUDA_TRY(cudaFuncSetAttribute(k_plane_forward<T, SIO, C, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA));
-  GWB_CUDA_TRY(cudaFuncSetAttribute(k_pencil_vloc<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
+  GWB_CUDA_TRY(allow_smem(k_plane_inverse<T, SIO, C, C>));
+  GWB_CUDA_TRY(allow_smem(k_plane_forward<T, SIO, C, C>));
+  GWB_CUDA_TRY(allow_smem(k_pencil_vloc<T, C>));
   cplx<T>* W = (cplx<T>*)h->d_W;
   const bool cubic = g.n[0] == g.n[1] && g.n[1] == g.n[2];
   const int nreg = (cubic && g.n[0] == 36 && C == kCode36) ? 36 : ((cubic && g.n[0] == 24 && C == kCode24) ? 24 : 0);
   const size_t smR = (size_t)PLR * nreg * (nreg + 1) * sizeof(cplx<T>);
   if (nreg == 36) {
-    GWB_CUDA_TRY(cudaFuncSetAttribute(k_plane_inverse_reg<T, SIO, 36>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smR));
-    GWB_CUDA_TRY(cudaFuncSetAttribute(k_plane_forward_reg<T, SIO, 36>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smR));
+    GWB_CUDA_TRY(allow_smem(k_plane_inverse_reg<T, SIO, 36>));
+    GWB_CUDA_TRY(allow_smem(k_plane_forward_reg<T, SIO, 36>));
   } else if (nreg == 24) {
-    GWB_CUDA_TRY(cudaFuncSetAttribute(k_plane_inverse_reg<T, SIO, 24>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smR));
-    GWB_CUDA_TRY(cudaFuncSetAttribute(k_plane_forward_reg<T, SIO, 24>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smR));
+    GWB_CUDA_TRY(allow_smem(k_plane_inverse_reg<T, SIO, 24>));
+    GWB_CUDA_TRY(allow_smem(k_plane_forward_reg<T, SIO, 24>));
   }
   for (int b0 = 0; b0 < nb; b0 += nbc) {
     const int cb = std::min(nbc, nb - b0);

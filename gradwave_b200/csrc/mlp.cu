@@ -592,7 +592,7 @@ int gwb_mlp_forward(const float* params, int32_t n, const float* feats, float* o
   GWB_REQUIRE(params && feats && out && n >= 0, "bad arguments");
   if (n == 0) return GWB_OK;
   const size_t sm = NPARAM * sizeof(float);
-  GWB_CUDA_TRY(cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  GWB_CUDA_TRY(allow_smem(k_mlp_forward));
   const int blocks = std::min((n + 255) / 256, 4 * 148);
   k_mlp_forward<<<blocks, 256, sm, (cudaStream_t)stream>>>(params, n, feats, out);
   GWB_LAUNCH_CHECK();
@@ -605,7 +605,7 @@ int gwb_mlp_loss_grad(const float* params, int32_t n, const float* feats, const 
   GWB_REQUIRE(params && feats && target && weight && grad && loss && n >= 0, "bad arguments");
   if (n == 0) return GWB_OK;
   const size_t sm = (2 * NPARAM + TS * NIN + 8 * TS * HID + TS) * sizeof(float);
-  GWB_CUDA_TRY(cudaFuncSetAttribute(k_mlp_loss_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  GWB_CUDA_TRY(allow_smem(k_mlp_loss_grad));
   const int tiles = (n + TS - 1) / TS;
   const int blocks = std::min(tiles, 2 * 148);
   k_mlp_loss_grad<<<blocks, 256, sm, (cudaStream_t)stream>>>(params, n, feats, target, weight, grad, loss);
@@ -630,7 +630,7 @@ int gwb_mlp_backward(const float* params, int32_t n, const float* feats, const f
   GWB_REQUIRE(params && feats && dout && grad && n >= 0, "bad arguments");
   if (n == 0) return GWB_OK;
   const size_t sm = (2 * NPARAM + TS * NIN + 8 * TS * HID + TS) * sizeof(float);
-  GWB_CUDA_TRY(cudaFuncSetAttribute(k_mlp_loss_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  GWB_CUDA_TRY(allow_smem(k_mlp_loss_grad));
   const int tiles = (n + TS - 1) / TS;
   const int blocks = std::min(tiles, 2 * 148);
   k_mlp_loss_grad<<<blocks, 256, sm, (cudaStream_t)stream>>>(params, n, feats, nullptr, dout, grad, nullptr);

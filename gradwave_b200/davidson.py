@@ -513,6 +513,76 @@ def _native_solve(ham, x0, t, mask, tol, max_iter, max_dim, mode, time_applies=F
     return BatchedDavidsonResult(eig, vec, int(st.n_iter), rn, int(st.n_apply_low), int(st.n_apply_full), info)
 
 
+def _k_groups() -> int:
+    """Number of concurrent k-groups of a native solve (``GWB_KGROUPS``)."""
+    try:
+        return max(1, int(os.environ.get("GWB_KGROUPS", "1")))
+    except ValueError:
+        raise ValueError("GWB_KGROUPS must be a positive integer") from None
+
+
+def _native_solve_grouped(ham, x0, t, mask, tol, max_iter, max_dim_factor, mode, time_applies, model, groups):
+    """The k-points split into contiguous groups balanced by plane-wave count,
+    each solved by the native driver from its own host thread on its own CUDA
+    stream. Every k is an independent eigenproblem, so the groups need no
+    communication; running them side by side lets one group's latency-bound
+    steps (the per-k subspace eigensolver, one CTA per k) overlap another
+    group's bandwidth-bound applies and products on the same GPU. None when a
+    group reports an unrepaired breakdown (the caller retries on the host)."""
+    import threading
+    from .sharding import shard_range_weighted
+    nk, nb = int(x0.shape[0]), int(x0.shape[1])
+    g_n = min(groups, nk)
+    cost = mask.sum(dim=1).to("cpu", torch.float64).numpy()
+    ranges = [shard_range_weighted(cost, g, g_n) for g in range(g_n)]
+    dev = x0.device
+    main = torch.cuda.current_stream(dev)
+    streams = ham.__dict__.setdefault("_group_streams", {})
+    for g in range(g_n):
+        if g not in streams:
+            streams[g] = torch.cuda.Stream(device=dev)
+    subs = [ham.k_slice(s, e) for s, e in ranges]
+    results: list = [None] * g_n
+    errors: list = [None] * g_n
+
+    def work(g):
+        try:
+            s, e = ranges[g]
+            md = min(max_dim_factor * nb, int(mask[s:e].sum(dim=1).min()))
+            with torch.cuda.device(dev), torch.cuda.stream(streams[g]):
+                results[g] = _native_solve(subs[g], x0[s:e], t[s:e], mask[s:e], tol, max_iter, md, mode,
+                                           time_applies=time_applies, model=model)
+        except BaseException as exc:  # re-raised on the caller's thread
+            errors[g] = exc
+
+    for g in range(g_n):
+        streams[g].wait_stream(main)
+    threads = [threading.Thread(target=work, args=(g,)) for g in range(g_n)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    for g in range(g_n):
+        main.wait_stream(streams[g])
+    for exc in errors:
+        if exc is not None:
+            raise exc
+    if any(r is None for r in results):
+        return None
+    for r in results:  # the group outputs are read on the caller's stream from here on
+        for x in (r.eigenvalues, r.eigenvectors, r.residual_norms):
+            x.record_stream(main)
+    info = {"native": True, "k_groups": g_n, "max_dim": max(r.info["max_dim"] for r in results)}
+    for key in ("n_restart", "n_cert", "n_repair", "n_rollback", "n_apply_calls", "apply_ms"):
+        if key in results[0].info:
+            info[key] = sum(r.info[key] for r in results)
+    return BatchedDavidsonResult(torch.cat([r.eigenvalues for r in results]),
+                                 torch.cat([r.eigenvectors for r in results]),
+                                 max(r.n_iter for r in results),
+                                 torch.cat([r.residual_norms for r in results]),
+                                 sum(r.n_apply_low for r in results), sum(r.n_apply_full for r in results), info)
+
+
 def davidson_batched(h_apply, x0, t, mask, tol: float = 1e-9, max_iter: int = 40, max_dim_factor: int = 4,
                      sync_free: bool = False, history_out=None, *, mode: str = "fp64",
                      precond="teter") -> BatchedDavidsonResult:
@@ -537,9 +607,15 @@ def davidson_batched(h_apply, x0, t, mask, tol: float = 1e-9, max_iter: int = 40
                        or hasattr(precond, "params"))
                   and history_out is None and int(x0.shape[1]) <= max_dim <= int(_lib.load().gwb_heev_max_dim()))
         if native:
-            res = _native_solve(ham, x0, t, mask, tol, max_iter, max_dim, mode,
-                                time_applies=os.environ.get("GWB_TIME_APPLIES", "0") == "1",
-                                model=getattr(precond, "params", None))
+            time_applies = os.environ.get("GWB_TIME_APPLIES", "0") == "1"
+            model = getattr(precond, "params", None)
+            groups = _k_groups()
+            if groups > 1 and int(x0.shape[0]) > 1 and hasattr(ham, "k_slice"):
+                res = _native_solve_grouped(ham, x0, t, mask, tol, max_iter, max_dim_factor, mode, time_applies,
+                                            model, groups)
+            else:
+                res = _native_solve(ham, x0, t, mask, tol, max_iter, max_dim, mode, time_applies=time_applies,
+                                    model=model)
             if res is not None:
                 return res
         return _Solver(h_apply, x0, t, mask, tol, max_iter, max_dim_factor, mode, precond, history_out).run()

@@ -144,5 +144,17 @@ class BatchedHamiltonian:
             self._ws = ws
         return ws
 
+    def k_slice(self, start: int, end: int) -> "BatchedHamiltonian":
+        """The Hamiltonian of the k-points [start, end) (its own handle and
+        scratch, cached): the unit of the k-group solves, which run
+        concurrently on separate streams."""
+        cache = self.__dict__.setdefault("_kslices", {})
+        key = (int(start), int(end))
+        if key not in cache:
+            from .sharding import slice_batched
+            cache[key] = BatchedHamiltonian(slice_batched(self.bk, start, end), self.shape, self.v_eff_r,
+                                            self.p[start:end])
+        return cache[key]
+
     def scratch_bytes(self) -> int:
         return int(_lib.load().gwb_ham_scratch_bytes(self._h))
