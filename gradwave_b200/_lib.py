@@ -87,6 +87,10 @@ _SIGNATURES = {
                   _D, _D, _P, _I64, _I64, _I64, _P],
     "gwb_zgemm_nh": [_I64, _I64, _I64, _D, _D, _P, _I64, _I64, _P, _I64, _I64, _D, _D, _P, _I64, _I64, _I64, _P,
                      ctypes.c_size_t, _P],
+    "gwb_tc_planes": [_I64, _I64, _I64, _P, _I64, _I64, ctypes.c_int, ctypes.c_int, _P, _I64, _I64, _I64, _P],
+    "gwb_zgemm_tc_work_bytes": [ctypes.c_int, _I64, _I64, _I64, _I64],
+    "gwb_zgemm_tc": [ctypes.c_int, _I64, _I64, _I64, _D, _D, _P, _I64, _I64, _P, _I64, _I64, _D, _D, _P, _I64, _I64,
+                     _I64, _P, ctypes.c_size_t, _P, _P],
     "gwb_residual": [_I, _I, _I, _P, _I64, _P, _I64, _P, _I64, _P, _I64, _P, _P],
     "gwb_conv_stats": [_I, _I, _P, _D, _P, _P],
     "gwb_select_worst": [_I, _I, _P, _I, _P, _P],
@@ -115,7 +119,7 @@ _SIGNATURES = {
 _RESTYPES = {"gwb_last_error": ctypes.c_char_p, "gwb_version": ctypes.c_char_p,
              "gwb_launch_count": ctypes.c_ulonglong,
              "gwb_ham_scratch_bytes": ctypes.c_size_t, "gwb_heev_scratch_doubles": ctypes.c_int64,
-             "gwb_precond_learned_work_bytes": ctypes.c_int64}
+             "gwb_precond_learned_work_bytes": ctypes.c_int64, "gwb_zgemm_tc_work_bytes": ctypes.c_int64}
 
 
 def declared_symbols() -> list[str]:

@@ -32,6 +32,13 @@ Modes:
                       than 30 % counts as a float32 stall only once the
                       residual is within 100x of the float32 floor (early
                       rounds stagnate without any precision limit).
+In both float32-expansion modes the first of the two projection passes of
+the expansion block, D -= (D V^H) V, runs as split-precision BF16 products on
+the tensor cores (``gradwave_b200.tc``, error ~1e-5 relative) against a BF16
+plane copy of the basis kept current row block by row block; the float64
+second pass then removes that error, so the block is orthogonal to the basis
+to float64 round-off as before (``GWB_TC_PROJECT=0`` keeps both passes in
+float64).
 ``precond`` is ``"teter"`` or an object with ``apply_into(...)`` (the learned
 preconditioner, ``gradwave_b200.learned``), which falls back to TPA per band.
 """
@@ -200,6 +207,14 @@ class _Solver:
         self.stream = _lib.stream_ptr(self.dev)
         self.x0 = x0
         self.prof = _PhaseTimer(os.environ.get("GWB_PROFILE", "0") == "1")
+        # tensor-core first projection pass (float32-expansion modes): BF16
+        # planes of the basis V, of the expansion block D and of D V^H
+        self.tc = None
+        if mode in ("fp32exp", "mixed") and x0.dtype == torch.complex128 and _tc_projection():
+            from .tc import PlaneSet
+            self.tc = (PlaneSet(self.nk, self.max_dim, self.npw, self.dev),
+                       PlaneSet(self.nk, self.nb, self.npw, self.dev),
+                       PlaneSet(self.nk, self.nb, self.max_dim, self.dev))
 
     # -- primitives -----------------------------------------------------------
     def apply_block(self, src: torch.Tensor, src_off: int, src_ks: int, nrows: int, dst: torch.Tensor,
@@ -248,6 +263,26 @@ class _Solver:
                 Z[:, :n].copy_(Ztmp[:, :n])
         return True
 
+    def v_rows_changed(self, r0: int, r1: int):
+        """Refresh the BF16 planes of basis rows [r0, r1) (tensor-core pass)."""
+        if self.tc is not None and r1 > r0:
+            md, npw = self.max_dim, self.npw
+            self.tc[0].write(self.ws.V, r1 - r0, row0=r0, src_ld=npw, src_kstride=md * npw, offset=r0 * npw,
+                             stream=self.stream)
+
+    def project_tc(self, n: int, m: int):
+        """D -= (D V^H) V over the first m basis rows as split-BF16
+        tensor-core products (error ~1e-5 relative; a float64 pass follows)."""
+        from .tc import OP_H, OP_N, zgemm_tc
+        pv, pd, pc = self.tc
+        ws, npw = self.ws, self.npw
+        ds = ws.D.shape[1] * npw
+        pd.write(ws.D, n, src_ld=npw, src_kstride=ds, stream=self.stream)
+        zgemm_tc(OP_H, n, m, npw, pd, pv, ws.C, m, n * m, stream=self.stream, status=ws.flags)
+        pc.write(ws.C, n, src_ld=m, src_kstride=n * m, cols=m, stream=self.stream)
+        zgemm_tc(OP_N, n, npw, m, pc, pv, ws.D, npw, ds, alpha=-1.0, beta=1.0, stream=self.stream,
+                 status=ws.flags)
+
     def project_out(self, Dblk: torch.Tensor, n: int, m: int, passes: int = 2):
         """D -= (D V^H) V over the first m basis rows (float64 GEMMs)."""
         ws, nk, npw, md = self.ws, self.nk, self.npw, self.max_dim
@@ -272,7 +307,10 @@ class _Solver:
         D[:, :n].mul_(self.mask[:, None, :])
         if not safe:
             if m:
-                self.project_out(D, n, m, passes=1)
+                if self.tc is not None:
+                    self.project_tc(n, m)
+                else:
+                    self.project_out(D, n, m, passes=1)
             _lib.call("gwb_row_repair", self.nk, n, self.npw, _ptr(D), D.shape[1] * self.npw,
                       _ptr(self.mask_u8), 1e-8, _ptr(ws.flags), self.stream)
             if m:
@@ -373,6 +411,8 @@ class _Solver:
         if st[2] != 0:
             raise _lib.GwbError(_lib.GWB_ERR_NOT_CONVERGED, "subspace eigensolver: QL iteration limit")
         flags = int(st[3])
+        if flags & _lib.GWB_ERR_TIMEOUT:
+            raise _lib.GwbError(_lib.GWB_ERR_TIMEOUT, "tensor-core projection: a bounded pipeline wait ran out")
         if flags & 1:
             self.n_repair += 1
         self.breakdown = bool(flags & 2)
@@ -384,6 +424,7 @@ class _Solver:
         ws.D[:, :nb].copy_(self.x0.to(torch.complex128))
         self.orthonormalize_new(nb, 0, safe=True)
         ws.V[:, :nb].copy_(ws.D[:, :nb])
+        self.v_rows_changed(0, nb)
         self.apply_block(ws.V, 0, md * npw, nb, ws.HV, 0, md * npw, low=self.fp32_exp)
         # m: basis rows in use; m0: first column of s not formed yet (0 = rebuild)
         m, m0 = nb, 0
@@ -420,6 +461,7 @@ class _Solver:
                         # images and continue with float64 expansion applies
                         ws.V[:, :nb].copy_(ws.X)
                         ws.HV[:, :nb].copy_(ws.HX)
+                        self.v_rows_changed(0, nb)
                         m, m0 = nb, 0
                         self.fp32_exp = False
             if self.history_out is not None:
@@ -441,11 +483,13 @@ class _Solver:
                     ws.HX.copy_(torch.linalg.solve_triangular(r.transpose(-1, -2), ws.HX, upper=False))
                 ws.V[:, :nb].copy_(ws.X)
                 ws.HV[:, :nb].copy_(ws.HX)
+                self.v_rows_changed(0, nb)
                 m, m0 = nb, 0
             with self.prof("orthonormalize"):
                 self.orthonormalize_new(n_add, m, safe=safe_next)
                 safe_next = False
                 ws.V[:, m:m + n_add].copy_(ws.D[:, :n_add])
+                self.v_rows_changed(m, m + n_add)
             with self.prof("apply"):
                 self.apply_block(ws.V, m * npw, md * npw, n_add, ws.HV, m * npw, md * npw, low=self.fp32_exp)
             m_prev = m
@@ -472,6 +516,7 @@ class _Solver:
         if self.out_dtype != torch.complex128:
             x = x.to(self.out_dtype)
         info = {"n_restart": self.n_restart, "n_cert": self.n_cert, "n_fallback_qr": self.n_fallback_qr,
+                "tc_projection": self.tc is not None,
                 "n_repair": self.n_repair, "n_rollback": self.n_rollback,
                 "max_dim": self.max_dim, "phase_ms": self.prof.summary()}
         return BatchedDavidsonResult(eig.clone(), x, it, ws.rn.clone(), self.n_low, self.n_full, info)
@@ -511,6 +556,15 @@ def _native_solve(ham, x0, t, mask, tol, max_iter, max_dim, mode, time_applies=F
     if time_applies:
         info["apply_ms"] = float(st.apply_ms)
     return BatchedDavidsonResult(eig, vec, int(st.n_iter), rn, int(st.n_apply_low), int(st.n_apply_full), info)
+
+
+def _tc_projection() -> bool:
+    """Whether the float32-expansion modes run their first projection pass on
+    the tensor cores (``GWB_TC_PROJECT``, default 1)."""
+    v = os.environ.get("GWB_TC_PROJECT", "1")
+    if v not in ("0", "1"):
+        raise ValueError("GWB_TC_PROJECT must be 0 or 1")
+    return v == "1"
 
 
 def _k_groups() -> int:

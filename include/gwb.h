@@ -135,6 +135,35 @@ int gwb_zgemm_nh(int64_t M, int64_t N, int64_t K, double alpha_re, double alpha_
                  void* C, int64_t ldc, int64_t strideC, int64_t batch, void* work, size_t work_bytes,
                  void* stream);
 
+/* Split-precision complex products on the tensor cores (tcgen05, BF16
+ * operands, FP32 accumulation in tensor memory). An operand is a "plane set":
+ * per batch entry four BF16 planes re_hi, re_lo, im_hi, im_lo (x = hi + lo to
+ * about 2^-17 |x|), each rows_cap x ld (ld a multiple of 8, 16-byte aligned
+ * base), plane q of entry b at element (4 b + q) * rows_cap * ld.
+ *
+ * gwb_tc_planes: rows [0, rows) x cols of complex src (dtype GWB_C64 or
+ * GWB_C128, row stride src_ld, batch stride src_kstride, elements; conj != 0
+ * stores the conjugate) into plane rows [row0, row0 + rows), columns cols..ld-1
+ * zeroed. */
+int gwb_tc_planes(int64_t nk, int64_t rows, int64_t cols, const void* src, int64_t src_ld, int64_t src_kstride,
+                  int dtype, int conj, void* planes, int64_t ld, int64_t rows_cap, int64_t row0, void* stream);
+
+/* C = alpha A op(B) + beta C per batch entry (float64 complex C, row-major,
+ * ldc / strideC in elements); A: M x K planes; opB = 2: op(B) = B^H with B an
+ * N x K plane set; opB = 0: op(B) = B with B a K x N plane set. Twelve BF16
+ * tensor-core products per complex multiply-add (re/im x hi/lo), error about
+ * 2^-15 sum_k |a_ik||b_kj|. opB = 2 splits K over CTAs when the tile grid is
+ * small, with the partial sums in `work` (gwb_zgemm_tc_work_bytes; with less,
+ * fewer splits). A wait that runs out ORs GWB_ERR_TIMEOUT into *status (a
+ * device int). The products of the first projection pass of the
+ * expansion block, gradwave solvers/davidson.py:428-432; no counterpart in
+ * the reference's precision choices (it has float64 and float32 only). */
+int64_t gwb_zgemm_tc_work_bytes(int opB, int64_t M, int64_t N, int64_t K, int64_t batch);
+int gwb_zgemm_tc(int opB, int64_t M, int64_t N, int64_t K, double alpha_re, double alpha_im, const void* A_planes,
+                 int64_t lda, int64_t a_rows_cap, const void* B_planes, int64_t ldb, int64_t b_rows_cap,
+                 double beta_re, double beta_im, void* C, int64_t ldc, int64_t strideC, int64_t batch, void* work,
+                 size_t work_bytes, int* status, void* stream);
+
 /* r = hx - eig * x and rn = |r| per (k, band); eig (nk, eig_kstride) float64.
  * Replaces gradwave solvers/davidson.py:656-657. */
 int gwb_residual(int32_t nk, int32_t nb, int32_t npw, const void* x, int64_t x_kstride, const void* hx,

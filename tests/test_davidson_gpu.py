@@ -109,13 +109,41 @@ def test_native_and_host_driver_agree(cuda_device, monkeypatch):
         native = davidson_batched(h.apply, x0, bk.t, bk.mask, tol=1e-10, max_iter=200, mode=mode)
         assert native.info.get("native")
         monkeypatch.setenv("GWB_NATIVE", "0")
+        monkeypatch.setenv("GWB_TC_PROJECT", "0")  # both passes in float64, as the native driver
         host = davidson_batched(h.apply, x0, bk.t, bk.mask, tol=1e-10, max_iter=200, mode=mode)
         monkeypatch.delenv("GWB_NATIVE")
+        monkeypatch.delenv("GWB_TC_PROJECT")
         assert not host.info.get("native")
         for res in (native, host):
             assert float(res.residual_norms.max()) < 1e-10
             assert np.abs(res.eigenvalues.cpu().numpy() - g["eigenvalues"]).max() < 1e-9
         assert abs(native.n_iter - host.n_iter) <= 3
+
+
+@pytest.mark.parametrize("mode", ["fp32exp", "mixed"])
+def test_tensor_core_projection_pass_keeps_parity(cuda_device, monkeypatch, mode):
+    """The float32-expansion modes of the host driver run the first projection
+    pass as split-BF16 tensor-core products; the float64 second pass removes
+    their error: same eigenvalues as the reference, an orthonormal block, and
+    about the same number of rounds as with both passes in float64."""
+    from gradwave_b200.davidson import davidson_batched
+    g = load_golden("si8_cubic")
+    ci, bk, h = _cell_ham("si8_cubic")
+    x0 = ci.identity_start().to(cuda_device)
+    monkeypatch.setenv("GWB_NATIVE", "0")
+    runs = {}
+    for tc in ("1", "0"):
+        monkeypatch.setenv("GWB_TC_PROJECT", tc)
+        runs[tc] = davidson_batched(h.apply, x0, bk.t, bk.mask, tol=1e-10, max_iter=200, mode=mode)
+    res = runs["1"]
+    assert res.info["tc_projection"] and not runs["0"].info["tc_projection"]
+    assert float(res.residual_norms.max()) < 1e-10
+    assert np.abs(res.eigenvalues.cpu().numpy() - g["eigenvalues"]).max() < EIG_TOL_HA
+    x = res.eigenvectors
+    gram = x @ x.conj().transpose(-1, -2)
+    eye = torch.eye(gram.shape[-1], dtype=gram.dtype, device=gram.device)
+    assert float((gram - eye).abs().max()) < 1e-12
+    assert res.n_iter <= runs["0"].n_iter + 5
 
 
 def test_registry_adapters_and_two_stage(cuda_device):
