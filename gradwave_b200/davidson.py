@@ -33,12 +33,13 @@ Modes:
                       residual is within 100x of the float32 floor (early
                       rounds stagnate without any precision limit).
 In both float32-expansion modes the first of the two projection passes of
-the expansion block, D -= (D V^H) V, runs as split-precision BF16 products on
-the tensor cores (``gradwave_b200.tc``, error ~1e-5 relative) against a BF16
-plane copy of the basis kept current row block by row block; the float64
-second pass then removes that error, so the block is orthogonal to the basis
-to float64 round-off as before (``GWB_TC_PROJECT=0`` keeps both passes in
-float64).
+the expansion block, D -= (D V^H) V, and the first Cholesky-QR round run as
+split-precision BF16 products on the tensor cores (``gradwave_b200.tc``,
+error ~1e-6 relative) against a BF16 plane copy of the basis kept current
+row block by row block; the float64 projection pass and the float64
+Cholesky-QR round that follow remove that error, so the block is orthonormal
+and orthogonal to the basis to float64 round-off as before
+(``GWB_TC_PROJECT=0`` keeps every step in float64).
 ``precond`` is ``"teter"`` or an object with ``apply_into(...)`` (the learned
 preconditioner, ``gradwave_b200.learned``), which falls back to TPA per band.
 """
@@ -89,16 +90,23 @@ def _nh_work(dev) -> torch.Tensor:
     return w
 
 
+# A B^H products with at most this many outputs per batch entry go to the
+# split-K kernel (which fills the GPU where cuBLAS's output tiles cannot);
+# larger outputs to cuBLAS ZGEMM
+_NH_MAX_OUT = 160 * 160
+
+
 def zgemm(opA, opB, M, N, K, A, lda, sA, B, ldb, sB, C, ldc, sC, batch, alpha=1.0, beta=0.0,
-          a_off=0, b_off=0, c_off=0, stream=None):
+          a_off=0, b_off=0, c_off=0, stream=None, work=None):
     """Row-major batched complex128 GEMM (offsets in elements): A B^H products
-    with a small output go to the split-K kernel gwb_zgemm_nh, the rest to
-    cuBLAS through gwb_zgemm."""
+    with a small output go to the split-K kernel gwb_zgemm_nh (partial sums in
+    ``work``, default a per-device buffer), the rest to cuBLAS through
+    gwb_zgemm."""
     s = _lib.stream_ptr(C.device) if stream is None else stream
     a = complex(alpha)
     b = complex(beta)
-    if opA == _N and opB == _H and M * N * batch * 16 <= (24 << 20):
-        w = _nh_work(C.device)
+    w = _nh_work(C.device) if work is None else work
+    if opA == _N and opB == _H and M * N <= _NH_MAX_OUT and M * N * batch * 16 <= w.numel():
         _lib.call("gwb_zgemm_nh", M, N, K, a.real, a.imag, _ptr(A, a_off), lda, sA, _ptr(B, b_off), ldb, sB,
                   b.real, b.imag, _ptr(C, c_off), ldc, sC, batch, w.data_ptr(), w.numel(), s)
         return
@@ -205,6 +213,10 @@ class _Solver:
         self.breakdown = False
         self.mask_u8 = self.mask.to(torch.uint8).contiguous()
         self.stream = _lib.stream_ptr(self.dev)
+        # scratch owned by this solve, so that solves on other streams (k
+        # groups) never share it: split-K partial sums, tensor-core partials
+        self.nh_work = torch.empty(24 << 20, dtype=torch.uint8, device=self.dev)
+        self.tc_work = None
         self.x0 = x0
         self.prof = _PhaseTimer(os.environ.get("GWB_PROFILE", "0") == "1")
         # tensor-core first projection pass (float32-expansion modes): BF16
@@ -217,6 +229,11 @@ class _Solver:
                        PlaneSet(self.nk, self.nb, self.max_dim, self.dev))
 
     # -- primitives -----------------------------------------------------------
+    def zgemm(self, *args, **kw):
+        kw.setdefault("work", self.nh_work)
+        kw.setdefault("stream", self.stream)
+        zgemm(*args, **kw)
+
     def apply_block(self, src: torch.Tensor, src_off: int, src_ks: int, nrows: int, dst: torch.Tensor,
                     dst_off: int, dst_ks: int, low: bool):
         """H on nrows rows of src (k stride src_ks) into dst rows (k stride dst_ks)."""
@@ -240,25 +257,24 @@ class _Solver:
         dview.copy_(out)
 
     def cholqr2(self, Y: torch.Tensor, n: int, Ytmp: torch.Tensor, Z: torch.Tensor | None = None,
-                Ztmp: torch.Tensor | None = None, sync: bool = True):
-        """Orthonormalise the first n rows of Y (nk, >=n, npw) in place by two
-        rounds of float64 Gram -> Cholesky -> L^-1 (Z, if given, gets the same
-        row transform). With sync, a Cholesky breakdown is checked on the host
-        and reported as False (Y untouched by the failing round); without, it
-        only sets bit 1 of ws.flags, read with the next round's statistics."""
+                Ztmp: torch.Tensor | None = None, sync: bool = True, passes: int = 2):
+        """Orthonormalise the first n rows of Y (nk, >=n, npw) in place by
+        ``passes`` (default two) rounds of float64 Gram -> Cholesky -> L^-1 (Z,
+        if given, gets the same row transform). With sync, a Cholesky breakdown
+        is checked on the host and reported as False (Y untouched by the
+        failing round); without, it only sets bit 1 of ws.flags, read with the
+        next round's statistics."""
         ws, nk, npw = self.ws, self.nk, self.npw
         ys, zs = Y.shape[1] * npw, None if Z is None else Z.shape[1] * npw
-        for _ in range(2):
-            zgemm(_N, _H, n, n, npw, Y, npw, ys, Y, npw, ys, ws.G, n, n * n, nk, stream=self.stream)
-            _lib.call("gwb_chol_inv", nk, n, _ptr(ws.G), n, n * n, _ptr(ws.Linv), n * n, _ptr(ws.info),
-                      None if sync else _ptr(ws.flags), self.stream)
-            if sync and int(ws.info.max()) != 0:
+        for _ in range(passes):
+            self.zgemm(_N, _H, n, n, npw, Y, npw, ys, Y, npw, ys, ws.G, n, n * n, nk, stream=self.stream)
+            if not self.chol_inv(n, sync):
                 return False
-            zgemm(_N, _N, n, npw, n, ws.Linv, n, n * n, Y, npw, ys, Ytmp, npw, Ytmp.shape[1] * npw, nk,
+            self.zgemm(_N, _N, n, npw, n, ws.Linv, n, n * n, Y, npw, ys, Ytmp, npw, Ytmp.shape[1] * npw, nk,
                   stream=self.stream)
             Y[:, :n].copy_(Ytmp[:, :n])
             if Z is not None:
-                zgemm(_N, _N, n, npw, n, ws.Linv, n, n * n, Z, npw, zs, Ztmp, npw, Ztmp.shape[1] * npw, nk,
+                self.zgemm(_N, _N, n, npw, n, ws.Linv, n, n * n, Z, npw, zs, Ztmp, npw, Ztmp.shape[1] * npw, nk,
                       stream=self.stream)
                 Z[:, :n].copy_(Ztmp[:, :n])
         return True
@@ -273,24 +289,70 @@ class _Solver:
     def project_tc(self, n: int, m: int):
         """D -= (D V^H) V over the first m basis rows as split-BF16
         tensor-core products (error ~1e-5 relative; a float64 pass follows)."""
-        from .tc import OP_H, OP_N, zgemm_tc
+        from .tc import OP_H, OP_N, work_bytes, zgemm_tc
         pv, pd, pc = self.tc
         ws, npw = self.ws, self.npw
         ds = ws.D.shape[1] * npw
+        need = work_bytes(OP_H, n, m, npw, self.nk)
+        if self.tc_work is None or self.tc_work.numel() < need:
+            self.tc_work = torch.empty(max(need, 1 << 20), dtype=torch.uint8, device=self.dev)
         pd.write(ws.D, n, src_ld=npw, src_kstride=ds, stream=self.stream)
-        zgemm_tc(OP_H, n, m, npw, pd, pv, ws.C, m, n * m, stream=self.stream, status=ws.flags)
+        zgemm_tc(OP_H, n, m, npw, pd, pv, ws.C, m, n * m, stream=self.stream, status=ws.flags, work=self.tc_work)
         pc.write(ws.C, n, src_ld=m, src_kstride=n * m, cols=m, stream=self.stream)
         zgemm_tc(OP_N, n, npw, m, pc, pv, ws.D, npw, ds, alpha=-1.0, beta=1.0, stream=self.stream,
-                 status=ws.flags)
+                 status=ws.flags, work=self.tc_work)
+
+    def chol_inv(self, n: int, sync: bool) -> bool:
+        """ws.Linv[:n, :n] = L^-1 for the Cholesky factor L of ws.G (both as
+        (nk, n, n) with ld n). Up to 64 columns the libgwb.so kernel (the Gram
+        matrix in shared memory, one CTA per k); above that cuSOLVER's Cholesky
+        and triangular solve (the one-CTA kernel is latency-bound there: 49 ms
+        against 2 ms at n = 480). With sync a breakdown returns False; without,
+        it sets bit 1 of ws.flags."""
+        ws, nk = self.ws, self.nk
+        if n <= 64:
+            _lib.call("gwb_chol_inv", nk, n, _ptr(ws.G), n, n * n, _ptr(ws.Linv), n * n, _ptr(ws.info),
+                      None if sync else _ptr(ws.flags), self.stream)
+            return not sync or int(ws.info.max()) == 0
+        G = ws.G.view(-1)[: nk * n * n].view(nk, n, n)
+        L, info = torch.linalg.cholesky_ex(G)
+        Li = ws.Linv.view(-1)[: nk * n * n].view(nk, n, n)
+        eye = torch.eye(n, dtype=G.dtype, device=G.device).expand(nk, n, n)
+        Li.copy_(torch.linalg.solve_triangular(L, eye, upper=False))
+        if sync:
+            return int(info.max()) == 0
+        ws.flags.bitwise_or_((info.amax() != 0).to(torch.int32) * 2)
+        return True
+
+    def cholqr_tc(self, n: int) -> bool:
+        """One Cholesky-QR round of D[:, :n] as split-BF16 tensor-core products:
+        Gram D D^H (FP32-accumulated, summed in float64), float64 Cholesky and
+        triangular inverse, D <- L^-1 D. Leaves D nearly orthonormal (to about
+        1e-6 kappa(D)^2) for the float64 round that follows; False, with D
+        untouched, when the Cholesky breaks down (checked on the host)."""
+        from .tc import OP_H, OP_N, work_bytes, zgemm_tc
+        _, pd, pc = self.tc
+        ws, nk, npw = self.ws, self.nk, self.npw
+        ds = ws.D.shape[1] * npw
+        need = work_bytes(OP_H, n, n, npw, nk)
+        if self.tc_work is None or self.tc_work.numel() < need:
+            self.tc_work = torch.empty(max(need, 1 << 20), dtype=torch.uint8, device=self.dev)
+        pd.write(ws.D, n, src_ld=npw, src_kstride=ds, stream=self.stream)
+        zgemm_tc(OP_H, n, n, npw, pd, pd, ws.G, n, n * n, stream=self.stream, status=ws.flags, work=self.tc_work)
+        if not self.chol_inv(n, sync=True):
+            return False
+        pc.write(ws.Linv, n, src_ld=n, src_kstride=n * n, cols=n, stream=self.stream)
+        zgemm_tc(OP_N, n, npw, n, pc, pd, ws.D, npw, ds, stream=self.stream, status=ws.flags, work=self.tc_work)
+        return True
 
     def project_out(self, Dblk: torch.Tensor, n: int, m: int, passes: int = 2):
         """D -= (D V^H) V over the first m basis rows (float64 GEMMs)."""
         ws, nk, npw, md = self.ws, self.nk, self.npw, self.max_dim
         ds = Dblk.shape[1] * npw
         for _ in range(passes):
-            zgemm(_N, _H, n, m, npw, Dblk, npw, ds, ws.V, npw, md * npw, ws.C, m, n * m, nk,
+            self.zgemm(_N, _H, n, m, npw, Dblk, npw, ds, ws.V, npw, md * npw, ws.C, m, n * m, nk,
                   stream=self.stream)
-            zgemm(_N, _N, n, npw, m, ws.C, m, n * m, ws.V, npw, md * npw, Dblk, npw, ds, nk, alpha=-1.0,
+            self.zgemm(_N, _N, n, npw, m, ws.C, m, n * m, ws.V, npw, md * npw, Dblk, npw, ds, nk, alpha=-1.0,
                   beta=1.0, stream=self.stream)
 
     def orthonormalize_new(self, n: int, m: int, safe: bool = False):
@@ -313,9 +375,13 @@ class _Solver:
                     self.project_out(D, n, m, passes=1)
             _lib.call("gwb_row_repair", self.nk, n, self.npw, _ptr(D), D.shape[1] * self.npw,
                       _ptr(self.mask_u8), 1e-8, _ptr(ws.flags), self.stream)
+            # tensor-core Cholesky-QR round before the float64 projection, so
+            # that the float64 pass still sets the orthogonality to the basis;
+            # one float64 Cholesky-QR round then finishes the block
+            tc_round = self.tc is not None and self.cholqr_tc(n)
             if m:
                 self.project_out(D, n, m, passes=1)
-            self.cholqr2(D, n, ws.D2, sync=False)
+            self.cholqr2(D, n, ws.D2, sync=False, passes=1 if tc_round else 2)
             return
         if m:
             self.project_out(D, n, m)
@@ -340,15 +406,15 @@ class _Solver:
         nnew = m - m0
         if nnew > 0:
             with self.prof("subspace_gemm"):
-                zgemm(_N, _H, m, nnew, npw, ws.V, npw, md * npw, ws.HV, npw, md * npw, ws.C, nnew, m * nnew, nk,
+                self.zgemm(_N, _H, m, nnew, npw, ws.V, npw, md * npw, ws.HV, npw, md * npw, ws.C, nnew, m * nnew, nk,
                       b_off=m0 * npw, stream=self.stream)
                 _lib.call("gwb_subspace_insert", nk, m, m0, _ptr(ws.C), _ptr(ws.S), md, md * md, self.stream)
         with self.prof("eigh"):
             eig, u, ldu = self.eigh(m)
         with self.prof("ritz_gemm"):
-            zgemm(_T, _N, nb, npw, m, u, ldu, m * ldu, ws.V, npw, md * npw, ws.X, npw, nb * npw, nk,
+            self.zgemm(_T, _N, nb, npw, m, u, ldu, m * ldu, ws.V, npw, md * npw, ws.X, npw, nb * npw, nk,
                   stream=self.stream)
-            zgemm(_T, _N, nb, npw, m, u, ldu, m * ldu, ws.HV, npw, md * npw, ws.HX, npw, nb * npw, nk,
+            self.zgemm(_T, _N, nb, npw, m, u, ldu, m * ldu, ws.HV, npw, md * npw, ws.HX, npw, nb * npw, nk,
                   stream=self.stream)
         with self.prof("residual"):
             self.residuals(eig)
@@ -383,16 +449,16 @@ class _Solver:
         ws, nk, nb, npw = self.ws, self.nk, self.nb, self.npw
         self.n_cert += 1
         self.apply_block(ws.X, 0, nb * npw, nb, ws.HX, 0, nb * npw, low=False)
-        zgemm(_N, _H, nb, nb, npw, ws.X, npw, nb * npw, ws.HX, npw, nb * npw, ws.G, nb, nb * nb, nk,
+        self.zgemm(_N, _H, nb, nb, npw, ws.X, npw, nb * npw, ws.HX, npw, nb * npw, ws.G, nb, nb * nb, nk,
               stream=self.stream)
         s = ws.G.conj()
         ws.Gs.copy_(0.5 * (s + s.conj().transpose(-1, -2)))
         eig, u, ldu = self.eigh(nb, ws.Gs, nb)
         eig = eig.clone()
-        zgemm(_T, _N, nb, npw, nb, u, ldu, nb * ldu, ws.X, npw, nb * npw, ws.D2, npw, nb * npw, nk,
+        self.zgemm(_T, _N, nb, npw, nb, u, ldu, nb * ldu, ws.X, npw, nb * npw, ws.D2, npw, nb * npw, nk,
               stream=self.stream)
         ws.X.copy_(ws.D2)
-        zgemm(_T, _N, nb, npw, nb, u, ldu, nb * ldu, ws.HX, npw, nb * npw, ws.D2, npw, nb * npw, nk,
+        self.zgemm(_T, _N, nb, npw, nb, u, ldu, nb * ldu, ws.HX, npw, nb * npw, ws.D2, npw, nb * npw, nk,
               stream=self.stream)
         ws.HX.copy_(ws.D2)
         self.residuals(eig)
@@ -567,22 +633,29 @@ def _tc_projection() -> bool:
     return v == "1"
 
 
-def _k_groups() -> int:
-    """Number of concurrent k-groups of a native solve (``GWB_KGROUPS``)."""
+def _k_groups(default: int) -> int:
+    """Number of concurrent k-groups of a solve (``GWB_KGROUPS``, else
+    ``default``)."""
+    v = os.environ.get("GWB_KGROUPS")
+    if v is None:
+        return default
     try:
-        return max(1, int(os.environ.get("GWB_KGROUPS", "1")))
+        return max(1, int(v))
     except ValueError:
         raise ValueError("GWB_KGROUPS must be a positive integer") from None
 
 
-def _native_solve_grouped(ham, x0, t, mask, tol, max_iter, max_dim_factor, mode, time_applies, model, groups):
+def _solve_grouped(ham, x0, t, mask, tol, max_iter, max_dim_factor, mode, groups, *, native, time_applies=False,
+                   model=None, precond="teter"):
     """The k-points split into contiguous groups balanced by plane-wave count,
-    each solved by the native driver from its own host thread on its own CUDA
-    stream. Every k is an independent eigenproblem, so the groups need no
-    communication; running them side by side lets one group's latency-bound
-    steps (the per-k subspace eigensolver, one CTA per k) overlap another
-    group's bandwidth-bound applies and products on the same GPU. None when a
-    group reports an unrepaired breakdown (the caller retries on the host)."""
+    each solved from its own host thread on its own CUDA stream, by the native
+    driver (``native``) or by the host driver. Every k is an independent
+    eigenproblem, so the groups need no communication; running them side by
+    side lets one group's latency-bound steps (the per-k subspace eigensolver)
+    overlap another group's bandwidth-bound applies and products on the same
+    GPU. Each group keeps the reference's uniform-subspace rule inside itself.
+    None when a native group reports an unrepaired breakdown (the caller
+    retries on the host)."""
     import threading
     from .sharding import shard_range_weighted
     nk, nb = int(x0.shape[0]), int(x0.shape[1])
@@ -602,13 +675,24 @@ def _native_solve_grouped(ham, x0, t, mask, tol, max_iter, max_dim_factor, mode,
     def work(g):
         try:
             s, e = ranges[g]
-            md = min(max_dim_factor * nb, int(mask[s:e].sum(dim=1).min()))
-            with torch.cuda.device(dev), torch.cuda.stream(streams[g]):
-                results[g] = _native_solve(subs[g], x0[s:e], t[s:e], mask[s:e], tol, max_iter, md, mode,
-                                           time_applies=time_applies, model=model)
+            with torch.cuda.device(dev), torch.cuda.stream(streams[g]), torch.no_grad():
+                if native:
+                    md = min(max_dim_factor * nb, int(mask[s:e].sum(dim=1).min()))
+                    results[g] = _native_solve(subs[g], x0[s:e], t[s:e], mask[s:e], tol, max_iter, md, mode,
+                                               time_applies=time_applies, model=model)
+                else:
+                    results[g] = _Solver(subs[g].apply, x0[s:e], t[s:e], mask[s:e], tol, max_iter, max_dim_factor,
+                                         mode, precond, None).run()
         except BaseException as exc:  # re-raised on the caller's thread
             errors[g] = exc
 
+    if not native:
+        # torch loads its CUDA linear-algebra backend lazily on the first call,
+        # which must not happen from several threads at once
+        a = torch.eye(2, dtype=torch.complex128, device=dev)
+        torch.linalg.eigh(a)
+        torch.linalg.qr(a)
+        torch.linalg.solve_triangular(torch.linalg.cholesky_ex(a)[0], a, upper=False)
     for g in range(g_n):
         streams[g].wait_stream(main)
     threads = [threading.Thread(target=work, args=(g,)) for g in range(g_n)]
@@ -626,10 +710,12 @@ def _native_solve_grouped(ham, x0, t, mask, tol, max_iter, max_dim_factor, mode,
     for r in results:  # the group outputs are read on the caller's stream from here on
         for x in (r.eigenvalues, r.eigenvectors, r.residual_norms):
             x.record_stream(main)
-    info = {"native": True, "k_groups": g_n, "max_dim": max(r.info["max_dim"] for r in results)}
-    for key in ("n_restart", "n_cert", "n_repair", "n_rollback", "n_apply_calls", "apply_ms"):
+    info = {"native": native, "k_groups": g_n, "max_dim": max(r.info["max_dim"] for r in results)}
+    for key in ("n_restart", "n_cert", "n_repair", "n_rollback", "n_apply_calls", "apply_ms", "n_fallback_qr"):
         if key in results[0].info:
             info[key] = sum(r.info[key] for r in results)
+    if "tc_projection" in results[0].info:
+        info["tc_projection"] = results[0].info["tc_projection"]
     return BatchedDavidsonResult(torch.cat([r.eigenvalues for r in results]),
                                  torch.cat([r.eigenvectors for r in results]),
                                  max(r.n_iter for r in results),
@@ -660,16 +746,28 @@ def davidson_batched(h_apply, x0, t, mask, tol: float = 1e-9, max_iter: int = 40
                   and (precond is None or (isinstance(precond, str) and precond == "teter")
                        or hasattr(precond, "params"))
                   and history_out is None and int(x0.shape[1]) <= max_dim <= int(_lib.load().gwb_heev_max_dim()))
+        nk = int(x0.shape[0])
         if native:
             time_applies = os.environ.get("GWB_TIME_APPLIES", "0") == "1"
             model = getattr(precond, "params", None)
-            groups = _k_groups()
-            if groups > 1 and int(x0.shape[0]) > 1 and hasattr(ham, "k_slice"):
-                res = _native_solve_grouped(ham, x0, t, mask, tol, max_iter, max_dim_factor, mode, time_applies,
-                                            model, groups)
+            groups = _k_groups(1)
+            if groups > 1 and nk > 1 and hasattr(ham, "k_slice"):
+                res = _solve_grouped(ham, x0, t, mask, tol, max_iter, max_dim_factor, mode, groups, native=True,
+                                     time_applies=time_applies, model=model)
             else:
                 res = _native_solve(ham, x0, t, mask, tol, max_iter, max_dim, mode, time_applies=time_applies,
                                     model=model)
+            if res is not None:
+                return res
+        # host driver: a basis beyond the batched eigensolver goes to cuSOLVER,
+        # one matrix at a time, so by default every k (up to 8) gets its own
+        # group and the eigensolves of different k overlap
+        own_apply = ham is not None and getattr(h_apply, "__func__", None) is getattr(type(ham), "apply", None)
+        groups = _k_groups(min(nk, 8) if max_dim > int(_lib.load().gwb_heev_max_dim()) else 1)
+        if (groups > 1 and nk > 1 and own_apply and hasattr(ham, "k_slice") and history_out is None
+                and x0.is_cuda and x0.dtype == torch.complex128):
+            res = _solve_grouped(ham, x0, t, mask, tol, max_iter, max_dim_factor, mode, groups, native=False,
+                                 precond=precond)
             if res is not None:
                 return res
         return _Solver(h_apply, x0, t, mask, tol, max_iter, max_dim_factor, mode, precond, history_out).run()

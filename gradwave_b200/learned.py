@@ -150,23 +150,19 @@ class LearnedPreconditioner:
         solver.n_tpa_fallback = int(0)  # read lazily by callers that want it
         eigc = eig.contiguous()
         solver._lp_eig = eigc
-        work = _precond_work(solver.dev, nk, nb, npw)
+        work = getattr(solver, "_lp_work", None)
+        if work is None:  # per solve: concurrent solves on other streams never share it
+            work = _precond_work(solver.dev, nk, nb, npw)
+            solver._lp_work = work
         _lib.call("gwb_precond_learned", self.params.data_ptr(), nk, nb, n_add, npw, ws.X.data_ptr(), nb * npw,
                   ws.R.data_ptr(), nb * npw, solver.t.data_ptr(), eigc.data_ptr(), ws.sel.data_ptr(),
                   tpa_only.data_ptr(), ws.D.data_ptr(), nb * npw, work.data_ptr(), work.numel(), solver.stream)
 
 
-_WORK: dict = {}
-
-
 def _precond_work(dev, nk: int, n_rows: int, npw: int) -> torch.Tensor:
-    """Scratch of gwb_precond_learned for up to n_rows selected rows per k (cached)."""
+    """Scratch of gwb_precond_learned for up to n_rows selected rows per k."""
     need = int(_lib.load().gwb_precond_learned_work_bytes(nk, n_rows, npw))
-    key = (str(dev), need)
-    if key not in _WORK:
-        _WORK.clear()
-        _WORK[key] = torch.empty(max(need, 8), dtype=torch.uint8, device=dev)
-    return _WORK[key]
+    return torch.empty(max(need, 8), dtype=torch.uint8, device=dev)
 
 
 # ---------------------------------------------------------------------------

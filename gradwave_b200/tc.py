@@ -79,21 +79,28 @@ def _work(device, nbytes: int) -> torch.Tensor:
     return w
 
 
+def work_bytes(op_b: int, M: int, N: int, K: int, batch: int) -> int:
+    """Bytes of partial-sum scratch ``zgemm_tc`` uses for these sizes."""
+    return int(_lib.load().gwb_zgemm_tc_work_bytes(op_b, M, N, K, batch))
+
+
 def zgemm_tc(op_b: int, M: int, N: int, K: int, A: PlaneSet, B: PlaneSet, C: torch.Tensor, ldc: int, strideC: int,
              alpha: complex = 1.0, beta: complex = 0.0, c_offset: int = 0, stream: int | None = None,
-             status: torch.Tensor | None = None) -> None:
+             status: torch.Tensor | None = None, work: torch.Tensor | None = None) -> None:
     """C = alpha A op(B) + beta C (per batch entry; complex128 C with row
     stride ``ldc`` and batch stride ``strideC``, from element ``c_offset``).
     op_b = OP_H: B holds N rows of length K; OP_N: B holds K rows of length N.
     A timed-out pipeline wait ORs GWB_ERR_TIMEOUT into ``status`` (an int32
-    device tensor; default: the per-device flag read by ``check_status``)."""
+    device tensor; default: the per-device flag read by ``check_status``).
+    ``work``: partial-sum scratch (default: a per-device buffer; callers that
+    run products concurrently on several streams pass their own)."""
     if C.dtype != torch.complex128:
         raise TypeError("zgemm_tc writes complex128")
     if A.nk != B.nk:
         raise ValueError("plane sets of different batch sizes")
     dev = C.device
-    nbytes = int(_lib.load().gwb_zgemm_tc_work_bytes(op_b, M, N, K, A.nk))
-    work = _work(dev, nbytes)
+    if work is None:
+        work = _work(dev, work_bytes(op_b, M, N, K, A.nk))
     alpha, beta = complex(alpha), complex(beta)
     _lib.call("gwb_zgemm_tc", op_b, int(M), int(N), int(K), alpha.real, alpha.imag, A.t.data_ptr(), A.ld,
               A.rows_cap, B.t.data_ptr(), B.ld, B.rows_cap, beta.real, beta.imag, C.data_ptr() + 16 * c_offset,
