@@ -398,6 +398,56 @@ __global__ void k_tc_planes(int nk, int rows, int cols, const S* __restrict__ sr
   }
 }
 
+// planes of bd = becp D for the nonlocal term: rows (k, b) of becp
+// (complex128, nproj per row) times the real nproj x nproj D, split into the
+// four BF16 planes of a (nk, 4, nb, ldq) set, columns nproj..ldq-1 zero; TB_R
+// rows per CTA share each read of D.
+constexpr int TB_R = 4;
+__global__ void __launch_bounds__(256) k_becp_d_planes(int nk, int nb, int nproj, const cplx<double>* __restrict__ becp,
+                                                       const double* __restrict__ D, __nv_bfloat16* __restrict__ planes,
+                                                       int64_t ldq) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<double>* rows = reinterpret_cast<cplx<double>*>(smem_raw);  // TB_R x nproj
+  const int64_t r0 = (int64_t)blockIdx.x * TB_R;
+  const int64_t nrows = (int64_t)nk * nb;
+  for (int i = threadIdx.x; i < TB_R * nproj; i += blockDim.x) {
+    const int64_t r = r0 + i / nproj;
+    rows[i] = r < nrows ? becp[r * nproj + i % nproj] : mk<double>(0.0, 0.0);
+  }
+  __syncthreads();
+  const int64_t plane = (int64_t)nb * ldq;
+  for (int q = threadIdx.x; q < ldq; q += blockDim.x) {
+    double ar[TB_R], ai[TB_R];
+#pragma unroll
+    for (int r = 0; r < TB_R; ++r) ar[r] = ai[r] = 0.0;
+    if (q < nproj) {
+      for (int p = 0; p < nproj; ++p) {
+        const double d = D[(int64_t)p * nproj + q];
+#pragma unroll
+        for (int r = 0; r < TB_R; ++r) {
+          const cplx<double> v = rows[r * nproj + p];
+          ar[r] += v.x * d;
+          ai[r] += v.y * d;
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < TB_R; ++r) {
+      const int64_t row = r0 + r;
+      if (row >= nrows) break;
+      const int64_t k = row / nb, b = row % nb;
+      __nv_bfloat16 h, l;
+      __nv_bfloat16* base = planes + 4 * k * plane + b * ldq + q;
+      split_bf16(ar[r], h, l);
+      base[0] = h;
+      base[plane] = l;
+      split_bf16(ai[r], h, l);
+      base[2 * plane] = h;
+      base[3 * plane] = l;
+    }
+  }
+}
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -460,6 +510,21 @@ int64_t pick_splits(int64_t tiles, int64_t nkt) {
 }
 
 }  // namespace
+
+// bd = becp D written as BF16 planes (the A operand of the nonlocal update
+// out += bd P); used by the Hamiltonian apply.
+int tc_becp_d_planes(int nk, int nb, int nproj, const cplx<double>* becp, const double* D, void* planes, int64_t ldq,
+                     cudaStream_t st) {
+  const int64_t rows = (int64_t)nk * nb;
+  const unsigned blocks = (unsigned)((rows + TB_R - 1) / TB_R);
+  const size_t sm = (size_t)TB_R * nproj * sizeof(cplx<double>);
+  GWB_CUDA_TRY(allow_smem(k_becp_d_planes));
+  k_becp_d_planes<<<blocks, 256, sm, st>>>(nk, nb, nproj, becp, D, (__nv_bfloat16*)planes, ldq);
+  GWB_LAUNCH_CHECK();
+  count_launches(1);
+  return GWB_OK;
+}
+
 }  // namespace gwb
 
 using namespace gwb;

@@ -81,6 +81,19 @@ struct gwb_ham {
   size_t part_bytes = 0;
   void* d_bd = nullptr;  // becp * D
   size_t bd_bytes = 0;
+  // tensor-core nonlocal term (float32 applies of complex128 blocks)
+  void* d_pplanes = nullptr;  // BF16 planes of P: (nk, 4, nproj, ldp)
+  size_t pplanes_bytes = 0;
+  bool pplanes_ok = false;
+  void* d_cplanes = nullptr;  // BF16 planes of the input rows: (nk, 4, nb, ldp)
+  size_t cplanes_bytes = 0;
+  void* d_becp = nullptr;  // becp (nk, nb, nproj) complex128
+  size_t becp_bytes = 0;
+  void* d_bdplanes = nullptr;  // BF16 planes of becp D: (nk, 4, nb, ldq)
+  size_t bdplanes_bytes = 0;
+  void* d_tcwork = nullptr;  // split-K partial sums
+  size_t tcwork_bytes = 0;
+  int* d_tcstatus = nullptr;  // pipeline-wait timeouts of the tensor-core products
   bool have_t = false, have_v = false, have_p = false;
 };
 
@@ -621,6 +634,56 @@ static int local_chunks(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t 
   return GWB_OK;
 }
 
+int tc_becp_d_planes(int nk, int nb, int nproj, const cplx<double>* becp, const double* D, void* planes, int64_t ldq,
+                     cudaStream_t st);
+
+// Projector counts from which the float32 apply of complex128 blocks runs its
+// nonlocal term on the tensor cores (GWB_TC_NONLOCAL=0 keeps the CUDA-core
+// kernels everywhere).
+constexpr int TC_NONLOCAL_MIN_NPROJ = 128;
+
+static bool tc_nonlocal_enabled(const gwb_ham* h) {
+  static const bool env_on = [] {
+    const char* v = std::getenv("GWB_TC_NONLOCAL");
+    return !(v && v[0] == '0');
+  }();
+  return env_on && h->nproj >= TC_NONLOCAL_MIN_NPROJ;
+}
+
+// out += P^T D (P^* . c) with split-BF16 tensor-core products:
+// becp = c P^H (A B^H, FP32 accumulation, float64 slice sums), bd = becp D in
+// float64 written as BF16 planes, out += bd P (A B, P read MN-major). The
+// BF16 planes of P are built once per set of projectors.
+static int nonlocal_tc(gwb_ham* h, const cplx<double>* c, int64_t ck, cplx<double>* out, int64_t ok, int nb,
+                       cudaStream_t st) {
+  const int nk = h->nk, np = h->nproj, npw = h->npw_max;
+  const int64_t ldp = ((int64_t)npw + 7) / 8 * 8, ldq = ((int64_t)np + 7) / 8 * 8;
+  int rc;
+  if (!h->d_tcstatus) {
+    GWB_CUDA_TRY(cudaMalloc((void**)&h->d_tcstatus, sizeof(int)));
+    GWB_CUDA_TRY(cudaMemsetAsync(h->d_tcstatus, 0, sizeof(int), st));
+  }
+  if (!h->pplanes_ok) {
+    if ((rc = ensure_buf(&h->d_pplanes, &h->pplanes_bytes, (size_t)nk * 4 * np * ldp * 2))) return rc;
+    if ((rc = gwb_tc_planes(nk, np, npw, h->d_p64, npw, (int64_t)np * npw, GWB_C128, 0, h->d_pplanes, ldp, np, 0,
+                            st)))
+      return rc;
+    h->pplanes_ok = true;
+  }
+  if ((rc = ensure_buf(&h->d_cplanes, &h->cplanes_bytes, (size_t)nk * 4 * nb * ldp * 2))) return rc;
+  if ((rc = ensure_buf(&h->d_becp, &h->becp_bytes, (size_t)nk * nb * np * 16))) return rc;
+  if ((rc = ensure_buf(&h->d_bdplanes, &h->bdplanes_bytes, (size_t)nk * 4 * nb * ldq * 2))) return rc;
+  const int64_t wb = gwb_zgemm_tc_work_bytes(2, nb, np, npw, nk);
+  if (wb > 0 && (rc = ensure_buf(&h->d_tcwork, &h->tcwork_bytes, (size_t)wb))) return rc;
+  if ((rc = gwb_tc_planes(nk, nb, npw, c, npw, ck, GWB_C128, 0, h->d_cplanes, ldp, nb, 0, st))) return rc;
+  if ((rc = gwb_zgemm_tc(2, nb, np, npw, 1.0, 0.0, h->d_cplanes, ldp, nb, h->d_pplanes, ldp, np, 0.0, 0.0, h->d_becp,
+                         np, (int64_t)nb * np, nk, h->d_tcwork, h->tcwork_bytes, h->d_tcstatus, st)))
+    return rc;
+  if ((rc = tc_becp_d_planes(nk, nb, np, (const cplx<double>*)h->d_becp, h->d_d64, h->d_bdplanes, ldq, st))) return rc;
+  return gwb_zgemm_tc(0, nb, npw, np, 1.0, 0.0, h->d_bdplanes, ldq, nb, h->d_pplanes, ldp, np, 1.0, 0.0, out, npw, ok,
+                      nk, nullptr, 0, h->d_tcstatus, st);
+}
+
 template <typename T, typename SIO>
 static int apply_impl(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t ok, int nb, cudaStream_t st) {
   const FftGeom& g = h->g;
@@ -646,6 +709,9 @@ static int apply_impl(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t ok
   else if (cubic && c0 == kCode96) rcl = local_chunks<T, SIO, kCode96>(h, c, ck, out, ok, nb, nbc, st, smA, smB);
   else rcl = local_chunks<T, SIO, 0u>(h, c, ck, out, ok, nb, nbc, st, smA, smB);
   if (rcl) return rcl;
+  if constexpr (std::is_same<T, float>::value && std::is_same<SIO, cplx<double>>::value) {
+    if (h->nproj > 0 && tc_nonlocal_enabled(h)) return nonlocal_tc(h, c, ck, out, ok, nb, st);
+  }
   if (h->nproj > 0) {
     const int ns = nl_slices(h, nb);
     const int gslice = ((h->npw_max + ns - 1) / ns + NL_TG - 1) / NL_TG * NL_TG;
@@ -806,6 +872,7 @@ int gwb_ham_destroy(gwb_ham* h) {
   if (!h) return GWB_OK;
   void* ptrs[] = {h->d_npw, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos, h->d_t64, h->d_t32, h->d_v64,
                   h->d_v32, h->d_p64, h->d_p32, h->d_d64, h->d_d32, h->d_W, h->d_part, h->d_bd,
+                  h->d_pplanes, h->d_cplanes, h->d_becp, h->d_bdplanes, h->d_tcwork, h->d_tcstatus,
                   h->d_tw64[0], h->d_tw64[1], h->d_tw64[2], h->d_tw32[0], h->d_tw32[1], h->d_tw32[2]};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -851,6 +918,7 @@ int gwb_ham_set_projectors(gwb_ham* h, const void* p, const double* dij, void* s
   GWB_CUDA_TRY(cudaMemcpyAsync(h->d_p64, p, np * 16, cudaMemcpyDeviceToDevice, st));
   k_c128_to_c64<<<blocks_for(np, 256), 256, 0, st>>>((const cplx<double>*)p, h->d_p32, np);
   GWB_CUDA_TRY(cudaMemcpyAsync(h->d_d64, dij, nd * 8, cudaMemcpyDeviceToDevice, st));
+  h->pplanes_ok = false;  // the tensor-core planes of P are rebuilt on next use
   k_scale_copy<float><<<blocks_for(nd, 256), 256, 0, st>>>(dij, h->d_d32, nd, 1.0);
   GWB_LAUNCH_CHECK();
   h->have_p = true;
@@ -894,7 +962,23 @@ int gwb_ham_apply(gwb_ham* h, const void* c, void* out, int32_t nb, int32_t io_d
 }
 
 size_t gwb_ham_scratch_bytes(const gwb_ham* h) {
-  return h ? h->W_bytes + h->part_bytes + h->bd_bytes : 0;
+  return h ? h->W_bytes + h->part_bytes + h->bd_bytes + h->pplanes_bytes + h->cplanes_bytes + h->becp_bytes +
+                 h->bdplanes_bytes + h->tcwork_bytes
+           : 0;
+}
+
+int gwb_ham_tc_status(gwb_ham* h, int* status) {
+  GWB_REQUIRE(h && status, "null argument");
+  *status = 0;
+  if (!h->d_tcstatus) return GWB_OK;
+  GWB_CUDA_TRY(cudaSetDevice(h->device));
+  GWB_CUDA_TRY(cudaMemcpy(status, h->d_tcstatus, sizeof(int), cudaMemcpyDeviceToHost));
+  if (*status) {
+    GWB_CUDA_TRY(cudaMemset(h->d_tcstatus, 0, sizeof(int)));
+    set_error("tensor-core nonlocal term: a bounded pipeline wait ran out");
+    return GWB_ERR_TIMEOUT;
+  }
+  return GWB_OK;
 }
 
 }  // extern "C"

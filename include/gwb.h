@@ -110,6 +110,14 @@ int gwb_ham_apply_strided(gwb_ham* h, const void* c, int64_t c_kstride, void* ou
 /* Bytes of handle-owned device scratch currently held. */
 size_t gwb_ham_scratch_bytes(const gwb_ham* h);
 
+/* Float32 applies of complex128 blocks with nproj >= 128 run the nonlocal
+ * term as split-BF16 tensor-core products (gwb_zgemm_tc; error ~1e-6 of the
+ * term, below the float32 arithmetic of the rest; GWB_TC_NONLOCAL=0 in the
+ * environment keeps the CUDA-core kernels). This reads (synchronously) and
+ * clears the handle's record of a timed-out pipeline wait in them: *status
+ * = 0 and GWB_OK if none, else GWB_ERR_TIMEOUT. */
+int gwb_ham_tc_status(gwb_ham* h, int* status);
+
 /* ======================================================================= */
 /* Davidson steps (complex128 blocks, float64 reductions)                  */
 /* A "k stride" is the distance in complex elements between the blocks of   */

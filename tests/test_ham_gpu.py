@@ -90,3 +90,31 @@ def test_apply_band_chunking_invariant(cuda_device, monkeypatch):
     ci2, h2 = _ham("si8_cubic")
     chunked = h2.apply(c)
     assert torch.equal(full, chunked)
+
+
+def test_apply_si64_checksums_and_tensor_core_nonlocal(cuda_device):
+    """The 64-atom cell (72^3 box, 256 projectors): float64 checksums against
+    the reference, and the float32 apply, whose nonlocal term runs as
+    split-BF16 tensor-core products from 128 projectors up, within the float32
+    bar of the float64 result; no pipeline wait ran out."""
+    import ctypes
+    from gradwave_b200 import _lib
+    g = load_golden("si64_cubic")
+    ci, h = _ham("si64_cubic")
+    assert np.array_equal(ci.bk.npw.numpy(), g["npw"])
+    c = random_block(11, ci.bk.nk, 2, ci.bk.npw_max)
+    out = h.apply(torch.from_numpy(c).to(cuda_device)).cpu().numpy()
+    ref = g["apply_chk"]
+    assert np.abs(checksums(out, 11) - ref).max() / np.abs(ref).max() < TOL64
+    rng = np.random.default_rng(3)
+    nb = 6
+    cm = (rng.standard_normal((ci.bk.nk, nb, ci.bk.npw_max))
+          + 1j * rng.standard_normal((ci.bk.nk, nb, ci.bk.npw_max))) * ci.bk.mask.numpy()[:, None, :]
+    x = torch.from_numpy(cm).to(cuda_device)
+    o64 = h.apply(x).cpu().numpy()
+    o32 = h.apply_fp32(x).cpu().numpy()
+    assert _rel(o32, o64) < TOL32
+    assert np.all(o32[~ci.bk.mask.numpy()[:, None, :].repeat(nb, 1)] == 0)
+    st = ctypes.c_int(-1)
+    _lib.call("gwb_ham_tc_status", h._h, ctypes.byref(st))
+    assert st.value == 0
