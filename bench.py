@@ -399,7 +399,10 @@ def run_apply(args):
 
 
 def run_once(args):
-    """One warm-up and one timed solve of the workload (for ncu launch lists)."""
+    """``--warmup`` untimed and one wall-timed solve of the workload (for ncu
+    launch lists and the larger cells): rounds, applies, eigenvalue and band
+    energy error against the reference's golden eigenvalues, and with
+    GWB_PROFILE=1 the per-phase CUDA-event times of the host driver."""
     import torch
     from gradwave_b200.cells import make_cell
     from gradwave_b200.davidson import davidson_batched
@@ -416,8 +419,69 @@ def run_once(args):
     t0 = time.perf_counter()
     r = davidson_batched(h.apply, x0, bk.t, bk.mask, tol=args.tol, max_iter=300, mode=mode, precond=pc)
     torch.cuda.synchronize()
-    print(json.dumps({"mode": "once", "config": args.config, "solver": args.solver, "n_iter": r.n_iter,
-                      "wall_ms": (time.perf_counter() - t0) * 1e3}), flush=True)
+    wall = (time.perf_counter() - t0) * 1e3
+    out = {"mode": "once", "config": args.config, "solver": args.solver, "n_iter": r.n_iter, "wall_ms": wall,
+           "n_apply_low": r.n_apply_low, "n_apply_full": r.n_apply_full,
+           "max_residual_ev": float(r.residual_norms.max())}
+    for key in ("native", "k_groups", "tc_projection", "phase_ms"):
+        if key in r.info:
+            out[key] = r.info[key]
+    gold = _golden(args.config)
+    if gold is not None:
+        eig = r.eigenvalues.cpu().numpy()
+        err = float(np.abs(eig - gold["eigenvalues"]).max())
+        nocc = ci.nocc()
+        w = np.asarray(ci.kweights)
+        be = 2.0 * float(np.sum(w[:, None] * (eig[:, :nocc] - gold["eigenvalues"][:, :nocc])))
+        out.update({"eig_err_ha": err / HA, "band_energy_err_ha": abs(be) / HA, "within_1e-8_ha": err <= EIG_TOL_EV})
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_tc(args):
+    """The split-BF16 tensor-core products at one Davidson shape: nk batches of
+    D (n x npw) against a basis V (m x npw): C = D V^H (A B^H, split-K) and
+    D -= C V (A B), each ``--warmup`` untimed and ``--steps`` timed calls
+    (CUDA events), next to cuBLAS ZGEMM on the same operands, with the error
+    against the float64 product relative to sum_k |d||v|."""
+    import torch
+    from gradwave_b200.tc import OP_H, OP_N, PlaneSet, check_status, zgemm_tc
+    dev = torch.device("cuda", 0)
+    nk, n, m, npw = (int(v) for v in args.tc_shape.split(","))
+    g = torch.Generator(device="cpu").manual_seed(0)
+    D = torch.randn(nk, n, npw, dtype=torch.complex128, generator=g).to(dev)
+    V = torch.randn(nk, m, npw, dtype=torch.complex128, generator=g).to(dev)
+    pd, pv, pc = PlaneSet(nk, n, npw, dev), PlaneSet(nk, m, npw, dev), PlaneSet(nk, n, m, dev)
+    C = torch.zeros(nk, n, m, dtype=torch.complex128, device=dev)
+    D2 = D.clone()
+
+    def ev(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / max(args.steps, 1)
+
+    t_planes = ev(lambda: (pd.write(D, n), pv.write(V, m)))
+    t_nh = ev(lambda: zgemm_tc(OP_H, n, m, npw, pd, pv, C, m, n * m))
+    pc.write(C, n)
+    t_nn = ev(lambda: zgemm_tc(OP_N, n, npw, m, pc, pv, D2, npw, n * npw, alpha=-1.0, beta=1.0))
+    torch.cuda.synchronize()
+    check_status(dev)
+    ref = D @ V.conj().transpose(-1, -2)
+    err = float(((C - ref).abs() / (D.abs() @ V.abs().transpose(-1, -2))).max())
+    t_z_nh = ev(lambda: torch.matmul(D, V.conj().transpose(-1, -2), out=ref))
+    t_z_nn = ev(lambda: torch.baddbmm(D, C, V, beta=1.0, alpha=-1.0))
+    flop = 8.0 * nk * n * m * npw  # complex multiply-adds x 8
+    print(json.dumps({"mode": "tc", "shape": {"nk": nk, "n": n, "m": m, "npw": npw}, "planes_ms": t_planes,
+                      "a_bh_ms": t_nh, "a_b_ms": t_nn, "zgemm_a_bh_ms": t_z_nh, "zgemm_a_b_ms": t_z_nn,
+                      "a_bh_tflops_equiv": flop / t_nh / 1e9, "a_b_tflops_equiv": flop / t_nn / 1e9,
+                      "bf16_tflops_issued_a_bh": 3.0 * flop / t_nh / 1e9, "rel_err": err}), flush=True)
     return 0
 
 
@@ -448,7 +512,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--mode", default="solve", choices=["solve", "apply", "once"],
+    ap.add_argument("--tc-shape", default="4,160,640,37000", help="--mode tc: nk,n,m,npw")
+    ap.add_argument("--mode", default="solve", choices=["solve", "apply", "once", "tc"],
                     help="apply: only time Hamiltonian applies; once: a single solve (profiling)")
     ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64"], help="arithmetic of --mode apply")
     ap.add_argument("--solver", default="learned-mixed", choices=["plain", "fp32exp", "mixed", "learned-mixed"],
@@ -456,6 +521,8 @@ def main():
     args = ap.parse_args()
     if args.mode == "apply":
         return run_apply(args)
+    if args.mode == "tc":
+        return run_tc(args)
     if args.mode == "once":
         return run_once(args)
     if args.impl == "reference":

@@ -716,6 +716,13 @@ def _solve_grouped(ham, x0, t, mask, tol, max_iter, max_dim_factor, mode, groups
             info[key] = sum(r.info[key] for r in results)
     if "tc_projection" in results[0].info:
         info["tc_projection"] = results[0].info["tc_projection"]
+    if results[0].info.get("phase_ms"):
+        # per-phase event times summed over the groups (which overlap in time)
+        ph: dict = {}
+        for r in results:
+            for k, v in r.info.get("phase_ms", {}).items():
+                ph[k] = round(ph.get(k, 0.0) + v, 4)
+        info["phase_ms"] = dict(sorted(ph.items(), key=lambda kv: -kv[1]))
     return BatchedDavidsonResult(torch.cat([r.eigenvalues for r in results]),
                                  torch.cat([r.eigenvectors for r in results]),
                                  max(r.n_iter for r in results),
