@@ -423,7 +423,7 @@ def run_once(args):
     out = {"mode": "once", "config": args.config, "solver": args.solver, "n_iter": r.n_iter, "wall_ms": wall,
            "n_apply_low": r.n_apply_low, "n_apply_full": r.n_apply_full,
            "max_residual_ev": float(r.residual_norms.max())}
-    for key in ("native", "k_groups", "tc_projection", "phase_ms"):
+    for key in ("native", "k_groups", "tc_projection", "n_tc_fallback", "phase_ms"):
         if key in r.info:
             out[key] = r.info[key]
     gold = _golden(args.config)

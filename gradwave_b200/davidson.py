@@ -33,13 +33,15 @@ Modes:
                       residual is within 100x of the float32 floor (early
                       rounds stagnate without any precision limit).
 In both float32-expansion modes the first of the two projection passes of
-the expansion block, D -= (D V^H) V, and the first Cholesky-QR round run as
-split-precision BF16 products on the tensor cores (``gradwave_b200.tc``,
-error ~1e-6 relative) against a BF16 plane copy of the basis kept current
-row block by row block; the float64 projection pass and the float64
-Cholesky-QR round that follow remove that error, so the block is orthonormal
-and orthogonal to the basis to float64 round-off as before
-(``GWB_TC_PROJECT=0`` keeps every step in float64).
+the expansion block, D -= (D V^H) V, runs as split-precision BF16 products on
+the tensor cores (``gradwave_b200.tc``, error ~1e-6 of the unit input rows)
+against a BF16 plane copy of the basis kept current row block by row block;
+the float64 projection pass and float64 CholQR2 that follow remove that
+error, so the block is orthonormal and orthogonal to the basis to float64
+round-off as before. A block in which some row keeps less than 1e-2 of its
+norm is redone in float64 (``GWB_TC_PROJECT=0`` keeps every step in float64;
+``GWB_TC_STEPS`` selects steps, including an optional tensor-core
+Cholesky-QR round).
 ``precond`` is ``"teter"`` or an object with ``apply_into(...)`` (the learned
 preconditioner, ``gradwave_b200.learned``), which falls back to TPA per band.
 """
@@ -210,6 +212,7 @@ class _Solver:
         self.n_fallback_qr = 0
         self.n_repair = 0
         self.n_rollback = 0
+        self.n_tc_fallback = 0
         self.breakdown = False
         self.mask_u8 = self.mask.to(torch.uint8).contiguous()
         self.stream = _lib.stream_ptr(self.dev)
@@ -222,7 +225,8 @@ class _Solver:
         # tensor-core first projection pass (float32-expansion modes): BF16
         # planes of the basis V, of the expansion block D and of D V^H
         self.tc = None
-        if mode in ("fp32exp", "mixed") and x0.dtype == torch.complex128 and _tc_projection():
+        self.tc_steps = _tc_steps() if mode in ("fp32exp", "mixed") and x0.dtype == torch.complex128 else frozenset()
+        if self.tc_steps:
             from .tc import PlaneSet
             self.tc = (PlaneSet(self.nk, self.max_dim, self.npw, self.dev),
                        PlaneSet(self.nk, self.nb, self.npw, self.dev),
@@ -281,14 +285,18 @@ class _Solver:
 
     def v_rows_changed(self, r0: int, r1: int):
         """Refresh the BF16 planes of basis rows [r0, r1) (tensor-core pass)."""
-        if self.tc is not None and r1 > r0:
+        if self.tc is not None and self.tc_steps & {"nh", "nn"} and r1 > r0:
             md, npw = self.max_dim, self.npw
             self.tc[0].write(self.ws.V, r1 - r0, row0=r0, src_ld=npw, src_kstride=md * npw, offset=r0 * npw,
                              stream=self.stream)
 
-    def project_tc(self, n: int, m: int):
+    def project_tc(self, n: int, m: int) -> bool:
         """D -= (D V^H) V over the first m basis rows as split-BF16
-        tensor-core products (error ~1e-5 relative; a float64 pass follows)."""
+        tensor-core products (error ~1e-6 of the unit input rows; a float64
+        pass follows). A row that keeps less than 1e-2 of its norm would be
+        dominated by that error (near-converged bands whose corrections lie
+        almost in the basis), so then the whole block is redone with the
+        float64 pass from a saved copy (checked on the host). False if so."""
         from .tc import OP_H, OP_N, work_bytes, zgemm_tc
         pv, pd, pc = self.tc
         ws, npw = self.ws, self.npw
@@ -296,11 +304,27 @@ class _Solver:
         need = work_bytes(OP_H, n, m, npw, self.nk)
         if self.tc_work is None or self.tc_work.numel() < need:
             self.tc_work = torch.empty(max(need, 1 << 20), dtype=torch.uint8, device=self.dev)
-        pd.write(ws.D, n, src_ld=npw, src_kstride=ds, stream=self.stream)
-        zgemm_tc(OP_H, n, m, npw, pd, pv, ws.C, m, n * m, stream=self.stream, status=ws.flags, work=self.tc_work)
-        pc.write(ws.C, n, src_ld=m, src_kstride=n * m, cols=m, stream=self.stream)
-        zgemm_tc(OP_N, n, npw, m, pc, pv, ws.D, npw, ds, alpha=-1.0, beta=1.0, stream=self.stream,
-                 status=ws.flags, work=self.tc_work)
+        md = self.max_dim
+        ws.D2[:, :n].copy_(ws.D[:, :n])
+        if "nh" in self.tc_steps:
+            pd.write(ws.D, n, src_ld=npw, src_kstride=ds, stream=self.stream)
+            zgemm_tc(OP_H, n, m, npw, pd, pv, ws.C, m, n * m, stream=self.stream, status=ws.flags,
+                     work=self.tc_work)
+        else:
+            self.zgemm(_N, _H, n, m, npw, ws.D, npw, ds, ws.V, npw, md * npw, ws.C, m, n * m, self.nk)
+        if "nn" in self.tc_steps:
+            pc.write(ws.C, n, src_ld=m, src_kstride=n * m, cols=m, stream=self.stream)
+            zgemm_tc(OP_N, n, npw, m, pc, pv, ws.D, npw, ds, alpha=-1.0, beta=1.0, stream=self.stream,
+                     status=ws.flags, work=self.tc_work)
+        else:
+            self.zgemm(_N, _N, n, npw, m, ws.C, m, n * m, ws.V, npw, md * npw, ws.D, npw, ds, self.nk, alpha=-1.0,
+                       beta=1.0)
+        if float(torch.linalg.vector_norm(ws.D[:, :n], dim=-1).min()) < 1e-2:
+            ws.D[:, :n].copy_(ws.D2[:, :n])
+            self.project_out(ws.D, n, m, passes=1)
+            self.n_tc_fallback += 1
+            return False
+        return True
 
     def chol_inv(self, n: int, sync: bool) -> bool:
         """ws.Linv[:n, :n] = L^-1 for the Cholesky factor L of ws.G (both as
@@ -337,9 +361,21 @@ class _Solver:
         need = work_bytes(OP_H, n, n, npw, nk)
         if self.tc_work is None or self.tc_work.numel() < need:
             self.tc_work = torch.empty(max(need, 1 << 20), dtype=torch.uint8, device=self.dev)
+        # unit rows first, so the FP32-accumulated Gram matrix resolves every
+        # row to the same relative accuracy
+        blk = ws.D[:, :n]
+        blk.div_(torch.linalg.vector_norm(blk, dim=-1, keepdim=True))
         pd.write(ws.D, n, src_ld=npw, src_kstride=ds, stream=self.stream)
         zgemm_tc(OP_H, n, n, npw, pd, pd, ws.G, n, n * n, stream=self.stream, status=ws.flags, work=self.tc_work)
         if not self.chol_inv(n, sync=True):
+            self.n_tc_fallback += 1
+            return False
+        # unit rows: 1 / L_ii is the inverse distance of row i from the span
+        # of the rows before it; above 100 the BF16 error of the block,
+        # amplified by L^-1, would swamp the new directions
+        Li = ws.Linv.view(-1)[: nk * n * n].view(nk, n, n)
+        if float(torch.diagonal(Li, dim1=-2, dim2=-1).abs().max()) > 1e2:
+            self.n_tc_fallback += 1
             return False
         pc.write(ws.Linv, n, src_ld=n, src_kstride=n * n, cols=n, stream=self.stream)
         zgemm_tc(OP_N, n, npw, n, pc, pd, ws.D, npw, ds, stream=self.stream, status=ws.flags, work=self.tc_work)
@@ -369,7 +405,7 @@ class _Solver:
         D[:, :n].mul_(self.mask[:, None, :])
         if not safe:
             if m:
-                if self.tc is not None:
+                if self.tc_steps & {"nh", "nn"}:
                     self.project_tc(n, m)
                 else:
                     self.project_out(D, n, m, passes=1)
@@ -378,7 +414,7 @@ class _Solver:
             # tensor-core Cholesky-QR round before the float64 projection, so
             # that the float64 pass still sets the orthogonality to the basis;
             # one float64 Cholesky-QR round then finishes the block
-            tc_round = self.tc is not None and self.cholqr_tc(n)
+            tc_round = "chol" in self.tc_steps and self.cholqr_tc(n)
             if m:
                 self.project_out(D, n, m, passes=1)
             self.cholqr2(D, n, ws.D2, sync=False, passes=1 if tc_round else 2)
@@ -582,7 +618,8 @@ class _Solver:
         if self.out_dtype != torch.complex128:
             x = x.to(self.out_dtype)
         info = {"n_restart": self.n_restart, "n_cert": self.n_cert, "n_fallback_qr": self.n_fallback_qr,
-                "tc_projection": self.tc is not None,
+                "tc_projection": self.tc is not None, "tc_steps": sorted(self.tc_steps),
+                "n_tc_fallback": self.n_tc_fallback,
                 "n_repair": self.n_repair, "n_rollback": self.n_rollback,
                 "max_dim": self.max_dim, "phase_ms": self.prof.summary()}
         return BatchedDavidsonResult(eig.clone(), x, it, ws.rn.clone(), self.n_low, self.n_full, info)
@@ -624,13 +661,30 @@ def _native_solve(ham, x0, t, mask, tol, max_iter, max_dim, mode, time_applies=F
     return BatchedDavidsonResult(eig, vec, int(st.n_iter), rn, int(st.n_apply_low), int(st.n_apply_full), info)
 
 
-def _tc_projection() -> bool:
-    """Whether the float32-expansion modes run their first projection pass on
-    the tensor cores (``GWB_TC_PROJECT``, default 1)."""
-    v = os.environ.get("GWB_TC_PROJECT", "1")
-    if v not in ("0", "1"):
+_TC_STEP_NAMES = ("nh", "nn", "chol")
+
+
+def _tc_steps() -> frozenset:
+    """Steps of the float32-expansion modes' orthonormalisation that run as
+    tensor-core products: ``nh`` the coefficients D V^H of the first
+    projection pass, ``nn`` its update D -= C V, ``chol`` the first
+    Cholesky-QR round. ``GWB_TC_PROJECT=0`` turns all off; ``GWB_TC_STEPS`` (a
+    comma list) picks a subset. The default is the projection pass (nh, nn):
+    the tensor-core Cholesky-QR round perturbs the new directions by the BF16
+    error amplified by L^-1, and on the 64-atom cell that let one band stall
+    just above tolerance until the next restart (192-235 rounds against 64-75
+    without it), for a saving of two n x n x npw products per round."""
+    if os.environ.get("GWB_TC_PROJECT", "1") == "0":
+        return frozenset()
+    if os.environ.get("GWB_TC_PROJECT", "1") != "1":
         raise ValueError("GWB_TC_PROJECT must be 0 or 1")
-    return v == "1"
+    v = os.environ.get("GWB_TC_STEPS")
+    if v is None:
+        return frozenset(("nh", "nn"))
+    steps = frozenset(x.strip() for x in v.split(",") if x.strip())
+    if not steps <= set(_TC_STEP_NAMES):
+        raise ValueError(f"GWB_TC_STEPS must name steps among {_TC_STEP_NAMES}")
+    return steps
 
 
 def _k_groups(default: int) -> int:
@@ -711,7 +765,8 @@ def _solve_grouped(ham, x0, t, mask, tol, max_iter, max_dim_factor, mode, groups
         for x in (r.eigenvalues, r.eigenvectors, r.residual_norms):
             x.record_stream(main)
     info = {"native": native, "k_groups": g_n, "max_dim": max(r.info["max_dim"] for r in results)}
-    for key in ("n_restart", "n_cert", "n_repair", "n_rollback", "n_apply_calls", "apply_ms", "n_fallback_qr"):
+    for key in ("n_restart", "n_cert", "n_repair", "n_rollback", "n_apply_calls", "apply_ms", "n_fallback_qr",
+                "n_tc_fallback"):
         if key in results[0].info:
             info[key] = sum(r.info[key] for r in results)
     if "tc_projection" in results[0].info:

@@ -120,23 +120,27 @@ def test_native_and_host_driver_agree(cuda_device, monkeypatch):
         assert abs(native.n_iter - host.n_iter) <= 3
 
 
-@pytest.mark.parametrize("mode", ["fp32exp", "mixed"])
-def test_tensor_core_projection_pass_keeps_parity(cuda_device, monkeypatch, mode):
+@pytest.mark.parametrize("mode,steps", [("fp32exp", None), ("mixed", None), ("mixed", "nh,nn,chol")])
+def test_tensor_core_projection_pass_keeps_parity(cuda_device, monkeypatch, mode, steps):
     """The float32-expansion modes of the host driver run the first projection
-    pass as split-BF16 tensor-core products; the float64 second pass removes
-    their error: same eigenvalues as the reference, an orthonormal block, and
-    about the same number of rounds as with both passes in float64."""
+    pass (and, when selected, a first Cholesky-QR round) as split-BF16
+    tensor-core products; the float64 steps after them remove their error:
+    same eigenvalues as the reference, an orthonormal block, and about the
+    same number of rounds as with every step in float64."""
     from gradwave_b200.davidson import davidson_batched
     g = load_golden("si8_cubic")
     ci, bk, h = _cell_ham("si8_cubic")
     x0 = ci.identity_start().to(cuda_device)
     monkeypatch.setenv("GWB_NATIVE", "0")
+    if steps is not None:
+        monkeypatch.setenv("GWB_TC_STEPS", steps)
     runs = {}
     for tc in ("1", "0"):
         monkeypatch.setenv("GWB_TC_PROJECT", tc)
         runs[tc] = davidson_batched(h.apply, x0, bk.t, bk.mask, tol=1e-10, max_iter=200, mode=mode)
     res = runs["1"]
     assert res.info["tc_projection"] and not runs["0"].info["tc_projection"]
+    assert set(res.info["tc_steps"]) == ({"nh", "nn", "chol"} if steps else {"nh", "nn"})
     assert float(res.residual_norms.max()) < 1e-10
     assert np.abs(res.eigenvalues.cpu().numpy() - g["eigenvalues"]).max() < EIG_TOL_HA
     x = res.eigenvectors
