@@ -84,6 +84,7 @@ _SIGNATURES = {
     "gwb_ham_apply_strided": [_P, _P, _I64, _P, _I64, _I, _I, _I, _P],
     "gwb_ham_scratch_bytes": [_P],
     "gwb_ham_tc_status": [_P, _P],
+    "gwb_ham_density": [_P, _P, _I64, _I, _I, _P, _I64, _D, _P, _P],
     "gwb_zgemm": [ctypes.c_int, ctypes.c_int, _I64, _I64, _I64, _D, _D, _P, _I64, _I64, _P, _I64, _I64,
                   _D, _D, _P, _I64, _I64, _I64, _P],
     "gwb_zgemm_nh": [_I64, _I64, _I64, _D, _D, _P, _I64, _I64, _P, _I64, _I64, _D, _D, _P, _I64, _I64, _I64, _P,

@@ -94,6 +94,8 @@ struct gwb_ham {
   void* d_tcwork = nullptr;  // split-K partial sums
   size_t tcwork_bytes = 0;
   int* d_tcstatus = nullptr;  // pipeline-wait timeouts of the tensor-core products
+  double* d_rhok = nullptr;  // density accumulators, one box per k
+  size_t rhok_bytes = 0;
   bool have_t = false, have_v = false, have_p = false;
 };
 
@@ -231,6 +233,95 @@ __global__ void __launch_bounds__(128) k_pencil_vloc_reg(FftGeom g, cplx<T>* __r
     if (r <= M0) base[r * PLANE] = x[r];
     else if (r >= hi0) wrap[r * PLANE] = x[r];
   });
+}
+
+// Density (gradwave core/batch.py:562-587, density_b): after K1 has put a
+// chunk of bands into W (inverse FFT along axes 2 and 1 over the occupied
+// planes), the axis-0 inverse FFT of each pencil and rho_k[k][r] +=
+// w[k][b] |psi_b(r)|^2, float64. One CTA (general box) or one thread (cubic
+// box, whole pencil in registers) owns each output element of one k and loops
+// over the chunk's bands, so the sums need no atomics and run in a fixed order.
+template <typename T, unsigned C0>
+__global__ void __launch_bounds__(256) k_pencil_density(FftGeom g, const cplx<T>* __restrict__ W,
+                                                        const cplx<T>* __restrict__ tw0,
+                                                        const double* __restrict__ w, int64_t wk, int b0, int nbc,
+                                                        double* __restrict__ rho_k, int first) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2], L0 = g.L[0];
+  const int i1 = blockIdx.x, k = blockIdx.z;
+  const size_t N = (size_t)n0 * n1 * n2;
+  cplx<T>* S = reinterpret_cast<cplx<T>*>(smem_raw);  // [i0][i2]
+  cplx<T>* t0 = S + n0 * n2;
+  for (int i = threadIdx.x; i < n0; i += blockDim.x) t0[i] = tw0[i];
+  double* rk = rho_k + (size_t)k * N + (size_t)i1 * n2;
+  if (first)
+    for (int i = threadIdx.x; i < n0 * n2; i += blockDim.x) {
+      const int i0 = i / n2, i2 = i - i0 * n2;
+      rk[(size_t)i0 * n1 * n2 + i2] = 0.0;
+    }
+  for (int bl = 0; bl < nbc; ++bl) {
+    const double wb = w[(size_t)k * wk + b0 + bl];
+    if (wb == 0.0) continue;  // the same for every thread of the CTA
+    const cplx<T>* base = W + ((size_t)k * nbc + bl) * L0 * (size_t)(n1 * n2) + (size_t)i1 * n2;
+    __syncthreads();  // S of the previous band fully read
+    for (int i = threadIdx.x; i < n0 * n2; i += blockDim.x) {
+      const int r = i / n2, i2 = i - r * n2;
+      int j0;
+      if (r <= g.M[0]) j0 = r;
+      else if (r >= n0 - (L0 - g.M[0] - 1)) j0 = r - (n0 - L0);
+      else j0 = -1;
+      S[i] = j0 >= 0 ? base[(size_t)j0 * n1 * n2 + i2] : mk<T>(0, 0);
+    }
+    __syncthreads();
+    fft_any<T, true, +1, C0>(S, n2, g.plan[0], 1, n2, n2, n2, t0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < n0 * n2; i += blockDim.x) {
+      const int i0 = i / n2, i2 = i - i0 * n2;
+      const cplx<T> v = S[i];
+      rk[(size_t)i0 * n1 * n2 + i2] += wb * ((double)v.x * (double)v.x + (double)v.y * (double)v.y);
+    }
+  }
+}
+
+template <typename T, int N0>
+__global__ void __launch_bounds__(128) k_pencil_density_reg(FftGeom g, const cplx<T>* __restrict__ W,
+                                                            const double* __restrict__ w, int64_t wk, int b0,
+                                                            int nbc, double* __restrict__ rho_k, int first) {
+  constexpr int PLANE = N0 * N0;
+  const int L0 = g.L[0], M0 = g.M[0];
+  const int k = blockIdx.z;
+  const int pidx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pidx >= PLANE) return;
+  double* rk = rho_k + (size_t)k * N0 * PLANE + pidx;
+  if (first)
+    rdft_detail::StaticFor<0, N0>::run([&](auto rc) { rk[decltype(rc)::value * PLANE] = 0.0; });
+  const int hi0 = N0 - (L0 - M0 - 1);
+  for (int bl = 0; bl < nbc; ++bl) {
+    const double wb = w[(size_t)k * wk + b0 + bl];
+    if (wb == 0.0) continue;
+    const cplx<T>* base = W + ((size_t)k * nbc + bl) * L0 * (size_t)PLANE + pidx;
+    const cplx<T>* wrap = base - (ptrdiff_t)(N0 - L0) * PLANE;
+    cplx<T> x[N0];
+    rdft_detail::StaticFor<0, N0>::run([&](auto rc) {
+      constexpr int r = decltype(rc)::value;
+      x[r] = r <= M0 ? base[r * PLANE] : (r >= hi0 ? wrap[r * PLANE] : mk<T>(0, 0));
+    });
+    rdft<N0, +1>(x);
+    rdft_detail::StaticFor<0, N0>::run([&](auto rc) {
+      constexpr int r = decltype(rc)::value;
+      rk[r * PLANE] += wb * ((double)x[r].x * (double)x[r].x + (double)x[r].y * (double)x[r].y);
+    });
+  }
+}
+
+// rho[r] = scale sum_k rho_k[k][r], k in order.
+__global__ void k_density_sum(int nk, int64_t N, const double* __restrict__ rho_k, double scale,
+                              double* __restrict__ rho) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+    double a = 0.0;
+    for (int k = 0; k < nk; ++k) a += rho_k[(int64_t)k * N + i];
+    rho[i] = scale * a;
+  }
 }
 
 // K1 and K3 with whole transforms in registers (cubic box, N <= 48): a CTA
@@ -735,6 +826,80 @@ static int apply_impl(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t ok
   return GWB_OK;
 }
 
+
+// Density of nb bands (float64 FFTs): K1 per band chunk into W, then the
+// pencil kernel accumulating w |psi|^2 into rho_k, finally the k sum.
+template <typename SIO, unsigned C>
+static int density_chunks(gwb_ham* h, const SIO* c, int64_t ck, int nb, int nbc, const double* w, int64_t wk,
+                          cudaStream_t st, size_t smA, size_t smB) {
+  using T = double;
+  const FftGeom& g = h->g;
+  const cplx<T>* tw0 = (const cplx<T>*)h->d_tw64[0];
+  const cplx<T>* tw1 = (const cplx<T>*)h->d_tw64[1];
+  const cplx<T>* tw2 = (const cplx<T>*)h->d_tw64[2];
+  cplx<T>* W = (cplx<T>*)h->d_W;
+  const bool cubic = g.n[0] == g.n[1] && g.n[1] == g.n[2];
+  const int nreg = (cubic && g.n[0] == 36 && C == kCode36) ? 36 : ((cubic && g.n[0] == 24 && C == kCode24) ? 24 : 0);
+  const size_t smR = (size_t)PLR * nreg * (nreg + 1) * sizeof(cplx<T>);
+  GWB_CUDA_TRY(allow_smem(k_plane_inverse<T, SIO, C, C>));
+  GWB_CUDA_TRY(allow_smem(k_pencil_density<T, C>));
+  if (nreg == 36) GWB_CUDA_TRY(allow_smem(k_plane_inverse_reg<T, SIO, 36>));
+  if (nreg == 24) GWB_CUDA_TRY(allow_smem(k_plane_inverse_reg<T, SIO, 24>));
+  for (int b0 = 0; b0 < nb; b0 += nbc) {
+    const int cb = std::min(nbc, nb - b0);
+    const int first = b0 == 0;
+    dim3 gA(g.L[0], cb, h->nk), gP((g.L[0] + PLR - 1) / PLR, cb, h->nk);
+    dim3 gR((g.n[1] * g.n[2] + 127) / 128, 1, h->nk), gB(g.n[1], 1, h->nk);
+    if (nreg == 36) {
+      k_plane_inverse_reg<T, SIO, 36><<<gP, PLR * 36, smR, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos, c,
+                                                                 W, ck, b0, cb, h->npw_max);
+      k_pencil_density_reg<T, 36><<<gR, 128, 0, st>>>(g, W, w, wk, b0, cb, h->d_rhok, first);
+    } else if (nreg == 24) {
+      k_plane_inverse_reg<T, SIO, 24><<<gP, PLR * 24, smR, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos, c,
+                                                                 W, ck, b0, cb, h->npw_max);
+      k_pencil_density_reg<T, 24><<<gR, 128, 0, st>>>(g, W, w, wk, b0, cb, h->d_rhok, first);
+    } else {
+      k_plane_inverse<T, SIO, C, C><<<gA, 256, smA, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos, c, W,
+                                                         tw1, tw2, ck, b0, cb, h->npw_max);
+      k_pencil_density<T, C><<<gB, 256, smB, st>>>(g, W, tw0, w, wk, b0, cb, h->d_rhok, first);
+    }
+    GWB_LAUNCH_CHECK();
+    count_launches(2);
+  }
+  return GWB_OK;
+}
+
+template <typename SIO>
+static int density_impl(gwb_ham* h, const SIO* c, int64_t ck, int nb, const double* w, int64_t wk, double scale,
+                        double* rho, cudaStream_t st) {
+  const FftGeom& g = h->g;
+  const size_t es = sizeof(cplx<double>);
+  const size_t N = (size_t)g.n[0] * g.n[1] * g.n[2];
+  const size_t per_band = (size_t)h->nk * g.L[0] * g.n[1] * g.n[2] * es;
+  const size_t budget = std::max(w_budget_bytes(), per_band);
+  const size_t max_nbc = std::max<size_t>(1, budget / per_band);
+  const size_t nchunks = ((size_t)nb + max_nbc - 1) / max_nbc;
+  int nbc = (int)(((size_t)nb + nchunks - 1) / nchunks);
+  if (nbc < 1) nbc = 1;
+  int rc = ensure_buf(&h->d_W, &h->W_bytes, per_band * nbc);
+  if (rc) return rc;
+  rc = ensure_buf((void**)&h->d_rhok, &h->rhok_bytes, (size_t)h->nk * N * sizeof(double));
+  if (rc) return rc;
+  const size_t smA = plane_smem(g, es), smB = pencil_smem(g, es);
+  const unsigned c0 = g.plan[0].code, c1 = g.plan[1].code, c2 = g.plan[2].code;
+  const bool cubic = c0 == c1 && c1 == c2;
+  if (cubic && c0 == kCode24) rc = density_chunks<SIO, kCode24>(h, c, ck, nb, nbc, w, wk, st, smA, smB);
+  else if (cubic && c0 == kCode36) rc = density_chunks<SIO, kCode36>(h, c, ck, nb, nbc, w, wk, st, smA, smB);
+  else if (cubic && c0 == kCode72) rc = density_chunks<SIO, kCode72>(h, c, ck, nb, nbc, w, wk, st, smA, smB);
+  else if (cubic && c0 == kCode96) rc = density_chunks<SIO, kCode96>(h, c, ck, nb, nbc, w, wk, st, smA, smB);
+  else rc = density_chunks<SIO, 0u>(h, c, ck, nb, nbc, w, wk, st, smA, smB);
+  if (rc) return rc;
+  const int blocks = (int)std::min<size_t>((N + 255) / 256, 148 * 8);
+  k_density_sum<<<blocks, 256, 0, st>>>(h->nk, (int64_t)N, h->d_rhok, scale, rho);
+  GWB_LAUNCH_CHECK();
+  count_launches(1);
+  return GWB_OK;
+}
 }  // namespace gwb
 
 using namespace gwb;
@@ -872,7 +1037,7 @@ int gwb_ham_destroy(gwb_ham* h) {
   if (!h) return GWB_OK;
   void* ptrs[] = {h->d_npw, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos, h->d_t64, h->d_t32, h->d_v64,
                   h->d_v32, h->d_p64, h->d_p32, h->d_d64, h->d_d32, h->d_W, h->d_part, h->d_bd,
-                  h->d_pplanes, h->d_cplanes, h->d_becp, h->d_bdplanes, h->d_tcwork, h->d_tcstatus,
+                  h->d_pplanes, h->d_cplanes, h->d_becp, h->d_bdplanes, h->d_tcwork, h->d_tcstatus, h->d_rhok,
                   h->d_tw64[0], h->d_tw64[1], h->d_tw64[2], h->d_tw32[0], h->d_tw32[1], h->d_tw32[2]};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -961,9 +1126,23 @@ int gwb_ham_apply(gwb_ham* h, const void* c, void* out, int32_t nb, int32_t io_d
   return gwb_ham_apply_strided(h, c, ks, out, ks, nb, io_dtype, prec, stream);
 }
 
+int gwb_ham_density(gwb_ham* h, const void* c, int64_t c_kstride, int32_t nb, int32_t io_dtype,
+                    const double* weights, int64_t w_kstride, double scale, double* rho, void* stream) {
+  GWB_REQUIRE(h && c && weights && rho, "null argument");
+  GWB_REQUIRE(nb > 0, "nb must be positive");
+  GWB_REQUIRE(io_dtype == GWB_C64 || io_dtype == GWB_C128, "io_dtype must be GWB_C64 or GWB_C128");
+  GWB_REQUIRE(c_kstride >= (int64_t)nb * h->npw_max, "k stride smaller than nb * npw_max");
+  GWB_REQUIRE(w_kstride >= nb, "weight k stride smaller than nb");
+  GWB_CUDA_TRY(cudaSetDevice(h->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  if (io_dtype == GWB_C128)
+    return density_impl(h, (const cplx<double>*)c, c_kstride, nb, weights, w_kstride, scale, rho, st);
+  return density_impl(h, (const cplx<float>*)c, c_kstride, nb, weights, w_kstride, scale, rho, st);
+}
+
 size_t gwb_ham_scratch_bytes(const gwb_ham* h) {
   return h ? h->W_bytes + h->part_bytes + h->bd_bytes + h->pplanes_bytes + h->cplanes_bytes + h->becp_bytes +
-                 h->bdplanes_bytes + h->tcwork_bytes
+                 h->bdplanes_bytes + h->tcwork_bytes + h->rhok_bytes
            : 0;
 }
 

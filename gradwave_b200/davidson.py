@@ -812,6 +812,10 @@ def davidson_batched(h_apply, x0, t, mask, tol: float = 1e-9, max_iter: int = 40
         if native:
             time_applies = os.environ.get("GWB_TIME_APPLIES", "0") == "1"
             model = getattr(precond, "params", None)
+            # one group by default: two concurrent groups were ~5 % faster on
+            # si8 but change the rounds' trajectory (each group keeps its own
+            # uniform subspace), and in one such trajectory the learned fp64
+            # solve missed an eigenvalue by 0.72 eV
             groups = _k_groups(1)
             if groups > 1 and nk > 1 and hasattr(ham, "k_slice"):
                 res = _solve_grouped(ham, x0, t, mask, tol, max_iter, max_dim_factor, mode, groups, native=True,

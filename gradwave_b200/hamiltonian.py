@@ -156,5 +156,14 @@ class BatchedHamiltonian:
                                             self.p[start:end])
         return cache[key]
 
+    def density(self, coeffs: torch.Tensor, occ: torch.Tensor, kweights: torch.Tensor,
+                volume: float) -> torch.Tensor:
+        """rho(r) = sum_k w_k sum_n f_kn |psi_kn(r)|^2 / volume on this
+        operator's box, float64 (gradwave ``core/batch.py:562-587``,
+        ``density_b``), with this handle's geometry and scratch."""
+        from .density import density_from_handle
+        self._check(coeffs)
+        return density_from_handle(self._h, self.nk, self.npw_max, self.shape, coeffs, occ, kweights, volume)
+
     def scratch_bytes(self) -> int:
         return int(_lib.load().gwb_ham_scratch_bytes(self._h))

@@ -107,6 +107,19 @@ int gwb_ham_apply(gwb_ham* h, const void* c, void* out, int32_t nb, int32_t io_d
 int gwb_ham_apply_strided(gwb_ham* h, const void* c, int64_t c_kstride, void* out, int64_t out_kstride,
                           int32_t nb, int32_t io_dtype, int32_t prec, void* stream);
 
+/* Electron density on the box: rho[r] = scale * sum_k sum_b weights[k*w_kstride + b]
+ * |psi_kb(r)|^2 with psi_kb(r) = sum_G c_kb(G) exp(iG.r) (the unnormalised
+ * inverse FFT of the sphere coefficients; padded slots of c must be zero, as
+ * they are in the eigenvectors). rho is (n0*n1*n2) float64, device; the FFTs
+ * and sums run in float64 whatever the storage of c. For gradwave's
+ * density_b pass weights = kweights[k] * occ[k, b] and scale = 1 / volume.
+ * Needs only the geometry of the handle (no kinetic, potential or
+ * projectors), and uses the handle's scratch: do not overlap it with an
+ * apply on the same handle. Replaces gradwave core/batch.py:562-587
+ * (density_b) with g_to_r_b (core/batch.py:208-216). */
+int gwb_ham_density(gwb_ham* h, const void* c, int64_t c_kstride, int32_t nb, int32_t io_dtype,
+                    const double* weights, int64_t w_kstride, double scale, double* rho, void* stream);
+
 /* Bytes of handle-owned device scratch currently held. */
 size_t gwb_ham_scratch_bytes(const gwb_ham* h);
 

@@ -15,9 +15,10 @@ What is recorded, per case:
     random block - in full for small cases, else as projections on seeded
     random vectors (size-independent checksums);
   * solve: ``davidson_batched`` (``solvers/davidson.py:528-774``) from the
-    identity start at tol 1e-10 eV: eigenvalues, residual norms, rounds, applies.
+    identity start at tol 1e-10 eV: eigenvalues, residual norms, rounds, applies;
+  * density: ``density_b`` (``core/batch.py:562-587``) on a seeded block.
 
-Usage: python tests/golden/make_golden.py [small|big|all] [--ref /path/to/gradwave/src]
+Usage: python tests/golden/make_golden.py [small|big|all|density] [--ref /path/to/gradwave/src]
 """
 
 from __future__ import annotations
@@ -130,6 +131,35 @@ def run_case(name: str, seed_cell: int, apply_nb: int, full_apply: bool, solve: 
     return rec
 
 
+def density_case(name: str, nb: int, seed: int, full: bool) -> dict:
+    """``density_b`` (``core/batch.py:562-587``) on a seeded block with zero
+    padding and seeded occupations in [0, 2]; the full rho for small boxes,
+    else checksums (sum, sum of squares, projections on seeded vectors)."""
+    from gradwave.core.batch import density_b
+
+    ci = make_cell(name)
+    grid, bk, _ = reference_setup(ci)
+    nk, npw = bk.mask.shape
+    c = random_block(seed, nk, nb, npw) * bk.mask.numpy()[:, None, :]
+    occ = np.random.default_rng(seed + 1).uniform(0.0, 2.0, (nk, nb))
+    kw = np.asarray(ci.kweights, dtype=np.float64)
+    rho = density_b(torch.from_numpy(c), torch.from_numpy(occ), torch.from_numpy(kw), bk, grid.shape,
+                    grid.volume).numpy()
+    rec = {"nb": np.array(nb), "seed": np.array(seed), "occ": occ, "kweights": kw, "volume": np.array(grid.volume),
+           "rho_chk": density_checksums(rho, seed)}
+    if full:
+        rec["rho"] = rho
+    return rec
+
+
+def density_checksums(rho: np.ndarray, seed: int, nvec: int = 3) -> np.ndarray:
+    rng = np.random.default_rng(seed + 2000)
+    vals = [rho.sum(), (rho * rho).sum()]
+    for _ in range(nvec):
+        vals.append(float((rng.standard_normal(rho.shape) * rho).sum()))
+    return np.array(vals)
+
+
 def synthetic_case(seed: int = 2, nk: int = 4, npw: int = 80, nb: int = 8) -> dict:
     """Dense random Hermitian operator with a kinetic-like diagonal; isolates
     the eigensolver from the FFT."""
@@ -154,7 +184,7 @@ def synthetic_case(seed: int = 2, nk: int = 4, npw: int = 80, nb: int = 8) -> di
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("which", nargs="?", default="small", choices=["small", "big", "all"])
+    ap.add_argument("which", nargs="?", default="small", choices=["small", "big", "all", "density"])
     ap.add_argument("--ref", default="/root/reference/src")
     args = ap.parse_args()
     shim(args.ref)
@@ -167,6 +197,12 @@ def main():
             ("si8_cubic_fp32exp", lambda: run_case("si8_cubic", 0, 1, False, True, fp32_expansion=True)),
             ("si8_perturbed", lambda: run_case("si8_perturbed", 1, 2, False, False)),
             ("synthetic", synthetic_case),
+        ]
+    if args.which in ("density", "all"):
+        jobs += [
+            ("density_si2_fcc", lambda: density_case("si2_fcc", 6, 21, True)),
+            ("density_si8_cubic", lambda: density_case("si8_cubic", 5, 22, False)),
+            ("density_si64_cubic", lambda: density_case("si64_cubic", 3, 23, False)),
         ]
     if args.which in ("big", "all"):
         jobs += [

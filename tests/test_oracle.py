@@ -100,3 +100,21 @@ def test_mlp_oracle_backward_matches_finite_differences():
         pm[i] -= h
         fd = (mlp.loss_grad(pp, u, y, w, False)[0] - mlp.loss_grad(pm, u, y, w, False)[0]) / (2 * h)
         assert abs(fd - g[i]) <= 1e-6 * (abs(fd) + abs(g[i])) + 1e-12
+
+
+@pytest.mark.parametrize("name", ["si2_fcc", "si8_cubic"])
+def test_oracle_density_matches_reference(name):
+    """The numpy density (``oracle/density.py``) against the reference's own
+    ``density_b`` on the same seeded block and occupations."""
+    from gradwave_b200.cells import make_cell
+    from oracle.density import density_b
+    from tests.golden.make_golden import density_checksums
+    g = load_golden(f"density_{name}")
+    ci = make_cell(name)
+    nb, seed = int(g["nb"]), int(g["seed"])
+    c = random_block(seed, ci.bk.nk, nb, ci.bk.npw_max) * ci.bk.mask.numpy()[:, None, :]
+    rho = density_b(c, g["occ"], g["kweights"], ci.bk.flat_idx.numpy(), ci.shape, float(g["volume"]))
+    chk = density_checksums(rho, seed)
+    assert np.abs(chk - g["rho_chk"]).max() / np.abs(g["rho_chk"]).max() < 1e-12
+    if "rho" in g:
+        assert np.abs(rho - g["rho"]).max() / np.abs(g["rho"]).max() < 1e-12
