@@ -146,6 +146,34 @@ class CellInputs:
         return 2 * len(self.positions)   # 4 valence electrons per Si, 2 per band
 
 
+def _projector_tables(spheres, positions, volume):
+    """Per-k projector data of the analytic s + p Kleinman-Bylander channels
+    (the recipe every cell uses)."""
+    sp = _SPEC["species"]["Si"]
+    rc = float(sp["rc"])
+    pds = []
+    for s in spheres:
+        q = np.sqrt(s.kpg2)
+        tab = np.stack([np.exp(-0.5 * (q * rc) ** 2), q * rc * np.exp(-0.5 * (q * rc) ** 2)])
+        pds.append(build_projector_data(s, [0] * len(positions), [tab], [[0, 1]], [np.diag(sp["D"])], volume))
+    return pds
+
+
+def at_kpoints(ci: CellInputs, kpoints_frac, kweights=None) -> CellInputs:
+    """The same cell, box and frozen potential at other k-points (fractional
+    coordinates): spheres, batched tables and projectors rebuilt, weights
+    uniform unless given (the non-SCF set-up of gradwave
+    ``postscf/bands.py:68-85``)."""
+    kfr = np.asarray(kpoints_frac, dtype=np.float64).reshape(-1, 3)
+    kw = np.full(len(kfr), 1.0 / len(kfr)) if kweights is None else np.asarray(kweights, dtype=np.float64)
+    spheres = [build_gsphere(ci.grid, ci.ecut, k) for k in kfr]
+    bk = build_batched(spheres, _projector_tables(spheres, ci.positions, ci.grid.volume))
+    p = projectors_b(bk, ci.positions)
+    return CellInputs(name=f"{ci.name}@path", cell=ci.cell, positions=ci.positions, ecut=ci.ecut, grid=ci.grid,
+                      spheres=spheres, kpoints=kfr, kweights=kw, bk=bk, v_eff_r=ci.v_eff_r, p=p,
+                      nbands=ci.nbands, meta=dict(ci.meta))
+
+
 def make_cell(name: str, seed: int = 0) -> CellInputs:
     """Build one workload. ``seed`` only matters for seeded variants
     (displaced/strained cells, vacancy placement)."""
@@ -157,14 +185,7 @@ def make_cell(name: str, seed: int = 0) -> CellInputs:
     grid = build_fft_grid(cell, ecut, shape_override=spec["fft"])
     kfr, kw = _kpoints(spec["kpoints"])
     spheres = [build_gsphere(grid, ecut, k) for k in kfr]
-    rc = float(sp["rc"])
-    pds = []
-    for s in spheres:
-        q = np.sqrt(s.kpg2)
-        tab = np.stack([np.exp(-0.5 * (q * rc) ** 2), q * rc * np.exp(-0.5 * (q * rc) ** 2)])
-        pds.append(build_projector_data(s, [0] * len(pos), [tab], [[0, 1]],
-                                        [np.diag(sp["D"])], grid.volume))
-    bk = build_batched(spheres, pds)
+    bk = build_batched(spheres, _projector_tables(spheres, pos, grid.volume))
     extra = []
     meta = {}
     if "vacancies" in spec:

@@ -67,3 +67,31 @@ def test_fft_box_and_sphere_conventions():
     m = sph.miller
     assert np.array_equal(sph.flat_idx, (m[:, 0] % n0) * n1 * n2 + (m[:, 1] % n1) * n2 + (m[:, 2] % n2))
     assert np.all(np.diff(np.round(sph.kpg2, 10)) >= 0)
+
+
+def test_band_path_and_chunk_rule():
+    """The k-path stand-in for ASE's bandpath: special points on the path at
+    the labelled indices, segments sampled in proportion to their length,
+    monotone coordinate; the reference's chunk rule (at most 24 k, fewer when
+    dense boxes would pass 1.5 GB)."""
+    from gradwave_b200.bands import chunk_size, k_path
+    a = 5.43
+    cell = 0.5 * a * np.array([[0.0, 1.0, 1.0], [1.0, 0.0, 1.0], [1.0, 1.0, 0.0]])
+    pts = [("L", [0.5, 0.5, 0.5]), ("G", [0.0, 0.0, 0.0]), ("X", [0.5, 0.0, 0.5])]
+    k, x, labels = k_path(cell, pts, 31)
+    assert k.shape == (31, 3)
+    assert [lab for _, lab in labels] == ["L", "G", "X"]
+    for (i, _), (_, p) in zip(labels, pts):
+        assert np.allclose(k[i], p)
+    assert labels[0][0] == 0 and labels[-1][0] == 30
+    assert np.all(np.diff(x) > 0)
+    recip = 2 * np.pi * np.linalg.inv(cell).T
+    seg = [np.linalg.norm((np.array(pts[i + 1][1]) - np.array(pts[i][1])) @ recip) for i in range(2)]
+    n_seg = [labels[1][0] - labels[0][0], labels[2][0] - labels[1][0]]
+    assert abs(n_seg[0] / n_seg[1] - seg[0] / seg[1]) < 0.2
+    assert abs(x[-1] - sum(seg)) < 1e-12
+    with pytest.raises(ValueError):
+        k_path(cell, pts[:1], 10)
+    assert chunk_size(8, 24 ** 3) == 24
+    assert chunk_size(480, 96 ** 3) == 1
+    assert chunk_size(160, 72 ** 3) == int(1.5e9 / (160 * 72 ** 3 * 16))
