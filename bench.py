@@ -485,6 +485,40 @@ def run_tc(args):
     return 0
 
 
+def run_gamma(args):
+    """The Gamma real path on a Gamma-only cell: ``--warmup`` untimed and one
+    wall-timed ``davidson_gamma`` from the identity start on the lowest
+    half-sphere slots, to ``--tol``; eigenvalue error against the reference's
+    complex float64 golden eigenvalues."""
+    import torch
+    from gradwave_b200.cells import make_cell
+    from gradwave_b200.gamma import GammaHamiltonian, build_gamma_basis, davidson_gamma, gamma_start
+    dev = torch.device("cuda", 0)
+    ci = make_cell(args.config)
+    if ci.bk.nk != 1 or np.any(ci.kpoints != 0):
+        raise SystemExit(f"{args.config} is not a Gamma-only cell")
+    gb = build_gamma_basis(ci.spheres[0], ci.shape)
+    gh = GammaHamiltonian(gb, ci.v_eff_r, ci.p[0], ci.bk.dij_full, device=dev)
+    x0 = gamma_start(gb, ci.nbands, dev)
+    for _ in range(args.warmup):
+        davidson_gamma(gh, x0, tol=args.tol, max_iter=300)
+    torch.cuda.synchronize()
+    n0 = gh.n_apply
+    t0 = time.perf_counter()
+    r = davidson_gamma(gh, x0, tol=args.tol, max_iter=300)
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) * 1e3
+    out = {"mode": "gamma", "config": args.config, "tol_ev": args.tol, "n_iter": r.n_iter, "wall_ms": wall,
+           "band_applies": gh.n_apply - n0, "max_residual_ev": float(r.residual_norms.max()),
+           "nhalf": gb.nhalf, "npw": gb.npw}
+    gold = _golden(args.config)
+    if gold is not None:
+        err = float(np.abs(r.eigenvalues.cpu().numpy() - gold["eigenvalues"][0]).max())
+        out.update({"eig_err_ha": err / HA, "within_1e-8_ha": err <= EIG_TOL_EV})
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def _solver_choice(name, dev):
     """(mode, preconditioner) of a solver name: plain = float64 + TPA,
     fp32exp = the reference's float32-expansion mode + TPA, mixed = float32
@@ -513,7 +547,7 @@ def main():
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--tc-shape", default="4,160,640,37000", help="--mode tc: nk,n,m,npw")
-    ap.add_argument("--mode", default="solve", choices=["solve", "apply", "once", "tc"],
+    ap.add_argument("--mode", default="solve", choices=["solve", "apply", "once", "tc", "gamma"],
                     help="apply: only time Hamiltonian applies; once: a single solve (profiling)")
     ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64"], help="arithmetic of --mode apply")
     ap.add_argument("--solver", default="learned-mixed", choices=["plain", "fp32exp", "mixed", "learned-mixed"],
@@ -523,6 +557,8 @@ def main():
         return run_apply(args)
     if args.mode == "tc":
         return run_tc(args)
+    if args.mode == "gamma":
+        return run_gamma(args)
     if args.mode == "once":
         return run_once(args)
     if args.impl == "reference":

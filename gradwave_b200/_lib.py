@@ -85,6 +85,8 @@ _SIGNATURES = {
     "gwb_ham_scratch_bytes": [_P],
     "gwb_ham_tc_status": [_P, _P],
     "gwb_ham_density": [_P, _P, _I64, _I, _I, _P, _I64, _D, _P, _P],
+    "gwb_gamma_work_bytes": [_I, _I],
+    "gwb_gamma_apply": [_P, _I, _I, _I, _P, _I64, _P, _I64, _P, _P, _P, _P, _I, _P, _SZ, _P],
     "gwb_zgemm": [ctypes.c_int, ctypes.c_int, _I64, _I64, _I64, _D, _D, _P, _I64, _I64, _P, _I64, _I64,
                   _D, _D, _P, _I64, _I64, _I64, _P],
     "gwb_zgemm_nh": [_I64, _I64, _I64, _D, _D, _P, _I64, _I64, _P, _I64, _I64, _D, _D, _P, _I64, _I64, _I64, _P,
@@ -121,7 +123,8 @@ _SIGNATURES = {
 _RESTYPES = {"gwb_last_error": ctypes.c_char_p, "gwb_version": ctypes.c_char_p,
              "gwb_launch_count": ctypes.c_ulonglong,
              "gwb_ham_scratch_bytes": ctypes.c_size_t, "gwb_heev_scratch_doubles": ctypes.c_int64,
-             "gwb_precond_learned_work_bytes": ctypes.c_int64, "gwb_zgemm_tc_work_bytes": ctypes.c_int64}
+             "gwb_precond_learned_work_bytes": ctypes.c_int64, "gwb_zgemm_tc_work_bytes": ctypes.c_int64,
+             "gwb_gamma_work_bytes": ctypes.c_size_t}
 
 
 def declared_symbols() -> list[str]:

@@ -1,0 +1,304 @@
+"""Gamma-point real-wavefunction path on the B200 (drop-in for gradwave's
+``core/gamma.py``: ``build_gamma_basis``, ``GammaHamiltonian``,
+``davidson_gamma`` and the real embedding).
+
+At k = 0 the eigenstates can be taken real, c(-G) = conj(c(G)), so one member
+of each {G, -G} pair plus the real G = 0 coefficient carries the band. The
+half sphere is stored with G = 0 first and, for the others, the member whose
+Miller index is lexicographically positive in the order (m3, m2, m1) - the
+reference's layout, kept alike so half vectors pass between the two
+(``core/gamma.py:70-147``). The solver works in the real embedding
+phi = (Re c0, sqrt2 Re c1, sqrt2 Im c1, ...), where the full-sphere inner
+product is the plain dot product (``core/gamma.py:215-250``).
+
+What is B200-specific is the apply: ``gwb_gamma_apply`` packs two real bands
+into one complex row z = c_a + i c_b, runs the complex apply kernels on it
+(FFTs, V(r), kinetic, nonlocal) and unpacks both images through the G / -G
+symmetry. nb bands cost ceil(nb/2) complex rows: the halving of FFT work the
+reference gets from rfftn/irfftn, here without a separate real-FFT kernel,
+and the nonlocal term halves with it. The subspace algebra runs in real
+float64 (cuBLAS DGEMM, cuSOLVER symmetric eigensolver, Householder QR), as
+the reference's ``davidson_gamma`` runs the single-k ``davidson``
+(``solvers/davidson.py:330-395``) in the embedding.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from .constants import HBAR2_2M
+
+_R2 = 2.0 ** 0.5
+
+
+@dataclass
+class GammaBasis:
+    shape: tuple[int, int, int]
+    t_half: torch.Tensor         # (nhalf,) HBAR2_2M |G|^2 on the half sphere
+    metric_w: torch.Tensor       # (nhalf,) 1 at G = 0, else 2
+    full_flat_idx: torch.Tensor  # (npw,) sphere -> box flat index
+    rep_full_idx: torch.Tensor   # (nhalf,) half slot -> full-sphere index
+    src_half: torch.Tensor       # (npw,) full-sphere point -> its half slot
+    conj_full: torch.Tensor      # (npw,) bool: the point is the conjugate of its representative
+    partner_rep: torch.Tensor    # (nhalf,) full-sphere index of -G of each representative
+    t_full: torch.Tensor         # (npw,) kinetic on the full sphere
+
+    @property
+    def nhalf(self) -> int:
+        return int(self.t_half.shape[0])
+
+    @property
+    def npw(self) -> int:
+        return int(self.src_half.shape[0])
+
+
+def build_gamma_basis(sphere, shape, device=None) -> GammaBasis:
+    """Half-sphere maps of a k = 0 sphere (``basis.GSphere``: ``miller``,
+    ``kpg2``, ``flat_idx``). Raises when the sphere is not closed under
+    G -> -G (k is not Gamma)."""
+    n1, n2, n3 = (int(s) for s in shape)
+    miller = np.asarray(sphere.miller, dtype=np.int64)
+    npw = miller.shape[0]
+    dev = torch.device("cpu") if device is None else torch.device(device)
+
+    def flat(m):
+        return ((m[:, 0] % n1) * n2 + (m[:, 1] % n2)) * n3 + (m[:, 2] % n3)
+
+    where = np.full(n1 * n2 * n3, -1, dtype=np.int64)
+    where[flat(miller)] = np.arange(npw)
+    partner = where[flat(-miller)]
+    if np.any(partner < 0):
+        raise ValueError("the Gamma path needs a sphere closed under G -> -G (k must be Gamma)")
+    zero = np.all(miller == 0, axis=1)
+    if int(zero.sum()) != 1:
+        raise ValueError("a Gamma sphere holds exactly one G = 0")
+    m1, m2, m3 = miller[:, 0], miller[:, 1], miller[:, 2]
+    positive = (m3 > 0) | ((m3 == 0) & (m2 > 0)) | ((m3 == 0) & (m2 == 0) & (m1 > 0))
+    rep = np.concatenate([np.flatnonzero(zero), np.flatnonzero(positive)])
+    nhalf = rep.shape[0]
+    if 2 * nhalf - 1 != npw:
+        raise ValueError(f"half sphere of {nhalf} does not pair up {npw} points")
+    slot = np.full(npw, -1, dtype=np.int64)
+    slot[rep] = np.arange(nhalf)
+    is_rep = zero | positive
+    src = np.where(is_rep, slot, slot[partner])
+    kin = HBAR2_2M * np.asarray(sphere.kpg2, dtype=np.float64)
+    w = np.full(nhalf, 2.0)
+    w[0] = 1.0
+
+    def t(a, dt):
+        return torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
+
+    return GammaBasis(shape=(n1, n2, n3), t_half=t(kin[rep], torch.float64), metric_w=t(w, torch.float64),
+                      full_flat_idx=t(np.asarray(sphere.flat_idx), torch.int64), rep_full_idx=t(rep, torch.int64),
+                      src_half=t(src, torch.int64), conj_full=t(~is_rep, torch.bool),
+                      partner_rep=t(partner[rep], torch.int64), t_full=t(kin, torch.float64))
+
+
+def half_to_full(gb: GammaBasis, chalf: torch.Tensor) -> torch.Tensor:
+    """(nb, nhalf) -> (nb, npw) Hermitian-symmetric full sphere."""
+    c = chalf[:, gb.src_half.to(chalf.device)]
+    return torch.where(gb.conj_full.to(chalf.device)[None, :], c.conj(), c)
+
+
+def full_to_half(gb: GammaBasis, cfull: torch.Tensor) -> torch.Tensor:
+    """(nb, npw) -> (nb, nhalf); lossless for a Hermitian-symmetric row."""
+    return cfull[:, gb.rep_full_idx.to(cfull.device)]
+
+
+def metric_inner(gb: GammaBasis, a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
+    """Real Gram <a_m|b_n> = Re[a0* b0] + 2 sum_{G>0} Re[a* b] (nb, nb)."""
+    return torch.einsum("mp,np->mn", a.conj(), gb.metric_w.to(b.device) * b).real
+
+
+def embed_real(gb: GammaBasis, chalf: torch.Tensor) -> torch.Tensor:
+    """(nb, nhalf) complex -> (nb, 2 nhalf - 1) real, dot product = metric."""
+    nb = chalf.shape[0]
+    phi = torch.empty(nb, 2 * gb.nhalf - 1, dtype=torch.float64, device=chalf.device)
+    phi[:, 0] = chalf[:, 0].real
+    phi[:, 1::2] = _R2 * chalf[:, 1:].real
+    phi[:, 2::2] = _R2 * chalf[:, 1:].imag
+    return phi
+
+
+def unembed_real(gb: GammaBasis, phi: torch.Tensor) -> torch.Tensor:
+    """Inverse of ``embed_real``."""
+    nb = phi.shape[0]
+    c = torch.empty(nb, gb.nhalf, dtype=torch.complex128, device=phi.device)
+    c[:, 0] = phi[:, 0].to(torch.complex128)
+    c[:, 1:] = torch.complex(phi[:, 1::2], phi[:, 2::2]) / _R2
+    return c
+
+
+def kinetic_phi(gb: GammaBasis) -> torch.Tensor:
+    """The kinetic diagonal in the embedding (2 nhalf - 1,)."""
+    t = torch.empty(2 * gb.nhalf - 1, dtype=torch.float64, device=gb.t_half.device)
+    t[0] = gb.t_half[0]
+    t[1::2] = gb.t_half[1:]
+    t[2::2] = gb.t_half[1:]
+    return t
+
+
+class GammaHamiltonian:
+    """H at Gamma on the half sphere (``core/gamma.py:161-203``):
+    ``GammaHamiltonian(gb, v_eff_r, p, dij).apply(chalf)``, p the full-sphere
+    projectors (nproj, npw). ``apply_phi`` is the same operator in the real
+    embedding (what the solver uses), ``prec`` float64 or float32
+    arithmetic."""
+
+    def __init__(self, gb: GammaBasis, v_eff_r, p, dij, device=None):
+        dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+        self.gb, self.device, self.shape = gb, dev, gb.shape
+        npw, nhalf = gb.npw, gb.nhalf
+        p = torch.as_tensor(p).to(dev, torch.complex128).reshape(1, -1, npw).contiguous()
+        self.nproj = int(p.shape[1])
+        flat = np.ascontiguousarray(gb.full_flat_idx.cpu().numpy().astype(np.int64))
+        npw_arr = np.array([npw], dtype=np.int64)
+        geom = _lib.Geometry()
+        geom.nk, geom.npw_max, geom.nproj = 1, npw, self.nproj
+        for a in range(3):
+            geom.n[a] = int(gb.shape[a])
+        geom.npw = npw_arr.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+        geom.flat_idx = flat.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+        h = ctypes.c_void_p()
+        _lib.call("gwb_ham_create", ctypes.byref(geom), int(dev.index or 0), ctypes.byref(h))
+        self._h = h
+        self.t = gb.t_full.to(dev).reshape(1, npw).contiguous()
+        self.v = torch.as_tensor(v_eff_r).to(dev, torch.float64).contiguous()
+        self.p = p
+        self.dij = torch.as_tensor(dij).to(dev, torch.float64).contiguous()
+        with torch.cuda.device(dev):
+            s = _lib.stream_ptr(dev)
+            _lib.call("gwb_ham_set_kinetic", self._h, self.t.data_ptr(), s)
+            _lib.call("gwb_ham_set_potential", self._h, self.v.data_ptr(), s)
+            _lib.call("gwb_ham_set_projectors", self._h, self.p.data_ptr() if self.nproj else None,
+                      self.dij.data_ptr() if self.nproj else None, s)
+        i32 = dict(dtype=torch.int32, device=dev)
+        self.src_half = gb.src_half.to(**i32).contiguous()
+        self.conj_full = gb.conj_full.to(dev, torch.uint8).contiguous()
+        self.rep_full = gb.rep_full_idx.to(**i32).contiguous()
+        self.partner_rep = gb.partner_rep.to(**i32).contiguous()
+        self.t_phi = kinetic_phi(gb).to(dev)
+        self._work = None
+        self.n_apply = 0
+        assert nhalf * 2 - 1 == npw
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                torch.cuda.synchronize(self.device)
+                _lib.load().gwb_ham_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def apply_phi(self, phi: torch.Tensor, prec: int = _lib.GWB_FP64) -> torch.Tensor:
+        """H on real embedded rows (nb, 2 nhalf - 1) float64 -> same shape."""
+        _lib.require_cuda(phi, "phi")
+        nb = int(phi.shape[0])
+        out = torch.empty_like(phi)
+        if nb == 0:
+            return out
+        phi = phi.contiguous()
+        need = int(_lib.load().gwb_gamma_work_bytes(nb, self.gb.npw))
+        if self._work is None or self._work.numel() < need:
+            self._work = torch.empty(need, dtype=torch.uint8, device=self.device)
+        _lib.call("gwb_gamma_apply", self._h, nb, self.gb.nhalf, self.gb.npw, phi.data_ptr(), phi.shape[1],
+                  out.data_ptr(), out.shape[1], self.src_half.data_ptr(), self.conj_full.data_ptr(),
+                  self.rep_full.data_ptr(), self.partner_rep.data_ptr(), prec, self._work.data_ptr(),
+                  self._work.numel(), _lib.stream_ptr(self.device))
+        self.n_apply += nb
+        return out
+
+    def apply(self, chalf: torch.Tensor) -> torch.Tensor:
+        """H on half-sphere rows (nb, nhalf) complex -> (nb, nhalf)."""
+        return unembed_real(self.gb, self.apply_phi(embed_real(self.gb, chalf.to(self.device))))
+
+
+@dataclass
+class GammaDavidsonResult:
+    eigenvalues: torch.Tensor   # (nb,) ascending [eV]
+    eigenvectors: torch.Tensor  # (nb, nhalf) metric-orthonormal half-sphere rows
+    n_iter: int
+    residual_norms: torch.Tensor  # (nb,)
+
+
+def _orthonormalize(v: torch.Tensor, against: torch.Tensor | None = None) -> torch.Tensor:
+    """Two projection passes against ``against``, Householder QR of the rows,
+    rows with |R_ii| <= 1e-10 dropped (gradwave ``solvers/davidson.py:319-326``)."""
+    if against is not None and against.shape[0]:
+        v = v - (v @ against.T) @ against
+        v = v - (v @ against.T) @ against
+    q, r = torch.linalg.qr(v.T, mode="reduced")
+    keep = r.diagonal().abs() > 1e-10
+    return q.T[keep]
+
+
+def _teter(residual: torch.Tensor, t_g: torch.Tensor, t_band: torch.Tensor) -> torch.Tensor:
+    """TPA filter (gradwave ``solvers/precond.py:8-18``)."""
+    x = t_g[None, :] / torch.clamp(t_band[:, None], min=1e-12)
+    x2 = x * x
+    num = 27.0 + 18.0 * x + 12.0 * x2 + 8.0 * x2 * x
+    return residual * (num / (num + 16.0 * x2 * x2))
+
+
+@torch.no_grad()
+def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, max_iter: int = 40,
+                   max_dim_factor: int = 4) -> GammaDavidsonResult:
+    """Real-symmetric block Davidson on the half sphere
+    (``core/gamma.py:261-290``): the single-k Davidson of the reference
+    (``solvers/davidson.py:330-395``: Rayleigh-Ritz on the whole subspace,
+    TPA on every unconverged residual, QR orthonormalisation with rank
+    reveal, restart to [Ritz block, new directions] with a fresh apply) in the
+    real embedding, every step on the device."""
+    gb, dev = ham.gb, ham.device
+    phi0 = embed_real(gb, x0.to(dev, torch.complex128))
+    nb, nphi = phi0.shape
+    max_dim = min(max_dim_factor * nb, nphi)
+    t_phi = ham.t_phi
+    v = _orthonormalize(phi0.clone())
+    if v.shape[0] < nb:  # degenerate start: pad with seeded noise (``:345-350``)
+        gen = torch.Generator(device="cpu").manual_seed(1234)
+        pad = torch.randn(nb - v.shape[0], nphi, generator=gen, dtype=torch.float64).to(dev)
+        v = torch.cat([v, _orthonormalize(pad, against=v)])
+    hv = ham.apply_phi(v)
+    eig = torch.zeros(nb, dtype=torch.float64, device=dev)
+    x = v[:nb]
+    rn = torch.full((nb,), float("inf"), dtype=torch.float64, device=dev)
+    for it in range(1, max_iter + 1):
+        s = v @ hv.T
+        s = 0.5 * (s + s.T)
+        w, u = torch.linalg.eigh(s)
+        eig = w[:nb]
+        x = u[:, :nb].T @ v
+        hx = u[:, :nb].T @ hv
+        r = hx - eig[:, None] * x
+        rn = torch.linalg.vector_norm(r, dim=1)
+        unconv = rn > tol
+        if not bool(unconv.any()):
+            return GammaDavidsonResult(eig, unembed_real(gb, x), it, rn)
+        t_band = (x * x * t_phi[None, :]).sum(dim=1)
+        t = _orthonormalize(_teter(r[unconv], t_phi, t_band[unconv]), against=v)
+        if t.shape[0] == 0:
+            return GammaDavidsonResult(eig, unembed_real(gb, x), it, rn)
+        if v.shape[0] + t.shape[0] > max_dim:
+            v = _orthonormalize(torch.cat([x, t]))
+            hv = ham.apply_phi(v)
+        else:
+            v = torch.cat([v, t])
+            hv = torch.cat([hv, ham.apply_phi(t)])
+    return GammaDavidsonResult(eig, unembed_real(gb, x), max_iter, rn)
+
+
+def gamma_start(gb: GammaBasis, nb: int, device=None) -> torch.Tensor:
+    """Identity start on the lowest-|G|^2 half-sphere slots (the
+    ``scf/loop.py:705-706`` cold start restricted to real states)."""
+    x0 = torch.zeros(nb, gb.nhalf, dtype=torch.complex128, device=device)
+    x0[torch.arange(nb), torch.arange(nb)] = 1.0
+    return x0

@@ -120,6 +120,27 @@ int gwb_ham_apply_strided(gwb_ham* h, const void* c, int64_t c_kstride, void* ou
 int gwb_ham_density(gwb_ham* h, const void* c, int64_t c_kstride, int32_t nb, int32_t io_dtype,
                     const double* weights, int64_t w_kstride, double scale, double* rho, void* stream);
 
+/* Gamma point in the real embedding of the half sphere (replaces gradwave
+ * core/gamma.py:161-250, GammaHamiltonian.apply composed with embed_real and
+ * unembed_real). The handle is a k = 0 operator on the full sphere (nk = 1,
+ * npw_max = npw = 2 nhalf - 1, no padding). phi and out are nb rows of
+ * 2 nhalf - 1 float64 (row strides ldphi, ldout): phi = (Re c(0),
+ * sqrt2 Re c(G1), sqrt2 Im c(G1), ...) over the representatives G0 = 0, G1, ...
+ * Index tables (device int32 / uint8, from the reference's half-sphere maps):
+ *   src_half[g]    half slot of full-sphere point g (its representative)
+ *   conj_full[g]   1 where c(g) is the conjugate of its representative
+ *   rep_full[j]    full-sphere index of representative j
+ *   partner_rep[j] full-sphere index of -G_j (j = 0: itself)
+ * Two real bands run as one complex row of the apply (z = c_a + i c_b),
+ * unpacked by the G / -G symmetry: half the FFT and nonlocal work per band.
+ * prec: GWB_FP64 or GWB_FP32 arithmetic of the apply. work: at least
+ * gwb_gamma_work_bytes(nb, npw) bytes of device memory. */
+size_t gwb_gamma_work_bytes(int32_t nb, int32_t npw);
+int gwb_gamma_apply(gwb_ham* h, int32_t nb, int32_t nhalf, int32_t npw, const double* phi, int64_t ldphi,
+                    double* out, int64_t ldout, const int32_t* src_half, const uint8_t* conj_full,
+                    const int32_t* rep_full, const int32_t* partner_rep, int32_t prec, void* work,
+                    size_t work_bytes, void* stream);
+
 /* Bytes of handle-owned device scratch currently held. */
 size_t gwb_ham_scratch_bytes(const gwb_ham* h);
 

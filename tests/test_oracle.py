@@ -118,3 +118,29 @@ def test_oracle_density_matches_reference(name):
     assert np.abs(chk - g["rho_chk"]).max() / np.abs(g["rho_chk"]).max() < 1e-12
     if "rho" in g:
         assert np.abs(rho - g["rho"]).max() / np.abs(g["rho"]).max() < 1e-12
+
+
+@pytest.mark.parametrize("name", ["si2_fcc", "si216_vacancy"])
+def test_gamma_basis_and_oracle_apply_match_reference(name):
+    """The half-sphere layout built here equals the reference's
+    (``core/gamma.py:70-147``), and the oracle Gamma apply reproduces the
+    reference's ``GammaHamiltonian.apply`` on the same seeded half block."""
+    from gradwave_b200.cells import make_cell
+    from gradwave_b200.gamma import build_gamma_basis
+    from oracle.gamma import gamma_apply
+    from oracle.ham import from_cell
+    g = load_golden(f"gamma_{name}")
+    ci = make_cell(name)
+    gb = build_gamma_basis(ci.spheres[0], ci.shape)
+    assert np.array_equal(gb.rep_full_idx.numpy(), g["rep_full_idx"])
+    assert gb.npw == 2 * gb.nhalf - 1
+    full = gb.src_half.numpy()
+    assert np.array_equal(full[gb.rep_full_idx.numpy()], np.arange(gb.nhalf))
+    if name != "si2_fcc":
+        return  # the 96^3 apply is checked on the GPU
+    rng = np.random.default_rng(int(g["seed"]))
+    nb = int(g["nb_apply"])
+    ch = rng.standard_normal((nb, gb.nhalf)) + 1j * rng.standard_normal((nb, gb.nhalf))
+    ch[:, 0] = ch[:, 0].real
+    out = gamma_apply(from_cell(ci), gb.src_half.numpy(), gb.conj_full.numpy(), gb.rep_full_idx.numpy(), ch)
+    assert np.abs(out - g["apply_out"]).max() / np.abs(g["apply_out"]).max() < 1e-12
