@@ -511,6 +511,8 @@ def run_gamma(args):
     out = {"mode": "gamma", "config": args.config, "tol_ev": args.tol, "n_iter": r.n_iter, "wall_ms": wall,
            "band_applies": gh.n_apply - n0, "max_residual_ev": float(r.residual_norms.max()),
            "nhalf": gb.nhalf, "npw": gb.npw}
+    if r.phase_ms:
+        out["phase_ms"] = r.phase_ms
     gold = _golden(args.config)
     if gold is not None:
         err = float(np.abs(r.eigenvalues.cpu().numpy() - gold["eigenvalues"][0]).max())

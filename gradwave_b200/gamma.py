@@ -227,6 +227,7 @@ class GammaDavidsonResult:
     eigenvectors: torch.Tensor  # (nb, nhalf) metric-orthonormal half-sphere rows
     n_iter: int
     residual_norms: torch.Tensor  # (nb,)
+    phase_ms: dict | None = None  # CUDA-event times per step (GWB_PROFILE=1)
 
 
 def _orthonormalize(v: torch.Tensor, against: torch.Tensor | None = None) -> torch.Tensor:
@@ -238,6 +239,31 @@ def _orthonormalize(v: torch.Tensor, against: torch.Tensor | None = None) -> tor
     q, r = torch.linalg.qr(v.T, mode="reduced")
     keep = r.diagonal().abs() > 1e-10
     return q.T[keep]
+
+
+def _expand(t: torch.Tensor, v: torch.Tensor) -> torch.Tensor:
+    """New directions from preconditioned residuals: unit rows, two
+    projections against the orthonormal basis v, Householder QR dropping rows
+    that kept less than 1e-8 of their norm, then one more projection and QR so
+    that the kept rows are orthogonal to v at float64 round-off.
+
+    The reference's single-k Davidson orthonormalises the raw preconditioned
+    residuals with an absolute 1e-10 rank threshold (``solvers/davidson.py:
+    319-326,383``); their norm is of the order of the tolerance itself, so
+    below ~1e-8 eV rows of round-off survive, the basis loses orthogonality and
+    the solve stalls or diverges (on si216 at 1e-9 eV: residual 2e-2 after 300
+    rounds). Unit rows and a relative threshold, as the batched Davidson does
+    (``:406-457``), remove that floor."""
+    t = t / torch.linalg.vector_norm(t, dim=1, keepdim=True).clamp_min(1e-300)
+    t = t - (t @ v.T) @ v
+    t = t - (t @ v.T) @ v
+    q, r = torch.linalg.qr(t.T, mode="reduced")
+    t = q.T[r.diagonal().abs() > 1e-8]
+    if t.shape[0] == 0:
+        return t
+    t = t - (t @ v.T) @ v
+    q, _ = torch.linalg.qr(t.T, mode="reduced")
+    return q.T
 
 
 def _teter(residual: torch.Tensor, t_g: torch.Tensor, t_band: torch.Tensor) -> torch.Tensor:
@@ -254,9 +280,16 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
     """Real-symmetric block Davidson on the half sphere
     (``core/gamma.py:261-290``): the single-k Davidson of the reference
     (``solvers/davidson.py:330-395``: Rayleigh-Ritz on the whole subspace,
-    TPA on every unconverged residual, QR orthonormalisation with rank
-    reveal, restart to [Ritz block, new directions] with a fresh apply) in the
-    real embedding, every step on the device."""
+    TPA on every unconverged residual, restart to [Ritz block, new
+    directions]) in the real embedding, every step on the device. Two rules
+    follow the reference's batched Davidson instead of its single-k one: the
+    new directions are unit-normalised and rank-checked relative to their norm
+    (``_expand``), and a restart keeps the Ritz block's images HX rather than
+    applying H again (``solvers/davidson.py:745-759``), since [X, T] is
+    already orthonormal with X = U^T V and HX = U^T HV."""
+    import os
+    from .davidson import _PhaseTimer
+    prof = _PhaseTimer(os.environ.get("GWB_PROFILE", "0") == "1")
     gb, dev = ham.gb, ham.device
     phi0 = embed_real(gb, x0.to(dev, torch.complex128))
     nb, nphi = phi0.shape
@@ -272,28 +305,37 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
     x = v[:nb]
     rn = torch.full((nb,), float("inf"), dtype=torch.float64, device=dev)
     for it in range(1, max_iter + 1):
-        s = v @ hv.T
-        s = 0.5 * (s + s.T)
-        w, u = torch.linalg.eigh(s)
+        with prof("subspace_gemm"):
+            s = v @ hv.T
+            s = 0.5 * (s + s.T)
+        with prof("eigh"):
+            w, u = torch.linalg.eigh(s)
         eig = w[:nb]
-        x = u[:, :nb].T @ v
-        hx = u[:, :nb].T @ hv
-        r = hx - eig[:, None] * x
-        rn = torch.linalg.vector_norm(r, dim=1)
-        unconv = rn > tol
-        if not bool(unconv.any()):
-            return GammaDavidsonResult(eig, unembed_real(gb, x), it, rn)
-        t_band = (x * x * t_phi[None, :]).sum(dim=1)
-        t = _orthonormalize(_teter(r[unconv], t_phi, t_band[unconv]), against=v)
+        with prof("ritz_gemm"):
+            x = u[:, :nb].T @ v
+            hx = u[:, :nb].T @ hv
+        with prof("residual"):
+            r = hx - eig[:, None] * x
+            rn = torch.linalg.vector_norm(r, dim=1)
+            unconv = rn > tol
+            done = not bool(unconv.any())
+        if done:
+            return GammaDavidsonResult(eig, unembed_real(gb, x), it, rn, prof.summary())
+        with prof("orthonormalize"):
+            t_band = (x * x * t_phi[None, :]).sum(dim=1)
+            t = _expand(_teter(r[unconv], t_phi, t_band[unconv]), v)
         if t.shape[0] == 0:
-            return GammaDavidsonResult(eig, unembed_real(gb, x), it, rn)
+            return GammaDavidsonResult(eig, unembed_real(gb, x), it, rn, prof.summary())
+        with prof("apply"):
+            ht = ham.apply_phi(t)
         if v.shape[0] + t.shape[0] > max_dim:
-            v = _orthonormalize(torch.cat([x, t]))
-            hv = ham.apply_phi(v)
+            # the Ritz block spans what v keeps; t is orthogonal to all of v
+            v = torch.cat([x, t])
+            hv = torch.cat([hx, ht])
         else:
             v = torch.cat([v, t])
-            hv = torch.cat([hv, ham.apply_phi(t)])
-    return GammaDavidsonResult(eig, unembed_real(gb, x), max_iter, rn)
+            hv = torch.cat([hv, ht])
+    return GammaDavidsonResult(eig, unembed_real(gb, x), max_iter, rn, prof.summary())
 
 
 def gamma_start(gb: GammaBasis, nb: int, device=None) -> torch.Tensor:
