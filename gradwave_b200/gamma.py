@@ -202,10 +202,10 @@ class GammaHamiltonian:
         """H on real embedded rows (nb, 2 nhalf - 1) float64 -> same shape."""
         _lib.require_cuda(phi, "phi")
         nb = int(phi.shape[0])
-        out = torch.empty_like(phi)
+        phi = phi.contiguous()  # row-major rows for the kernels (solver blocks may come transposed)
+        out = torch.empty(phi.shape, dtype=torch.float64, device=phi.device)
         if nb == 0:
             return out
-        phi = phi.contiguous()
         need = int(_lib.load().gwb_gamma_work_bytes(nb, self.gb.npw))
         if self._work is None or self._work.numel() < need:
             self._work = torch.empty(need, dtype=torch.uint8, device=self.device)
@@ -257,6 +257,19 @@ def _expand(t: torch.Tensor, v: torch.Tensor) -> torch.Tensor:
     t = t / torch.linalg.vector_norm(t, dim=1, keepdim=True).clamp_min(1e-300)
     t = t - (t @ v.T) @ v
     t = t - (t @ v.T) @ v
+    # Cholesky-QR twice (float64 Gram, Cholesky, triangular solve: GEMM-rich)
+    # when every row keeps more than 1e-8 of its unit norm; else the
+    # Householder path below, which drops the dependent rows
+    ok = True
+    y = t
+    for _ in range(2):
+        L, info = torch.linalg.cholesky_ex(y @ y.T)
+        if int(info.max()) != 0 or float(torch.diagonal(L).min()) <= 1e-8:
+            ok = False
+            break
+        y = torch.linalg.solve_triangular(L, y, upper=False)
+    if ok:
+        return y
     q, r = torch.linalg.qr(t.T, mode="reduced")
     t = q.T[r.diagonal().abs() > 1e-8]
     if t.shape[0] == 0:
@@ -304,10 +317,18 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
     eig = torch.zeros(nb, dtype=torch.float64, device=dev)
     x = v[:nb]
     rn = torch.full((nb,), float("inf"), dtype=torch.float64, device=dev)
+    # the subspace matrix grows by the new columns only (m0: rows already in it)
+    S = torch.zeros(max_dim, max_dim, dtype=torch.float64, device=dev)
+    m0 = 0
     for it in range(1, max_iter + 1):
         with prof("subspace_gemm"):
-            s = v @ hv.T
-            s = 0.5 * (s + s.T)
+            m = v.shape[0]
+            blk = v @ hv[m0:m].T                       # (m, m - m0)
+            S[:m, m0:m] = blk
+            S[m0:m, :m0] = blk[:m0].T
+            S[m0:m, m0:m] = 0.5 * (blk[m0:] + blk[m0:].T)
+            m0 = m
+            s = S[:m, :m]
         with prof("eigh"):
             w, u = torch.linalg.eigh(s)
         eig = w[:nb]
@@ -332,6 +353,7 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
             # the Ritz block spans what v keeps; t is orthogonal to all of v
             v = torch.cat([x, t])
             hv = torch.cat([hx, ht])
+            m0 = 0
         else:
             v = torch.cat([v, t])
             hv = torch.cat([hv, ht])

@@ -81,3 +81,13 @@ def test_gamma_davidson_si216_matches_complex_reference(cuda_device):
     eig = res.eigenvalues.cpu().numpy()
     assert float(res.residual_norms.max()) < 1e-6
     assert np.abs(eig - gc["eigenvalues"][0]).max() < 1e-8 * HA
+
+
+def test_gamma_apply_accepts_transposed_blocks(cuda_device):
+    """Solver blocks can come out of a triangular solve with transposed
+    strides; the apply reads and writes row-major whatever the input layout."""
+    ci, gb, gh = _gamma("si2_fcc", cuda_device)
+    g = torch.Generator(device="cpu").manual_seed(3)
+    phi = torch.randn(2 * gb.nhalf - 1, 6, generator=g, dtype=torch.float64).to(cuda_device).T
+    assert not phi.is_contiguous()
+    assert torch.equal(gh.apply_phi(phi), gh.apply_phi(phi.contiguous()))
