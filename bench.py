@@ -500,15 +500,17 @@ def run_gamma(args):
     gb = build_gamma_basis(ci.spheres[0], ci.shape)
     gh = GammaHamiltonian(gb, ci.v_eff_r, ci.p[0], ci.bk.dij_full, device=dev)
     x0 = gamma_start(gb, ci.nbands, dev)
+    mode = "mixed" if args.solver in ("mixed", "fp32exp", "learned-mixed") else "fp64"
     for _ in range(args.warmup):
-        davidson_gamma(gh, x0, tol=args.tol, max_iter=300)
+        davidson_gamma(gh, x0, tol=args.tol, max_iter=300, mode=mode)
     torch.cuda.synchronize()
     n0 = gh.n_apply
     t0 = time.perf_counter()
-    r = davidson_gamma(gh, x0, tol=args.tol, max_iter=300)
+    r = davidson_gamma(gh, x0, tol=args.tol, max_iter=300, mode=mode)
     torch.cuda.synchronize()
     wall = (time.perf_counter() - t0) * 1e3
-    out = {"mode": "gamma", "config": args.config, "tol_ev": args.tol, "n_iter": r.n_iter, "wall_ms": wall,
+    out = {"mode": "gamma", "config": args.config, "solver": mode, "tol_ev": args.tol, "n_iter": r.n_iter,
+           "wall_ms": wall,
            "band_applies": gh.n_apply - n0, "max_residual_ev": float(r.residual_norms.max()),
            "nhalf": gb.nhalf, "npw": gb.npw}
     if r.phase_ms:

@@ -289,7 +289,7 @@ def _teter(residual: torch.Tensor, t_g: torch.Tensor, t_band: torch.Tensor) -> t
 
 @torch.no_grad()
 def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, max_iter: int = 40,
-                   max_dim_factor: int = 4) -> GammaDavidsonResult:
+                   max_dim_factor: int = 4, mode: str = "fp64") -> GammaDavidsonResult:
     """Real-symmetric block Davidson on the half sphere
     (``core/gamma.py:261-290``): the single-k Davidson of the reference
     (``solvers/davidson.py:330-395``: Rayleigh-Ritz on the whole subspace,
@@ -299,7 +299,18 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
     new directions are unit-normalised and rank-checked relative to their norm
     (``_expand``), and a restart keeps the Ritz block's images HX rather than
     applying H again (``solvers/davidson.py:745-759``), since [X, T] is
-    already orthonormal with X = U^T V and HX = U^T HV."""
+    already orthonormal with X = U^T V and HX = U^T HV.
+
+    ``mode="mixed"``: the expansion applies run in float32 arithmetic until
+    the largest residual reaches the float32 floor (32 eps_f32 max T) or stalls
+    within 100x of it; then the Ritz block is certified with a float64 apply and
+    a float64 nb x nb Rayleigh-Ritz, and unless that meets ``tol`` the basis
+    collapses to the certified block and the solve continues in float64 (the
+    complex path's mixed rule, ``davidson.py``; gradwave
+    ``solvers/davidson.py:226-308``). Every convergence decision is made on
+    float64 residuals."""
+    if mode not in ("fp64", "mixed"):
+        raise ValueError(f"mode must be 'fp64' or 'mixed', got {mode!r}")
     import os
     from .davidson import _PhaseTimer
     prof = _PhaseTimer(os.environ.get("GWB_PROFILE", "0") == "1")
@@ -313,7 +324,11 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
         gen = torch.Generator(device="cpu").manual_seed(1234)
         pad = torch.randn(nb - v.shape[0], nphi, generator=gen, dtype=torch.float64).to(dev)
         v = torch.cat([v, _orthonormalize(pad, against=v)])
-    hv = ham.apply_phi(v)
+    low = mode == "mixed"
+    f32, f64 = _lib.GWB_FP32, _lib.GWB_FP64
+    cert_floor = 32.0 * float(torch.finfo(torch.float32).eps) * max(float(t_phi.max()), 1.0)
+    prev = float("inf")
+    hv = ham.apply_phi(v, prec=f32 if low else f64)
     eig = torch.zeros(nb, dtype=torch.float64, device=dev)
     x = v[:nb]
     rn = torch.full((nb,), float("inf"), dtype=torch.float64, device=dev)
@@ -338,8 +353,25 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
         with prof("residual"):
             r = hx - eig[:, None] * x
             rn = torch.linalg.vector_norm(r, dim=1)
+            rmax = float(rn.max())
+        if low:
+            stalled = it > 1 and rmax > 0.7 * prev and rmax < 100.0 * cert_floor
+            prev = rmax
+            if rmax < max(tol, cert_floor) or stalled:
+                with prof("certify"):
+                    hx = ham.apply_phi(x, prec=f64)
+                    g = x @ hx.T
+                    w2, u2 = torch.linalg.eigh(0.5 * (g + g.T))
+                    x, hx, eig = u2.T @ x, u2.T @ hx, w2
+                    r = hx - eig[:, None] * x
+                    rn = torch.linalg.vector_norm(r, dim=1)
+                    rmax = float(rn.max())
+                if rmax >= tol:  # hand-off: float64 from the certified block on
+                    low = False
+                    v, hv, m0 = x, hx, 0
+        with prof("residual"):
             unconv = rn > tol
-            done = not bool(unconv.any())
+            done = rmax <= tol and not bool(unconv.any())
         if done:
             return GammaDavidsonResult(eig, unembed_real(gb, x), it, rn, prof.summary())
         with prof("orthonormalize"):
@@ -348,7 +380,7 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
         if t.shape[0] == 0:
             return GammaDavidsonResult(eig, unembed_real(gb, x), it, rn, prof.summary())
         with prof("apply"):
-            ht = ham.apply_phi(t)
+            ht = ham.apply_phi(t, prec=f32 if low else f64)
         if v.shape[0] + t.shape[0] > max_dim:
             # the Ritz block spans what v keeps; t is orthogonal to all of v
             v = torch.cat([x, t])
@@ -357,6 +389,12 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
         else:
             v = torch.cat([v, t])
             hv = torch.cat([hv, ht])
+    if low:  # out of rounds in float32: certify what there is
+        hx = ham.apply_phi(x, prec=f64)
+        g = x @ hx.T
+        w2, u2 = torch.linalg.eigh(0.5 * (g + g.T))
+        x, eig = u2.T @ x, w2
+        rn = torch.linalg.vector_norm(u2.T @ hx - eig[:, None] * x, dim=1)
     return GammaDavidsonResult(eig, unembed_real(gb, x), max_iter, rn, prof.summary())
 
 

@@ -170,7 +170,8 @@ def test_gamma_davidson_algebra_on_cpu():
 
     h = _Ham()
     h.gb, h.t_phi = gb, G.kinetic_phi(gb)
-    res = G.davidson_gamma(h, G.gamma_start(gb, ci.nbands), tol=1e-10, max_iter=100)
     g = load_golden("si2_fcc")
-    assert float(res.residual_norms.max()) < 1e-10
-    assert np.abs(res.eigenvalues.numpy() - g["eigenvalues"][0]).max() < 1e-9
+    for mode in ("fp64", "mixed"):
+        res = G.davidson_gamma(h, G.gamma_start(gb, ci.nbands), tol=1e-10, max_iter=100, mode=mode)
+        assert float(res.residual_norms.max()) < 1e-10
+        assert np.abs(res.eigenvalues.numpy() - g["eigenvalues"][0]).max() < 1e-9
