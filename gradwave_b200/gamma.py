@@ -213,6 +213,9 @@ class GammaHamiltonian:
                   out.data_ptr(), out.shape[1], self.src_half.data_ptr(), self.conj_full.data_ptr(),
                   self.rep_full.data_ptr(), self.partner_rep.data_ptr(), prec, self._work.data_ptr(),
                   self._work.numel(), _lib.stream_ptr(self.device))
+        nphi = 2 * self.gb.nhalf - 1
+        if out.shape[1] > nphi:  # padded rows (the solver's even width) keep their pad at zero
+            out[:, nphi:] = 0.0
         self.n_apply += nb
         return out
 
@@ -241,7 +244,49 @@ def _orthonormalize(v: torch.Tensor, against: torch.Tensor | None = None) -> tor
     return q.T[keep]
 
 
-def _expand(t: torch.Tensor, v: torch.Tensor) -> torch.Tensor:
+class _TcProjection:
+    """First projection pass of the expansion block on the tensor cores, for
+    the mixed schedule. The solver keeps its real rows at an even width, so a
+    row is also a complex row of half the length, and for such rows
+    Re(A B^H) is exactly the real product A B^T: the split-BF16 complex
+    kernels (``gradwave_b200.tc``) then compute the coefficients D V^T and the
+    update D -= C V (C real, imaginary part zero). The BF16 planes of the
+    basis are kept current row block by row block. A row that keeps less than
+    1e-2 of its unit norm would be dominated by the products' ~1e-6 error, so
+    then the block is redone in float64 (the complex path's rule)."""
+
+    def __init__(self, max_dim: int, nb: int, npad: int, dev):
+        from .tc import PlaneSet
+        self.nc = npad // 2
+        self.pv = PlaneSet(1, max_dim, self.nc, dev)
+        self.pt = PlaneSet(1, nb, self.nc, dev)
+        self.pc = PlaneSet(1, nb, max_dim, dev)
+        self.n_fallback = 0
+
+    def rows(self, v: torch.Tensor, r0: int, r1: int) -> None:
+        if r1 > r0:
+            vc = torch.view_as_complex(v.view(v.shape[0], self.nc, 2))
+            self.pv.write(vc, r1 - r0, row0=r0, src_ld=self.nc, src_kstride=0, offset=r0 * self.nc)
+
+    def project(self, t: torch.Tensor, v: torch.Tensor) -> torch.Tensor:
+        from .tc import OP_H, OP_N, zgemm_tc
+        n, m = t.shape[0], v.shape[0]
+        t = t.contiguous()
+        keep = t.clone()
+        tc = torch.view_as_complex(t.view(n, self.nc, 2))
+        self.pt.write(tc, n, src_ld=self.nc, src_kstride=0)
+        c = torch.empty(n, m, dtype=torch.complex128, device=t.device)
+        zgemm_tc(OP_H, n, m, self.nc, self.pt, self.pv, c, m, n * m)
+        c.imag.zero_()
+        self.pc.write(c, n, src_ld=m, src_kstride=0, cols=m)
+        zgemm_tc(OP_N, n, self.nc, m, self.pc, self.pv, tc, self.nc, n * self.nc, alpha=-1.0, beta=1.0)
+        if float(torch.linalg.vector_norm(t, dim=1).min()) < 1e-2:
+            self.n_fallback += 1
+            return keep - (keep @ v.T) @ v
+        return t
+
+
+def _expand(t: torch.Tensor, v: torch.Tensor, tcp: _TcProjection | None = None) -> torch.Tensor:
     """New directions from preconditioned residuals: unit rows, two
     projections against the orthonormal basis v, Householder QR dropping rows
     that kept less than 1e-8 of their norm, then one more projection and QR so
@@ -255,7 +300,7 @@ def _expand(t: torch.Tensor, v: torch.Tensor) -> torch.Tensor:
     rounds). Unit rows and a relative threshold, as the batched Davidson does
     (``:406-457``), remove that floor."""
     t = t / torch.linalg.vector_norm(t, dim=1, keepdim=True).clamp_min(1e-300)
-    t = t - (t @ v.T) @ v
+    t = tcp.project(t, v) if tcp is not None else t - (t @ v.T) @ v
     t = t - (t @ v.T) @ v
     # Cholesky-QR twice (float64 Gram, Cholesky, triangular solve: GEMM-rich)
     # when every row keeps more than 1e-8 of its unit norm; else the
@@ -318,12 +363,21 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
     phi0 = embed_real(gb, x0.to(dev, torch.complex128))
     nb, nphi = phi0.shape
     max_dim = min(max_dim_factor * nb, nphi)
-    t_phi = ham.t_phi
+    # rows are kept at an even width (one zero pad column), so that a real row
+    # is also a complex row for the tensor-core products
+    npad = nphi + (nphi & 1)
+    phi0 = torch.nn.functional.pad(phi0, (0, npad - nphi))
+    t_phi = torch.nn.functional.pad(ham.t_phi, (0, npad - nphi))
+    tcp = _TcProjection(max_dim, nb, npad, dev) if (mode == "mixed" and dev.type == "cuda"
+                                                    and os.environ.get("GWB_TC_PROJECT", "1") != "0") else None
     v = _orthonormalize(phi0.clone())
     if v.shape[0] < nb:  # degenerate start: pad with seeded noise (``:345-350``)
         gen = torch.Generator(device="cpu").manual_seed(1234)
         pad = torch.randn(nb - v.shape[0], nphi, generator=gen, dtype=torch.float64).to(dev)
+        pad = torch.nn.functional.pad(pad, (0, npad - nphi))
         v = torch.cat([v, _orthonormalize(pad, against=v)])
+    if tcp is not None:
+        tcp.rows(v, 0, v.shape[0])
     low = mode == "mixed"
     f32, f64 = _lib.GWB_FP32, _lib.GWB_FP64
     cert_floor = 32.0 * float(torch.finfo(torch.float32).eps) * max(float(t_phi.max()), 1.0)
@@ -368,17 +422,19 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
                     rmax = float(rn.max())
                 if rmax >= tol:  # hand-off: float64 from the certified block on
                     low = False
-                    v, hv, m0 = x, hx, 0
+                    v, hv, m0 = x.contiguous(), hx, 0
+                    if tcp is not None:
+                        tcp.rows(v, 0, v.shape[0])
         with prof("residual"):
             unconv = rn > tol
             done = rmax <= tol and not bool(unconv.any())
         if done:
-            return GammaDavidsonResult(eig, unembed_real(gb, x), it, rn, prof.summary())
+            return GammaDavidsonResult(eig, unembed_real(gb, x[:, :nphi]), it, rn, prof.summary())
         with prof("orthonormalize"):
             t_band = (x * x * t_phi[None, :]).sum(dim=1)
-            t = _expand(_teter(r[unconv], t_phi, t_band[unconv]), v)
+            t = _expand(_teter(r[unconv], t_phi, t_band[unconv]), v, tcp)
         if t.shape[0] == 0:
-            return GammaDavidsonResult(eig, unembed_real(gb, x), it, rn, prof.summary())
+            return GammaDavidsonResult(eig, unembed_real(gb, x[:, :nphi]), it, rn, prof.summary())
         with prof("apply"):
             ht = ham.apply_phi(t, prec=f32 if low else f64)
         if v.shape[0] + t.shape[0] > max_dim:
@@ -386,16 +442,21 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
             v = torch.cat([x, t])
             hv = torch.cat([hx, ht])
             m0 = 0
+            if tcp is not None:
+                tcp.rows(v, 0, v.shape[0])
         else:
+            r0 = v.shape[0]
             v = torch.cat([v, t])
             hv = torch.cat([hv, ht])
+            if tcp is not None:
+                tcp.rows(v, r0, v.shape[0])
     if low:  # out of rounds in float32: certify what there is
         hx = ham.apply_phi(x, prec=f64)
         g = x @ hx.T
         w2, u2 = torch.linalg.eigh(0.5 * (g + g.T))
         x, eig = u2.T @ x, w2
         rn = torch.linalg.vector_norm(u2.T @ hx - eig[:, None] * x, dim=1)
-    return GammaDavidsonResult(eig, unembed_real(gb, x), max_iter, rn, prof.summary())
+    return GammaDavidsonResult(eig, unembed_real(gb, x[:, :nphi]), max_iter, rn, prof.summary())
 
 
 def gamma_start(gb: GammaBasis, nb: int, device=None) -> torch.Tensor:
