@@ -502,14 +502,15 @@ def run_gamma(args):
     x0 = gamma_start(gb, ci.nbands, dev)
     mode = "mixed" if args.solver in ("mixed", "fp32exp", "learned-mixed") else "fp64"
     for _ in range(args.warmup):
-        davidson_gamma(gh, x0, tol=args.tol, max_iter=300, mode=mode)
+        davidson_gamma(gh, x0, tol=args.tol, max_iter=300, mode=mode, max_dim_factor=args.max_dim_factor)
     torch.cuda.synchronize()
     n0 = gh.n_apply
     t0 = time.perf_counter()
-    r = davidson_gamma(gh, x0, tol=args.tol, max_iter=300, mode=mode)
+    r = davidson_gamma(gh, x0, tol=args.tol, max_iter=300, mode=mode, max_dim_factor=args.max_dim_factor)
     torch.cuda.synchronize()
     wall = (time.perf_counter() - t0) * 1e3
-    out = {"mode": "gamma", "config": args.config, "solver": mode, "tol_ev": args.tol, "n_iter": r.n_iter,
+    out = {"mode": "gamma", "config": args.config, "solver": mode, "max_dim_factor": args.max_dim_factor,
+           "tol_ev": args.tol, "n_iter": r.n_iter,
            "wall_ms": wall,
            "band_applies": gh.n_apply - n0, "max_residual_ev": float(r.residual_norms.max()),
            "nhalf": gb.nhalf, "npw": gb.npw}
@@ -551,6 +552,7 @@ def main():
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--tc-shape", default="4,160,640,37000", help="--mode tc: nk,n,m,npw")
+    ap.add_argument("--max-dim-factor", type=int, default=4, help="--mode gamma: basis size / bands")
     ap.add_argument("--mode", default="solve", choices=["solve", "apply", "once", "tc", "gamma"],
                     help="apply: only time Hamiltonian applies; once: a single solve (profiling)")
     ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64"], help="arithmetic of --mode apply")
