@@ -95,3 +95,22 @@ def test_band_path_and_chunk_rule():
     assert chunk_size(8, 24 ** 3) == 24
     assert chunk_size(480, 96 ** 3) == 1
     assert chunk_size(160, 72 ** 3) == int(1.5e9 / (160 * 72 ** 3 * 16))
+
+
+def test_bench_reference_arm_contract():
+    """``bench.py --impl reference`` (the reference's CPU path, timed on the
+    host cores) prints one JSON line with the contract's keys; on the 2-atom
+    cell it runs in seconds."""
+    import json
+    import subprocess
+    import sys
+    out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--config", "si2_fcc",
+                          "--steps", "1", "--warmup", "0"], capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    for key in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["impl"] == "reference" and line["higher_is_better"] is False and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
