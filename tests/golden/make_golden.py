@@ -18,9 +18,11 @@ What is recorded, per case:
     identity start at tol 1e-10 eV: eigenvalues, residual norms, rounds, applies;
   * density: ``density_b`` (``core/batch.py:562-587``) on a seeded block;
   * Gamma path: the half-sphere layout, ``GammaHamiltonian.apply`` and
-    ``davidson_gamma`` (``core/gamma.py``).
+    ``davidson_gamma`` (``core/gamma.py``);
+  * generalized USPP/PAW solve: ``BatchedHS.s`` and ``davidson_gen_batched``
+    (``scf/uspp_batch.py``) with a synthetic augmentation matrix q.
 
-Usage: python tests/golden/make_golden.py [small|big|all|density|gamma] [--ref /path/to/gradwave/src]
+Usage: python tests/golden/make_golden.py [small|big|all|density|gamma|uspp] [--ref /path/to/gradwave/src]
 """
 
 from __future__ import annotations
@@ -192,6 +194,43 @@ def gamma_case(name: str, nb_apply: int, seed: int, solve: bool) -> dict:
     return rec
 
 
+def uspp_q(natoms: int, seed: int) -> np.ndarray:
+    """Synthetic augmentation matrix for the generalized problem: per atom a
+    seeded symmetric positive 4 x 4 block on its (s, p_y, p_z, p_x) projector
+    columns, scaled to norm 0.3, so that S = 1 + sum q |beta><beta| is
+    positive definite."""
+    rng = np.random.default_rng(seed)
+    q = np.zeros((4 * natoms, 4 * natoms))
+    for a in range(natoms):
+        m = rng.standard_normal((4, 4))
+        blk = m @ m.T
+        q[4 * a:4 * a + 4, 4 * a:4 * a + 4] = 0.3 * blk / np.linalg.norm(blk, 2)
+    return q
+
+
+def uspp_case(name: str, seed: int) -> dict:
+    """The generalized USPP/PAW band solve (``scf/uspp_batch.py``):
+    ``BatchedHS`` with the cell's D as the screened D and a synthetic q, its S
+    apply on a seeded block, and ``davidson_gen_batched`` from the identity
+    start at tol 1e-10 eV."""
+    from gradwave.scf.uspp_batch import BatchedHS, davidson_gen_batched
+
+    ci = make_cell(name)
+    grid, bk, p = reference_setup(ci)
+    q = uspp_q(len(ci.positions), seed)
+    assert q.shape[0] == p.shape[1]
+    hs = BatchedHS(bk, grid.shape, ci.v_eff_r, p, bk.dij_full, torch.from_numpy(q))
+    nk, npw = bk.mask.shape
+    c = torch.from_numpy(random_block(seed, nk, 2, npw))
+    rec = {"q": q, "seed": np.array(seed), "s_chk": checksums(hs.s(c).numpy(), seed)}
+    x0 = ci.identity_start()
+    t0 = time.perf_counter()
+    eig, x = davidson_gen_batched(hs, x0, ci.nbands, tol=TOL, max_iter=200)
+    rec["solve_seconds"] = np.array(time.perf_counter() - t0)
+    rec["eigenvalues"] = eig.numpy()
+    return rec
+
+
 def density_checksums(rho: np.ndarray, seed: int, nvec: int = 3) -> np.ndarray:
     rng = np.random.default_rng(seed + 2000)
     vals = [rho.sum(), (rho * rho).sum()]
@@ -224,7 +263,8 @@ def synthetic_case(seed: int = 2, nk: int = 4, npw: int = 80, nb: int = 8) -> di
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("which", nargs="?", default="small", choices=["small", "big", "all", "density", "gamma"])
+    ap.add_argument("which", nargs="?", default="small",
+                    choices=["small", "big", "all", "density", "gamma", "uspp"])
     ap.add_argument("--ref", default="/root/reference/src")
     args = ap.parse_args()
     shim(args.ref)
@@ -243,6 +283,11 @@ def main():
             ("density_si2_fcc", lambda: density_case("si2_fcc", 6, 21, True)),
             ("density_si8_cubic", lambda: density_case("si8_cubic", 5, 22, False)),
             ("density_si64_cubic", lambda: density_case("si64_cubic", 3, 23, False)),
+        ]
+    if args.which in ("uspp", "all"):
+        jobs += [
+            ("uspp_si2_fcc", lambda: uspp_case("si2_fcc", 41)),
+            ("uspp_si8_cubic", lambda: uspp_case("si8_cubic", 42)),
         ]
     if args.which in ("gamma", "all"):
         jobs += [
