@@ -501,15 +501,19 @@ def run_gamma(args):
     gh = GammaHamiltonian(gb, ci.v_eff_r, ci.p[0], ci.bk.dij_full, device=dev)
     x0 = gamma_start(gb, ci.nbands, dev)
     mode = "mixed" if args.solver in ("mixed", "fp32exp", "learned-mixed") else "fp64"
+    lock = {"auto": None, "on": True, "off": False}[args.lock]
+    kw = dict(tol=args.tol, max_iter=300, mode=mode, max_dim_factor=args.max_dim_factor, lock=lock,
+              n_buffer=args.n_buffer)
     for _ in range(args.warmup):
-        davidson_gamma(gh, x0, tol=args.tol, max_iter=300, mode=mode, max_dim_factor=args.max_dim_factor)
+        davidson_gamma(gh, x0, **kw)
     torch.cuda.synchronize()
     n0 = gh.n_apply
     t0 = time.perf_counter()
-    r = davidson_gamma(gh, x0, tol=args.tol, max_iter=300, mode=mode, max_dim_factor=args.max_dim_factor)
+    r = davidson_gamma(gh, x0, **kw)
     torch.cuda.synchronize()
     wall = (time.perf_counter() - t0) * 1e3
     out = {"mode": "gamma", "config": args.config, "solver": mode, "max_dim_factor": args.max_dim_factor,
+           "lock": (mode == "mixed") if lock is None else lock, "n_buffer": args.n_buffer,
            "tol_ev": args.tol, "n_iter": r.n_iter,
            "wall_ms": wall,
            "band_applies": gh.n_apply - n0, "max_residual_ev": float(r.residual_norms.max()),
@@ -553,6 +557,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--tc-shape", default="4,160,640,37000", help="--mode tc: nk,n,m,npw")
     ap.add_argument("--max-dim-factor", type=int, default=4, help="--mode gamma: basis size / bands")
+    ap.add_argument("--lock", default="auto", choices=["auto", "on", "off"],
+                    help="--mode gamma: lock converged pairs (auto: on in the mixed mode)")
+    ap.add_argument("--n-buffer", type=int, default=0, help="--mode gamma: buffer bands above the wanted ones")
     ap.add_argument("--mode", default="solve", choices=["solve", "apply", "once", "tc", "gamma"],
                     help="apply: only time Hamiltonian applies; once: a single solve (profiling)")
     ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64"], help="arithmetic of --mode apply")

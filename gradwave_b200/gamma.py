@@ -286,11 +286,31 @@ class _TcProjection:
         return t
 
 
-def _expand(t: torch.Tensor, v: torch.Tensor, tcp: _TcProjection | None = None) -> torch.Tensor:
+def _project_out(t: torch.Tensor, basis: torch.Tensor) -> torch.Tensor:
+    """t -= (t basis^T) basis, in place (one float64 GEMM pair)."""
+    if basis.shape[0]:
+        t.addmm_(t @ basis.T, basis, alpha=-1.0)
+    return t
+
+
+def _cholqr(y: torch.Tensor):
+    """Cholesky-QR of the rows of y: L = chol(y y^T), y <- L^-1 y, with the
+    triangular inverse formed once (n x n) and applied as one GEMM. Returns
+    None when the Gram matrix is not numerically positive definite (a row kept
+    less than 1e-8 of its unit norm)."""
+    L, info = torch.linalg.cholesky_ex(y @ y.T)
+    if int(info.max()) != 0 or float(torch.diagonal(L).min()) <= 1e-8:
+        return None
+    eye = torch.eye(L.shape[0], dtype=L.dtype, device=L.device)
+    return torch.linalg.solve_triangular(L, eye, upper=False) @ y
+
+
+def _expand(t: torch.Tensor, v: torch.Tensor, tcp: _TcProjection | None = None,
+            locked: torch.Tensor | None = None) -> torch.Tensor:
     """New directions from preconditioned residuals: unit rows, two
-    projections against the orthonormal basis v, Householder QR dropping rows
-    that kept less than 1e-8 of their norm, then one more projection and QR so
-    that the kept rows are orthogonal to v at float64 round-off.
+    projections against the orthonormal basis v (and the locked rows, which
+    are orthogonal to v), then Cholesky-QR; Householder QR dropping rows that
+    kept less than 1e-8 of their norm when Cholesky-QR breaks down.
 
     The reference's single-k Davidson orthonormalises the raw preconditioned
     residuals with an absolute 1e-10 rank threshold (``solvers/davidson.py:
@@ -298,28 +318,28 @@ def _expand(t: torch.Tensor, v: torch.Tensor, tcp: _TcProjection | None = None) 
     below ~1e-8 eV rows of round-off survive, the basis loses orthogonality and
     the solve stalls or diverges (on si216 at 1e-9 eV: residual 2e-2 after 300
     rounds). Unit rows and a relative threshold, as the batched Davidson does
-    (``:406-457``), remove that floor."""
+    (``:406-457``), remove that floor. The second Cholesky-QR round is skipped
+    when the first already left the Gram matrix within 1e-13 of the identity
+    (it would change the rows by that much)."""
     t = t / torch.linalg.vector_norm(t, dim=1, keepdim=True).clamp_min(1e-300)
-    t = tcp.project(t, v) if tcp is not None else t - (t @ v.T) @ v
-    t = t - (t @ v.T) @ v
-    # Cholesky-QR twice (float64 Gram, Cholesky, triangular solve: GEMM-rich)
-    # when every row keeps more than 1e-8 of its unit norm; else the
-    # Householder path below, which drops the dependent rows
-    ok = True
-    y = t
-    for _ in range(2):
-        L, info = torch.linalg.cholesky_ex(y @ y.T)
-        if int(info.max()) != 0 or float(torch.diagonal(L).min()) <= 1e-8:
-            ok = False
-            break
-        y = torch.linalg.solve_triangular(L, y, upper=False)
-    if ok:
-        return y
+    lk = locked if locked is not None else v[:0]
+    _project_out(t, lk)
+    t = tcp.project(t, v) if tcp is not None else _project_out(t, v)
+    _project_out(_project_out(t, lk), v)
+    y = _cholqr(t)
+    if y is not None:
+        g = y @ y.T
+        g.diagonal().sub_(1.0)
+        if float(g.abs().max()) < 1e-13:
+            return y
+        y2 = _cholqr(y)
+        if y2 is not None:
+            return y2
     q, r = torch.linalg.qr(t.T, mode="reduced")
     t = q.T[r.diagonal().abs() > 1e-8]
     if t.shape[0] == 0:
         return t
-    t = t - (t @ v.T) @ v
+    _project_out(_project_out(t, lk), v)
     q, _ = torch.linalg.qr(t.T, mode="reduced")
     return q.T
 
@@ -332,9 +352,41 @@ def _teter(residual: torch.Tensor, t_g: torch.Tensor, t_band: torch.Tensor) -> t
     return residual * (num / (num + 16.0 * x2 * x2))
 
 
+class _Locked:
+    """Converged Ritz pairs taken out of the active Rayleigh-Ritz: rows,
+    images, eigenvalues and residual norms, in preallocated buffers."""
+
+    def __init__(self, cap: int, npad: int, dev):
+        self.x = torch.empty(cap, npad, dtype=torch.float64, device=dev)
+        self.hx = torch.empty(cap, npad, dtype=torch.float64, device=dev)
+        self.eig = torch.empty(cap, dtype=torch.float64, device=dev)
+        self.rn = torch.empty(cap, dtype=torch.float64, device=dev)
+        self.n = 0
+
+    def add(self, x, hx, eig, rn) -> None:
+        k = int(x.shape[0])
+        self.x[self.n:self.n + k] = x
+        self.hx[self.n:self.n + k] = hx
+        self.eig[self.n:self.n + k] = eig
+        self.rn[self.n:self.n + k] = rn
+        self.n += k
+
+    def rows(self) -> torch.Tensor:
+        return self.x[:self.n]
+
+    def merge(self, eig, x, rn):
+        """Locked and active wanted pairs together, ascending."""
+        if self.n == 0:
+            return eig, x, rn
+        e = torch.cat([self.eig[:self.n], eig])
+        order = torch.argsort(e)
+        return e[order], torch.cat([self.x[:self.n], x])[order], torch.cat([self.rn[:self.n], rn])[order]
+
+
 @torch.no_grad()
 def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, max_iter: int = 40,
-                   max_dim_factor: int = 4, mode: str = "fp64") -> GammaDavidsonResult:
+                   max_dim_factor: int = 4, mode: str = "fp64", lock: bool | None = None,
+                   n_buffer: int = 0, buffer_tol: float = 1e-2) -> GammaDavidsonResult:
     """Real-symmetric block Davidson on the half sphere
     (``core/gamma.py:261-290``): the single-k Davidson of the reference
     (``solvers/davidson.py:330-395``: Rayleigh-Ritz on the whole subspace,
@@ -353,45 +405,96 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
     collapses to the certified block and the solve continues in float64 (the
     complex path's mixed rule, ``davidson.py``; gradwave
     ``solvers/davidson.py:226-308``). Every convergence decision is made on
-    float64 residuals."""
+    float64 residuals.
+
+    ``lock`` (default: on in the mixed mode, off in float64 mode, which keeps
+    the reference's rules): at a restart, wanted Ritz pairs whose float64
+    residual is within ``tol`` leave the active Rayleigh-Ritz for good. The
+    restarted basis holds only the unconverged Ritz vectors and the new
+    directions, so the eigensolve and the Ritz products of the rounds that
+    follow (often only a few stragglers left) run on a basis a fraction of
+    the size; the cap stays the reference's max_dim, so stragglers keep
+    their history. New directions are also projected against the locked
+    rows. A locked pair's coupling to the active space is its residual
+    (<= tol), so the active pairs move by O(tol^2/gap). Locking happens only
+    on float64 residuals, never in the float32 phase.
+
+    ``n_buffer`` extra Ritz pairs ride along above the wanted ones (started on
+    the next half-sphere slots): they keep the wanted block's upper edge away
+    from the first unwanted eigenvalue, are expanded only while their residual
+    exceeds ``buffer_tol`` (eV) and are neither tested nor returned."""
     if mode not in ("fp64", "mixed"):
         raise ValueError(f"mode must be 'fp64' or 'mixed', got {mode!r}")
+    if n_buffer < 0:
+        raise ValueError(f"n_buffer must be >= 0, got {n_buffer}")
     import os
     from .davidson import _PhaseTimer
     prof = _PhaseTimer(os.environ.get("GWB_PROFILE", "0") == "1")
+    lock = (mode == "mixed") if lock is None else bool(lock)
     gb, dev = ham.gb, ham.device
     phi0 = embed_real(gb, x0.to(dev, torch.complex128))
-    nb, nphi = phi0.shape
-    max_dim = min(max_dim_factor * nb, nphi)
+    nwant, nphi = phi0.shape
+    n_buffer = min(int(n_buffer), nphi - nwant)
+    if n_buffer:  # buffer starts: unit vectors on the next embedded coordinates
+        extra = torch.zeros(n_buffer, nphi, dtype=torch.float64, device=dev)
+        extra[torch.arange(n_buffer), torch.arange(nwant, nwant + n_buffer)] = 1.0
+        phi0 = torch.cat([phi0, extra])
+    nb = nwant + n_buffer
+
+    # the reference's basis cap, for the whole block (buffer bands included)
+    max_dim = max(min(max_dim_factor * nb, nphi), nb + 1)
+    # the active basis and its images live in preallocated buffers; a restart
+    # to [Ritz block, new directions] needs up to 2 nb rows
+    rows = max(max_dim, 2 * nb)
     # rows are kept at an even width (one zero pad column), so that a real row
     # is also a complex row for the tensor-core products
     npad = nphi + (nphi & 1)
     phi0 = torch.nn.functional.pad(phi0, (0, npad - nphi))
     t_phi = torch.nn.functional.pad(ham.t_phi, (0, npad - nphi))
-    tcp = _TcProjection(max_dim, nb, npad, dev) if (mode == "mixed" and dev.type == "cuda"
-                                                    and os.environ.get("GWB_TC_PROJECT", "1") != "0") else None
-    v = _orthonormalize(phi0.clone())
-    if v.shape[0] < nb:  # degenerate start: pad with seeded noise (``:345-350``)
+    tcp = _TcProjection(rows, nb, npad, dev) if (mode == "mixed" and dev.type == "cuda"
+                                                 and os.environ.get("GWB_TC_PROJECT", "1") != "0") else None
+    v0 = _orthonormalize(phi0.clone())
+    if v0.shape[0] < nb:  # degenerate start: pad with seeded noise (``:345-350``)
         gen = torch.Generator(device="cpu").manual_seed(1234)
-        pad = torch.randn(nb - v.shape[0], nphi, generator=gen, dtype=torch.float64).to(dev)
+        pad = torch.randn(nb - v0.shape[0], nphi, generator=gen, dtype=torch.float64).to(dev)
         pad = torch.nn.functional.pad(pad, (0, npad - nphi))
-        v = torch.cat([v, _orthonormalize(pad, against=v)])
+        v0 = torch.cat([v0, _orthonormalize(pad, against=v0)])
+    V = torch.empty(rows, npad, dtype=torch.float64, device=dev)
+    HV = torch.empty(rows, npad, dtype=torch.float64, device=dev)
+    m = nb
+    V[:m] = v0
     if tcp is not None:
-        tcp.rows(v, 0, v.shape[0])
+        tcp.rows(V, 0, m)
     low = mode == "mixed"
     f32, f64 = _lib.GWB_FP32, _lib.GWB_FP64
     cert_floor = 32.0 * float(torch.finfo(torch.float32).eps) * max(float(t_phi.max()), 1.0)
     prev = float("inf")
-    hv = ham.apply_phi(v, prec=f32 if low else f64)
-    eig = torch.zeros(nb, dtype=torch.float64, device=dev)
-    x = v[:nb]
-    rn = torch.full((nb,), float("inf"), dtype=torch.float64, device=dev)
+    HV[:m] = ham.apply_phi(V[:m], prec=f32 if low else f64)
+    locked = _Locked(nwant, npad, dev)
     # the subspace matrix grows by the new columns only (m0: rows already in it)
-    S = torch.zeros(max_dim, max_dim, dtype=torch.float64, device=dev)
+    S = torch.zeros(rows, rows, dtype=torch.float64, device=dev)
     m0 = 0
+
+    def certify(x):
+        """Float64 apply of the Ritz block and its nb x nb Rayleigh-Ritz
+        (gradwave ``solvers/davidson.py:281-308``)."""
+        hx = ham.apply_phi(x, prec=f64)
+        g = x @ hx.T
+        w2, u2 = torch.linalg.eigh(0.5 * (g + g.T))
+        x, hx = u2.T @ x, u2.T @ hx
+        r = hx - w2[:, None] * x
+        return x, hx, w2, r, torch.linalg.vector_norm(r, dim=1)
+
+    def finish(eig, x, rn, nw_a, it):
+        e, xx, r = locked.merge(eig[:nw_a], x[:nw_a], rn[:nw_a])
+        return GammaDavidsonResult(e, unembed_real(gb, xx[:, :nphi]), it, r, prof.summary())
+
+    it = 0
     for it in range(1, max_iter + 1):
+        nb_a = nb - locked.n      # active Ritz block
+        nw_a = nwant - locked.n   # wanted pairs still in it
+        v, hv = V[:m], HV[:m]
         with prof("subspace_gemm"):
-            m = v.shape[0]
             blk = v @ hv[m0:m].T                       # (m, m - m0)
             S[:m, m0:m] = blk
             S[m0:m, :m0] = blk[:m0].T
@@ -400,63 +503,74 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
             s = S[:m, :m]
         with prof("eigh"):
             w, u = torch.linalg.eigh(s)
-        eig = w[:nb]
+        eig = w[:nb_a]
         with prof("ritz_gemm"):
-            x = u[:, :nb].T @ v
-            hx = u[:, :nb].T @ hv
+            ut = u[:, :nb_a].T
+            x = ut @ v
+            hx = ut @ hv
         with prof("residual"):
             r = hx - eig[:, None] * x
             rn = torch.linalg.vector_norm(r, dim=1)
-            rmax = float(rn.max())
+            rmax = float(rn[:nw_a].max())
         if low:
             stalled = it > 1 and rmax > 0.7 * prev and rmax < 100.0 * cert_floor
             prev = rmax
-            if rmax < max(tol, cert_floor) or stalled:
+            if rmax < max(tol, cert_floor) or rmax <= tol or stalled:
                 with prof("certify"):
-                    hx = ham.apply_phi(x, prec=f64)
-                    g = x @ hx.T
-                    w2, u2 = torch.linalg.eigh(0.5 * (g + g.T))
-                    x, hx, eig = u2.T @ x, u2.T @ hx, w2
-                    r = hx - eig[:, None] * x
-                    rn = torch.linalg.vector_norm(r, dim=1)
-                    rmax = float(rn.max())
+                    x, hx, eig, r, rn = certify(x)
+                    rmax = float(rn[:nw_a].max())
                 if rmax >= tol:  # hand-off: float64 from the certified block on
                     low = False
-                    v, hv, m0 = x.contiguous(), hx, 0
+                    V[:nb_a] = x
+                    HV[:nb_a] = hx
+                    m, m0 = nb_a, 0
+                    x, hx = V[:nb_a], HV[:nb_a]
+                    v, hv = V[:m], HV[:m]
                     if tcp is not None:
-                        tcp.rows(v, 0, v.shape[0])
+                        tcp.rows(V, 0, m)
         with prof("residual"):
             unconv = rn > tol
-            done = rmax <= tol and not bool(unconv.any())
+            if n_buffer:
+                unconv[nw_a:] = rn[nw_a:] > max(tol, buffer_tol)
+            done = rmax <= tol
         if done:
-            return GammaDavidsonResult(eig, unembed_real(gb, x[:, :nphi]), it, rn, prof.summary())
+            return finish(eig, x, rn, nw_a, it)
         with prof("orthonormalize"):
             t_band = (x * x * t_phi[None, :]).sum(dim=1)
-            t = _expand(_teter(r[unconv], t_phi, t_band[unconv]), v, tcp)
-        if t.shape[0] == 0:
-            return GammaDavidsonResult(eig, unembed_real(gb, x[:, :nphi]), it, rn, prof.summary())
+            t = _expand(_teter(r[unconv], t_phi, t_band[unconv]), v, tcp, locked.rows())
+        if t.shape[0] == 0:  # no independent direction left
+            if low:
+                x, hx, eig, r, rn = certify(x)
+            return finish(eig, x, rn, nw_a, it)
         with prof("apply"):
             ht = ham.apply_phi(t, prec=f32 if low else f64)
-        if v.shape[0] + t.shape[0] > max_dim:
-            # the Ritz block spans what v keeps; t is orthogonal to all of v
-            v = torch.cat([x, t])
-            hv = torch.cat([hx, ht])
-            m0 = 0
+        with prof("restart"):
+            nt = int(t.shape[0])
+            lockable = (rn[:nw_a] <= tol) if (lock and not low) else None
+            n_lock = int(lockable.sum()) if lockable is not None else 0
+            if m + nt > max_dim:
+                # restart: [Ritz block, t]; t is orthogonal to all of v and to
+                # the locked rows. Wanted pairs within tol are locked first.
+                keep = torch.ones(nb_a, dtype=torch.bool, device=dev)
+                if n_lock:
+                    keep[:nw_a] = ~lockable
+                    locked.add(x[:nw_a][lockable], hx[:nw_a][lockable], eig[:nw_a][lockable],
+                               rn[:nw_a][lockable])
+                xk, hxk = x[keep], hx[keep]   # copies (x may alias V rows)
+                k = int(xk.shape[0])
+                V[:k] = xk
+                HV[:k] = hxk
+                r0, m, m0 = 0, k, 0
+            else:
+                r0 = m
+            V[m:m + nt] = t
+            HV[m:m + nt] = ht
+            m += nt
             if tcp is not None:
-                tcp.rows(v, 0, v.shape[0])
-        else:
-            r0 = v.shape[0]
-            v = torch.cat([v, t])
-            hv = torch.cat([hv, ht])
-            if tcp is not None:
-                tcp.rows(v, r0, v.shape[0])
+                tcp.rows(V, r0, m)
     if low:  # out of rounds in float32: certify what there is
-        hx = ham.apply_phi(x, prec=f64)
-        g = x @ hx.T
-        w2, u2 = torch.linalg.eigh(0.5 * (g + g.T))
-        x, eig = u2.T @ x, w2
-        rn = torch.linalg.vector_norm(u2.T @ hx - eig[:, None] * x, dim=1)
-    return GammaDavidsonResult(eig, unembed_real(gb, x[:, :nphi]), max_iter, rn, prof.summary())
+        x, hx, eig, r, rn = certify(x)
+    return finish(eig, x, rn, nwant - locked.n, max_iter)
 
 
 def gamma_start(gb: GammaBasis, nb: int, device=None) -> torch.Tensor:

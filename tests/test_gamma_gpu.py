@@ -73,14 +73,17 @@ def test_gamma_davidson_si2_matches_reference(cuda_device):
     assert float((gram - torch.eye(ci.nbands, dtype=gram.dtype, device=gram.device)).abs().max()) < 1e-12
 
 
-@pytest.mark.parametrize("mode,tol", [("fp64", 1e-6), ("fp64", 1e-10), ("mixed", 1e-10)])
-def test_gamma_davidson_si216_matches_complex_reference(cuda_device, mode, tol):
+@pytest.mark.parametrize("mode,tol,nbuf", [("fp64", 1e-6, 0), ("fp64", 1e-10, 0), ("mixed", 1e-10, 0),
+                                           ("mixed", 1e-10, 32)])
+def test_gamma_davidson_si216_matches_complex_reference(cuda_device, mode, tol, nbuf):
     """si216 on the Gamma path, float64 and mixed (float32 expansion applies,
-    float64 certification and hand-off), to 1e-6 and 1e-10 eV."""
+    float64 certification and hand-off, converged pairs locked), with and
+    without buffer bands, to 1e-6 and 1e-10 eV."""
     from gradwave_b200.gamma import davidson_gamma, gamma_start
     gc = load_golden("si216_vacancy")
     ci, gb, gh = _gamma("si216_vacancy", cuda_device)
-    res = davidson_gamma(gh, gamma_start(gb, ci.nbands, cuda_device), tol=tol, max_iter=200, mode=mode)
+    res = davidson_gamma(gh, gamma_start(gb, ci.nbands, cuda_device), tol=tol, max_iter=200, mode=mode,
+                         n_buffer=nbuf)
     eig = res.eigenvalues.cpu().numpy()
     assert float(res.residual_norms.max()) < tol
     assert np.abs(eig - gc["eigenvalues"][0]).max() < 1e-8 * HA

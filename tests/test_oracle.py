@@ -149,8 +149,9 @@ def test_gamma_basis_and_oracle_apply_match_reference(name):
 def test_gamma_davidson_algebra_on_cpu():
     """The real-embedding Davidson (``gradwave_b200.gamma.davidson_gamma``:
     incremental subspace matrix, Cholesky-QR expansion with the Householder
-    fallback, restarts keeping HX) driven on the CPU by the oracle Gamma apply:
-    si2 to 1e-10 eV, eigenvalues equal to the reference's complex solve."""
+    fallback, restarts keeping HX, locking of converged pairs, buffer bands)
+    driven on the CPU by the oracle Gamma apply: si2 to 1e-10 eV, eigenvalues
+    equal to the reference's complex solve, returned rows orthonormal."""
     import torch
     from gradwave_b200 import gamma as G
     from gradwave_b200.cells import make_cell
@@ -172,10 +173,17 @@ def test_gamma_davidson_algebra_on_cpu():
     h = _Ham()
     h.gb, h.t_phi = gb, G.kinetic_phi(gb)
     g = load_golden("si2_fcc")
-    for mode in ("fp64", "mixed"):
-        res = G.davidson_gamma(h, G.gamma_start(gb, ci.nbands), tol=1e-10, max_iter=100, mode=mode)
-        assert float(res.residual_norms.max()) < 1e-10
-        assert np.abs(res.eigenvalues.numpy() - g["eigenvalues"][0]).max() < 1e-9
+    cases = [("fp64", {}), ("mixed", {}), ("fp64", {"lock": True}), ("mixed", {"n_buffer": 4}),
+             ("fp64", {"lock": True, "n_buffer": 3, "max_dim_factor": 3})]
+    for mode, kw in cases:
+        res = G.davidson_gamma(h, G.gamma_start(gb, ci.nbands), tol=1e-10, max_iter=100, mode=mode, **kw)
+        assert float(res.residual_norms.max()) < 1e-10, (mode, kw)
+        assert res.eigenvalues.shape == (ci.nbands,) and res.eigenvectors.shape == (ci.nbands, gb.nhalf)
+        assert np.abs(res.eigenvalues.numpy() - g["eigenvalues"][0]).max() < 1e-9, (mode, kw)
+        gram = G.metric_inner(gb, res.eigenvectors, res.eigenvectors)
+        assert float((gram - torch.eye(ci.nbands, dtype=gram.dtype)).abs().max()) < 1e-12, (mode, kw)
+    with pytest.raises(ValueError):
+        G.davidson_gamma(h, G.gamma_start(gb, ci.nbands), n_buffer=-1)
 
 
 def test_oracle_uspp_overlap_and_dense_solve_match_reference():
