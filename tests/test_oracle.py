@@ -186,6 +186,40 @@ def test_gamma_davidson_algebra_on_cpu():
         G.davidson_gamma(h, G.gamma_start(gb, ci.nbands), n_buffer=-1)
 
 
+def test_gamma_locking_and_buffers_on_si8_gamma_point():
+    """Locking and buffer bands on a larger block: si8's Gamma point, 24 bands
+    with a threefold-degenerate level at the top of the block, driven on the
+    CPU by the oracle apply. Eigenvalues equal the reference's complex solve
+    at k = 0 to 1e-9 eV; the returned rows are orthonormal."""
+    import torch
+    from gradwave_b200 import gamma as G
+    from gradwave_b200.cells import at_kpoints, make_cell
+    from oracle.gamma import gamma_apply
+    from oracle.ham import from_cell
+    ci = at_kpoints(make_cell("si8_cubic"), [[0.0, 0.0, 0.0]])
+    gb = G.build_gamma_basis(ci.spheres[0], ci.shape)
+    orc = from_cell(ci)
+
+    class _Ham:
+        device = torch.device("cpu")
+
+        def apply_phi(self, phi, prec=None):
+            nphi = 2 * gb.nhalf - 1
+            ch = G.unembed_real(gb, phi[:, :nphi].contiguous()).numpy()
+            out = gamma_apply(orc, gb.src_half.numpy(), gb.conj_full.numpy(), gb.rep_full_idx.numpy(), ch)
+            return torch.nn.functional.pad(G.embed_real(gb, torch.from_numpy(out)), (0, phi.shape[1] - nphi))
+
+    h = _Ham()
+    h.gb, h.t_phi = gb, G.kinetic_phi(gb)
+    ref = load_golden("si8_cubic")["eigenvalues"][0]
+    for mode, kw in [("mixed", {}), ("fp64", {"lock": True, "n_buffer": 4})]:
+        res = G.davidson_gamma(h, G.gamma_start(gb, ci.nbands), tol=1e-10, max_iter=120, mode=mode, **kw)
+        assert float(res.residual_norms.max()) < 1e-10, (mode, kw)
+        assert np.abs(res.eigenvalues.numpy() - ref).max() < 1e-9, (mode, kw)
+        gram = G.metric_inner(gb, res.eigenvectors, res.eigenvectors)
+        assert float((gram - torch.eye(ci.nbands, dtype=gram.dtype)).abs().max()) < 1e-12, (mode, kw)
+
+
 def test_oracle_uspp_overlap_and_dense_solve_match_reference():
     """The numpy S apply (``oracle/uspp.py``) against the reference's
     ``BatchedHS.s`` checksums on the seeded blocks, and the dense
