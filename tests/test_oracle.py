@@ -182,6 +182,28 @@ def test_gamma_davidson_algebra_on_cpu():
         assert np.abs(res.eigenvalues.numpy() - g["eigenvalues"][0]).max() < 1e-9, (mode, kw)
         gram = G.metric_inner(gb, res.eigenvectors, res.eigenvectors)
         assert float((gram - torch.eye(ci.nbands, dtype=gram.dtype)).abs().max()) < 1e-12, (mode, kw)
+    # out of rounds after pairs were locked: the locked and active pairs come
+    # back together, ascending, with orthonormal rows
+    locks = []
+    add = G._Locked.add
+
+    def counted_add(self, *a):
+        locks.append(int(a[0].shape[0]))
+        return add(self, *a)
+
+    G._Locked.add = counted_add
+    try:
+        for mi in (14, 18):  # pairs get locked in rounds 12 and 16 of this solve
+            res = G.davidson_gamma(h, G.gamma_start(gb, ci.nbands), tol=1e-10, max_iter=mi, mode="fp64",
+                                   lock=True, n_buffer=3, max_dim_factor=3)
+            assert res.n_iter == mi and float(res.residual_norms.max()) > 1e-10
+            e = res.eigenvalues
+            assert e.shape == (ci.nbands,) and bool((e[1:] >= e[:-1]).all())
+            gram = G.metric_inner(gb, res.eigenvectors, res.eigenvectors)
+            assert float((gram - torch.eye(ci.nbands, dtype=gram.dtype)).abs().max()) < 1e-12
+    finally:
+        G._Locked.add = add
+    assert locks, "no pair was locked before the round limit"
     with pytest.raises(ValueError):
         G.davidson_gamma(h, G.gamma_start(gb, ci.nbands), n_buffer=-1)
 
