@@ -544,7 +544,9 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
             return finish(eig, x, rn, nw_a, it)
         with prof("orthonormalize"):
             t_band = (x * x * t_phi[None, :]).sum(dim=1)
-            t = _expand(_teter(r[unconv], t_phi, t_band[unconv]), v, tcp, locked.rows())
+            pr = _teter(r[unconv], t_phi, t_band[unconv])
+            pr[:, nphi:] = 0.0  # the pad column is not a coordinate of the operator
+            t = _expand(pr, v, tcp, locked.rows())
         if t.shape[0] == 0:  # no independent direction left
             if low:
                 x, hx, eig, r, rn = certify(x)

@@ -211,8 +211,10 @@ def test_gamma_davidson_algebra_on_cpu():
 def test_gamma_locking_and_buffers_on_si8_gamma_point():
     """Locking and buffer bands on a larger block: si8's Gamma point, 24 bands
     with a threefold-degenerate level at the top of the block, driven on the
-    CPU by the oracle apply. Eigenvalues equal the reference's complex solve
-    at k = 0 to 1e-9 eV; the returned rows are orthonormal."""
+    CPU by the oracle apply (and, for the mixed schedule, by the oracle apply
+    with float32 rounding and noise on its float32 calls). Eigenvalues equal
+    the reference's complex solve at k = 0 to 1e-9 eV; the returned rows are
+    orthonormal."""
     import torch
     from gradwave_b200 import gamma as G
     from gradwave_b200.cells import at_kpoints, make_cell
@@ -231,11 +233,29 @@ def test_gamma_locking_and_buffers_on_si8_gamma_point():
             out = gamma_apply(orc, gb.src_half.numpy(), gb.conj_full.numpy(), gb.rep_full_idx.numpy(), ch)
             return torch.nn.functional.pad(G.embed_real(gb, torch.from_numpy(out)), (0, phi.shape[1] - nphi))
 
+    class _NoisyHam(_Ham):
+        """float32-arithmetic applies stood in for by rounding the rows and
+        the images to float32 and adding 3e-7 relative noise; float64 applies
+        exact. The mixed schedule must still certify and finish in float64."""
+
+        gen = torch.Generator().manual_seed(5)
+
+        def apply_phi(self, phi, prec=None):
+            from gradwave_b200 import _lib
+            if prec != _lib.GWB_FP32:
+                return super().apply_phi(phi, prec)
+            o = super().apply_phi(phi.float().double(), prec)
+            o = o + 3e-7 * o.abs().max() * torch.randn(o.shape, generator=self.gen, dtype=o.dtype) / o.shape[1] ** 0.5
+            o[:, 2 * gb.nhalf - 1:] = 0.0  # the apply keeps the solver's pad column at zero
+            return o.float().double()
+
     h = _Ham()
     h.gb, h.t_phi = gb, G.kinetic_phi(gb)
+    hn = _NoisyHam()
+    hn.gb, hn.t_phi = gb, G.kinetic_phi(gb)
     ref = load_golden("si8_cubic")["eigenvalues"][0]
-    for mode, kw in [("mixed", {}), ("fp64", {"lock": True, "n_buffer": 4})]:
-        res = G.davidson_gamma(h, G.gamma_start(gb, ci.nbands), tol=1e-10, max_iter=120, mode=mode, **kw)
+    for hh, mode, kw in [(h, "mixed", {}), (h, "fp64", {"lock": True, "n_buffer": 4}), (hn, "mixed", {"n_buffer": 4})]:
+        res = G.davidson_gamma(hh, G.gamma_start(gb, ci.nbands), tol=1e-10, max_iter=120, mode=mode, **kw)
         assert float(res.residual_norms.max()) < 1e-10, (mode, kw)
         assert np.abs(res.eigenvalues.numpy() - ref).max() < 1e-9, (mode, kw)
         gram = G.metric_inner(gb, res.eigenvectors, res.eigenvectors)
