@@ -314,3 +314,31 @@ def test_uspp_davidson_algebra_on_cpu():
     eig, x = davidson_gen_batched(_HS(), ci.identity_start(), ci.nbands, tol=1e-10, max_iter=200)
     assert np.abs(eig.numpy() - g["eigenvalues"]).max() < 1e-10
     assert x.shape == (1, ci.nbands, ci.bk.npw_max)
+
+
+def test_fft_local_term_equals_dense_toeplitz():
+    """The FFT local term of the oracle apply (scatter, inverse FFT / N,
+    x v(r), forward FFT, gather) equals the dense Toeplitz product
+    M[i, j] = V(G_i - G_j), V = fftn(v)/N with box-wrapped index differences
+    (gradwave ``core/batch.py:333-464``, the CPU-only path this build leaves
+    out), to 1e-12; M is Hermitian and padded slots stay zero (gradwave
+    ``tests/unit/test_toeplitz_local.py:61-113``)."""
+    from gradwave_b200.cells import make_cell
+    from oracle.ham import from_cell
+    ci = make_cell("si8_cubic")
+    orc = from_cell(ci)
+    n1, n2, n3 = ci.shape
+    vhat = np.fft.fftn(ci.v_eff_r.numpy()) / (n1 * n2 * n3)
+    rng = np.random.default_rng(11)
+    for k in (0, 3):
+        npw = int(ci.bk.npw[k])
+        m = ci.spheres[k].miller
+        d = m[:, None, :] - m[None, :, :]
+        M = vhat[d[..., 0] % n1, d[..., 1] % n2, d[..., 2] % n3]
+        assert np.abs(M - M.conj().T).max() <= 1e-14 * np.abs(M).max()
+        c = np.zeros((ci.bk.nk, 3, ci.bk.npw_max), dtype=np.complex128)
+        c[k, :, :npw] = rng.standard_normal((3, npw)) + 1j * rng.standard_normal((3, npw))
+        loc = orc.local(c)[k]
+        ref = c[k, :, :npw] @ M.T
+        assert np.abs(loc[:, :npw] - ref).max() <= 1e-12 * np.abs(ref).max()
+        assert np.abs(orc.apply(c)[k, :, npw:]).max() == 0.0
