@@ -7,7 +7,6 @@ Tolerances: eigenvalues 1e-12 relative to the spectral radius, residual
 |A y - lambda y| 1e-12 relative, orthonormality 1e-12.
 """
 
-import ctypes
 
 import numpy as np
 import pytest
