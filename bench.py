@@ -185,7 +185,7 @@ def run_reference(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "c128/f64", "data": "synthetic (seeded Si cells)",
             "config": {"workload": args.config, "nk": nk, "nbands": ci.nbands, "fft": list(ci.shape),
                        "tol_ev": args.tol, "l2": "n/a (CPU)"},
-            "cpu_baseline": {"value": round(v, 3), "unit": "ms", "cores": threads, "kind": "port",
+            "cpu_baseline": {"value": round(v, 3), "unit": "ms", "cores": threads, "kind": "port", "cpu": _cpu_model(),
                              "sample": f"k-points {ks} of {nk} solved to tol {args.tol} eV, time scaled "
                                        f"by {nk}/{len(ks)}; float64 numpy/scipy restatement of the "
                                        "reference's davidson_batched + BatchedHamiltonian.apply"},
@@ -413,6 +413,19 @@ def _largest_config(dev, name: str = "si216_vacancy") -> dict:
     return out
 
 
+def _cpu_model() -> str:
+    """The host CPU's model name (``/proc/cpuinfo``), or the platform string."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or platform.machine()
+
+
 def _cpu_baseline(args, ci):
     """Oracle (float64 numpy) on a bounded sample: two k-points of the workload."""
     import torch
@@ -430,7 +443,7 @@ def _cpu_baseline(args, ci):
     davidson_batched(h.apply, ci.identity_start().numpy()[ks], bk.t.numpy()[ks], bk.mask.numpy()[ks],
                      tol=args.tol, max_iter=300)
     dt = (time.perf_counter() - t0) * 1e3 * nk / len(ks)
-    return {"value": round(dt, 1), "unit": "ms", "cores": threads, "kind": "port",
+    return {"value": round(dt, 1), "unit": "ms", "cores": threads, "kind": "port", "cpu": _cpu_model(),
             "sample": f"k-points {ks} of {nk} solved to tol {args.tol} eV with the float64 oracle, "
                       f"time scaled by {nk}/{len(ks)}"}
 
