@@ -5,7 +5,7 @@ activations, FP32 accumulation; kernels in ``csrc/mlp.cu``) corrects the
 Teter-Payne-Allan filter: K(G) = TPA(x) exp(o(u)) with the features u of
 ``gwb_precond_features`` (|k+G|^2 relative to the band's kinetic energy, the
 band eigenvalue, the residual amplitude at G and the band's kinetic scale).
-TPA stays the fallback and the judge: a band whose residual has not improved
+TPA stays the fallback and the yardstick: a band whose residual has not improved
 on its best value by 10 % for three consecutive rounds reverts to TPA for the
 rest of the solve.
 
