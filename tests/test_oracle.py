@@ -320,8 +320,8 @@ def test_fft_local_term_equals_dense_toeplitz():
     """The FFT local term of the oracle apply (scatter, inverse FFT / N,
     x v(r), forward FFT, gather) equals the dense Toeplitz product
     M[i, j] = V(G_i - G_j), V = fftn(v)/N with box-wrapped index differences
-    (gradwave ``core/batch.py:333-464``, the CPU-only path this build leaves
-    out), to 1e-12; M is Hermitian and padded slots stay zero (gradwave
+    (gradwave ``core/batch.py:333-464``, a CPU-only path that gradwave_b200
+    does not implement), to 1e-12; M is Hermitian and padded slots stay zero (gradwave
     ``tests/unit/test_toeplitz_local.py:61-113``)."""
     from gradwave_b200.cells import make_cell
     from oracle.ham import from_cell
