@@ -58,7 +58,7 @@ class DavidsonStats(ctypes.Structure):
                 ("n_cert", ctypes.c_int32), ("n_repair", ctypes.c_int32), ("n_rollback", ctypes.c_int32),
                 ("n_apply_low", ctypes.c_int64), ("n_apply_full", ctypes.c_int64),
                 ("max_residual", ctypes.c_double), ("apply_ms", ctypes.c_double),
-                ("n_apply_calls", ctypes.c_int64)]
+                ("n_apply_calls", ctypes.c_int64), ("n_tpa_fallback", ctypes.c_int64)]
 
 
 _lock = threading.Lock()
@@ -82,6 +82,8 @@ _SIGNATURES = {
     "gwb_ham_set_projectors": [_P, _P, _P, _P],
     "gwb_ham_apply": [_P, _P, _P, _I, _I, _I, _P],
     "gwb_ham_apply_strided": [_P, _P, _I64, _P, _I64, _I, _I, _I, _P],
+    "gwb_ham_set_overlap": [_P, _P, _P],
+    "gwb_ham_apply_hs": [_P, _P, _I64, _P, _I64, _P, _I64, _I, _I, _I, _P],
     "gwb_ham_scratch_bytes": [_P],
     "gwb_ham_tc_status": [_P, _P],
     "gwb_ham_density": [_P, _P, _I64, _I, _I, _P, _I64, _D, _P, _P],
@@ -93,6 +95,8 @@ _SIGNATURES = {
                      ctypes.c_size_t, _P],
     "gwb_tc_planes": [_I64, _I64, _I64, _P, _I64, _I64, ctypes.c_int, ctypes.c_int, _P, _I64, _I64, _I64, _P],
     "gwb_zgemm_tc_work_bytes": [ctypes.c_int, _I64, _I64, _I64, _I64],
+    "gwb_tc_set_wait_limit": [_I64],
+    "gwb_tc_test_withhold": [_I],
     "gwb_zgemm_tc": [ctypes.c_int, _I64, _I64, _I64, _D, _D, _P, _I64, _I64, _P, _I64, _I64, _D, _D, _P, _I64, _I64,
                      _I64, _P, ctypes.c_size_t, _P, _P],
     "gwb_residual": [_I, _I, _I, _P, _I64, _P, _I64, _P, _I64, _P, _I64, _P, _P],

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <vector>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -51,6 +52,14 @@ __global__ void k_masked_copy(const cplx<double>* __restrict__ src, int64_t sk, 
     const int g = (int)(i % npw);
     dst[k * dk + i] = mask[(int64_t)k * npw + g] ? src[k * sk + i] : mk<double>(0.0, 0.0);
   }
+}
+
+// *flag |= 4 when any of the n complex values is not finite
+__global__ void k_nonfinite(const cplx<double>* __restrict__ z, int64_t n, int* __restrict__ flag) {
+  bool bad = false;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    bad |= !(isfinite(z[i].x) && isfinite(z[i].y));
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 4);
 }
 
 __global__ void k_fill(double* __restrict__ p, int n, double v) {
@@ -113,7 +122,7 @@ struct Work {
   unsigned char* nh_work;
   Z16 *V, *HV, *S, *X, *HX, *R, *D, *D2, *C, *G, *Linv, *Gs, *U;
   double *Zs, *rn, *eig, *eig2, *stats, *rn_prev;
-  int *sel, *info, *heev_info, *flags;
+  int *sel, *info, *heev_info, *flags, *sync_flag;
   unsigned char *tpa_only, *stall_count;
   unsigned char* pl_work;
   size_t pl_work_bytes;
@@ -146,6 +155,7 @@ static size_t layout(const gwb_davidson_params& p, unsigned char* base, Work* w)
   t.info = b.take<int>(base, nk);
   t.heev_info = b.take<int>(base, nk);
   t.flags = b.take<int>(base, 1);
+  t.sync_flag = b.take<int>(base, 1);
   t.nh_work = b.take<unsigned char>(base, NH_WORK_BYTES);
   t.rn_prev = b.take<double>(base, nk * nb);
   t.tpa_only = b.take<unsigned char>(base, nk * nb);
@@ -182,6 +192,20 @@ class Solver {
       GWB_CUDA_TRY(cudaMemsetAsync(w_.tpa_only, 0, (size_t)nk_ * nb_, st_));
       GWB_CUDA_TRY(cudaMemsetAsync(w_.stall_count, 0, (size_t)nk_ * nb_, st_));
     }
+    // a non-finite start block is refused before any kernel uses it
+    {
+      int host_flag = 0;
+      GWB_CUDA_TRY(cudaMemsetAsync(w_.sync_flag, 0, sizeof(int), st_));
+      k_nonfinite<<<148, 256, 0, st_>>>(static_cast<const Z16*>(x0), (int64_t)nk_ * nbp, w_.sync_flag);
+      GWB_LAUNCH_CHECK();
+      count_launches(1);
+      GWB_CUDA_TRY(cudaMemcpyAsync(&host_flag, w_.sync_flag, sizeof(int), cudaMemcpyDeviceToHost, st_));
+      GWB_CUDA_TRY(cudaStreamSynchronize(st_));
+      if (host_flag & 4) {
+        set_error("the start block holds a non-finite value");
+        return GWB_ERR_NONFINITE;
+      }
+    }
     // initial block: masked copy, orthonormalised with host-checked CholQR2
     GWB_TRY(masked_copy(static_cast<const Z16*>(x0), nbp, w_.D, nbp, nb_));
     int ok = 0;
@@ -206,15 +230,23 @@ class Solver {
       bool breakdown = false;
       GWB_TRY(read_stats(&rnmax, &n_add, &breakdown));
       if (breakdown) {
+        // the expansion is redone from the same basis with different inputs:
+        // TPA in place of the network and a rank repair that replaces every
+        // row keeping less than 1e-4 (then 1e-1) of its norm after the first
+        // projection, since the rows that broke CholQR2 were nearly in the span
         ++n_rollback_;
         m = m0 = m_prev;
         --it;
+        force_tpa_ = true;
+        repair_thresh_ = repair_thresh_ < 1e-4 ? 1e-4 : 1e-1;
         if (n_rollback_ > 8) {
           set_error("repeated CholQR2 breakdown in the expansion block");
           return GWB_ERR_BREAKDOWN;
         }
         continue;
       }
+      force_tpa_ = false;
+      repair_thresh_ = 1e-8;
       if (fp32_exp_) {
         // mode 1 (the reference's rule) treats any round that shrinks the
         // residual by < 30 % as a float32 stall; mode 2 only once the residual
@@ -284,6 +316,13 @@ class Solver {
         out->apply_ms = 0.0;
       }
       out->n_apply_calls = n_apply_calls_;
+      out->n_tpa_fallback = 0;
+      if (p_.precond == 1) {
+        std::vector<unsigned char> fb((size_t)nk_ * nb_);
+        GWB_CUDA_TRY(cudaMemcpyAsync(fb.data(), w_.tpa_only, fb.size(), cudaMemcpyDeviceToHost, st_));
+        GWB_CUDA_TRY(cudaStreamSynchronize(st_));
+        for (unsigned char f : fb) out->n_tpa_fallback += f ? 1 : 0;
+      }
       out->n_iter = it;
       out->hit_max_iter = it >= p_.max_iter ? 1 : 0;
       out->n_restart = n_restart_;
@@ -395,6 +434,10 @@ class Solver {
     double hst[4];
     GWB_CUDA_TRY(cudaMemcpyAsync(hst, w_.stats, sizeof(hst), cudaMemcpyDeviceToHost, st_));
     GWB_CUDA_TRY(cudaStreamSynchronize(st_));
+    if (!(hst[0] == hst[0])) {
+      set_error("non-finite residual norm");
+      return GWB_ERR_NONFINITE;
+    }
     if (hst[2] != 0.0) {
       set_error("subspace eigensolver hit the QL iteration limit");
       return GWB_ERR_NOT_CONVERGED;
@@ -404,16 +447,12 @@ class Solver {
     *breakdown = (flags & 2) != 0;
     *rnmax = hst[0];
     *n_add = (int)hst[1];
-    if (!(hst[0] == hst[0])) {
-      set_error("non-finite residual norm");
-      return GWB_ERR_NONFINITE;
-    }
     return GWB_OK;
   }
 
   int precondition(int n_add, const double* eig) {
     const int64_t nbp = (int64_t)nb_ * npw_;
-    if (p_.precond == 1) {
+    if (p_.precond == 1 && !force_tpa_) {
       // stall fallback: a band whose residual has not improved on its best by
       // 10 % for 3 rounds keeps TPA from then on
       GWB_TRY(gwb_stall_update(w_.rn, w_.rn_prev, w_.stall_count, w_.tpa_only, nk_ * nb_, 0.9, 3, st_));
@@ -431,17 +470,17 @@ class Solver {
     *ok = 1;
     for (int pass = 0; pass < 2; ++pass) {
       GWB_TRY(zgemm(0, 2, n, n, npw_, Y, npw_, ys, Y, npw_, ys, w_.G, n, nn));
-      GWB_TRY(gwb_chol_inv(nk_, n, w_.G, n, nn, w_.Linv, nn, w_.info, sync ? nullptr : w_.flags, st_));
+      if (sync) GWB_CUDA_TRY(cudaMemsetAsync(w_.sync_flag, 0, sizeof(int), st_));
+      GWB_TRY(gwb_chol_inv(nk_, n, w_.G, n, nn, w_.Linv, nn, w_.info, sync ? w_.sync_flag : w_.flags, st_));
       if (sync) {
-        int host_info[4096];
-        const int cnt = std::min(nk_, 4096);
-        GWB_CUDA_TRY(cudaMemcpyAsync(host_info, w_.info, sizeof(int) * cnt, cudaMemcpyDeviceToHost, st_));
+        // bit 1 of the flag: a breakdown at any k
+        int host_flag = 0;
+        GWB_CUDA_TRY(cudaMemcpyAsync(&host_flag, w_.sync_flag, sizeof(int), cudaMemcpyDeviceToHost, st_));
         GWB_CUDA_TRY(cudaStreamSynchronize(st_));
-        for (int k = 0; k < cnt; ++k)
-          if (host_info[k] != 0) {
-            *ok = 0;
-            return GWB_OK;
-          }
+        if (host_flag & 2) {
+          *ok = 0;
+          return GWB_OK;
+        }
       }
       GWB_TRY(zgemm(0, 0, n, npw_, n, w_.Linv, n, nn, Y, npw_, ys, Ytmp, npw_, (int64_t)nb_ * npw_));
       GWB_TRY(copy_rows(Y, ys, Ytmp, (int64_t)nb_ * npw_, n));
@@ -463,7 +502,7 @@ class Solver {
     const int64_t nbp = (int64_t)nb_ * npw_;
     GWB_TRY(masked_copy(w_.D, nbp, w_.D, nbp, n));
     if (m) GWB_TRY(project_out(w_.D, nbp, n, m));
-    GWB_TRY(gwb_row_repair(nk_, n, npw_, w_.D, nbp, mask_, 1e-8, w_.flags, st_));
+    GWB_TRY(gwb_row_repair(nk_, n, npw_, w_.D, nbp, mask_, repair_thresh_, w_.flags, st_));
     if (m) GWB_TRY(project_out(w_.D, nbp, n, m));
     int ok = 1;
     return cholqr2(w_.D, nbp, n, w_.D2, nullptr, nullptr, false, &ok);
@@ -478,6 +517,8 @@ class Solver {
   cudaStream_t st_;
   int nk_, nb_, npw_, md_;
   bool fp32_exp_ = false;
+  bool force_tpa_ = false;       // the round after a rollback preconditions with TPA
+  double repair_thresh_ = 1e-8;  // rank-repair threshold of the expansion rows
   const double* last_eig_ = nullptr;
   int n_restart_ = 0, n_cert_ = 0, n_repair_ = 0, n_rollback_ = 0;
   int64_t n_low_ = 0, n_full_ = 0, n_apply_calls_ = 0;

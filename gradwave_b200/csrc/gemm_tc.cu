@@ -32,13 +32,16 @@
 // (K-major: 8-row atoms of 64 B; MN-major: 8 K-rows of 32 MN elements).
 // Thread 0 issues the loads, thread 32 the MMAs;
 // the four warps then read their 32 TMEM lanes each for the epilogue. Every
-// mbarrier wait is bounded (about two seconds of SM clock); a wait that runs
-// out ORs GWB_ERR_TIMEOUT (4) into *status and the CTA goes to its clean-up,
-// which always releases its TMEM.
+// mbarrier wait is bounded (by default about two seconds of SM clock;
+// gwb_tc_set_wait_limit changes it); a wait that runs out ORs
+// GWB_ERR_TIMEOUT (4) into *status and the CTA goes to its clean-up: the
+// producer first waits (bounded) until every TMA box it issued has landed,
+// all threads wait for the committed MMAs, and the TMEM is always released.
 #include <cuda.h>  // CUtensorMap and its enums (types only; the encoder is fetched from the driver at run time)
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
 #include "common.cuh"
@@ -60,7 +63,7 @@ constexpr int TC_B_BYTES = 32768;                  // B: 4 planes x 32 x 128 BF1
 constexpr int TC_STAGE_BYTES = TC_A_BYTES + TC_B_BYTES;
 constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024;  // + alignment slack
 constexpr int TC_TMEM_COLS = 2 * TC_N;             // re and im accumulators
-constexpr long long TC_WAIT_CYCLES = 4000000000LL;  // ~2 s at 1.9 GHz
+constexpr long long TC_WAIT_CYCLES = 4000000000LL;  // default wait limit: ~2 s at 1.9 GHz
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -83,10 +86,10 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
 }
 
 // Bounded wait for the phase with the given parity to complete.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
   const long long t0 = clock64();
   while (!mbar_try(bar, parity)) {
-    if (clock64() - t0 > TC_WAIT_CYCLES) return false;
+    if (clock64() - t0 > limit) return false;
   }
   return true;
 }
@@ -153,11 +156,14 @@ struct TcOut {
 };
 
 // One CTA: C tile (mt, nt) of batch entry blockIdx.z over the K steps
-// [kt0, kt1) of this split.
+// [kt0, kt1) of this split. wait_cycles bounds every mbarrier wait.
+// withhold >= 0 is the failure-test hook of gwb_tc_test_withhold: the
+// producer issues no load for that K step of the split, so its consumer's
+// wait must run out.
 template <bool NN>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_zgemm_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int M, int N,
-               int K, int kt_per_split, TcOut out, int* status) {
+               int K, int kt_per_split, TcOut out, int* status, long long wait_cycles, int withhold) {
   __shared__ __align__(8) uint64_t bar_full[TC_STAGES];
   __shared__ __align__(8) uint64_t bar_empty[TC_STAGES];
   __shared__ __align__(8) uint64_t bar_done;
@@ -196,15 +202,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   const uint32_t tmem = tmem_base_slot;
 
   if (tid == 0 && kt1 > kt0) {
-    // producer: TMA boxes of stage s for K step kt
+    // producer: TMA boxes of stage s for K step kt; last_round[s] is the
+    // last round for which stage s was armed (its loads may be in flight)
+    int last_round[TC_STAGES];
+#pragma unroll
+    for (int s = 0; s < TC_STAGES; ++s) last_round[s] = -1;
     for (int kt = kt0; kt < kt1; ++kt) {
       const int i = kt - kt0, s = i % TC_STAGES;
-      if (i >= TC_STAGES && !mbar_wait(smem_u32(&bar_empty[s]), ((i / TC_STAGES) - 1) & 1)) {
+      if (i >= TC_STAGES && !mbar_wait(smem_u32(&bar_empty[s]), ((i / TC_STAGES) - 1) & 1, wait_cycles)) {
         abort_flag = 1;
         atomicOr(status, GWB_ERR_TIMEOUT);
         break;
       }
       if (*(volatile int*)&abort_flag) break;
+      if (i == withhold) continue;
+      last_round[s] = i / TC_STAGES;
       const uint32_t full = smem_u32(&bar_full[s]);
       const uint32_t sa = dsm + s * TC_STAGE_BYTES, sb = sa + TC_A_BYTES;
       mbar_expect_tx(full, TC_STAGE_BYTES);
@@ -219,6 +231,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         tma_load_3d(sb, &mapB, full, k0, n0, 4 * b);
       }
     }
+    // no bulk copy may still be landing in shared memory when the CTA leaves:
+    // wait (bounded) for the last armed phase of every stage. Only this thread
+    // arms the full barriers, so a landed phase r leaves the barrier in phase
+    // r + 1 and the parity test of phase r holds from then on.
+#pragma unroll
+    for (int s = 0; s < TC_STAGES; ++s)
+      if (last_round[s] >= 0 && !mbar_wait(smem_u32(&bar_full[s]), last_round[s] & 1, wait_cycles))
+        atomicOr(status, GWB_ERR_TIMEOUT);
   } else if (tid == 32) {
     // MMA issuer
     constexpr uint32_t ID_POS = idesc(NN, false), ID_NEG = idesc(NN, true);
@@ -231,7 +251,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     constexpr int SA[3] = {0, 0, 1}, SB[3] = {0, 1, 0};  // hi hi, hi lo, lo hi
     for (int kt = kt0; kt < kt1; ++kt) {
       const int i = kt - kt0, s = i % TC_STAGES;
-      if (!mbar_wait(smem_u32(&bar_full[s]), (i / TC_STAGES) & 1)) {
+      if (!mbar_wait(smem_u32(&bar_full[s]), (i / TC_STAGES) & 1, wait_cycles)) {
         abort_flag = 1;
         atomicOr(status, GWB_ERR_TIMEOUT);
         break;
@@ -269,7 +289,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   // are conflict-free) -> whole rows of C, so that the global reads and writes
   // are coalesced
   const bool have = kt1 > kt0;
-  bool ok = have && mbar_wait(smem_u32(&bar_done), 0);
+  bool ok = have && mbar_wait(smem_u32(&bar_done), 0, wait_cycles);
   if (have && !ok) atomicOr(status, GWB_ERR_TIMEOUT);
   if (*(volatile int*)&abort_flag) ok = false;
   ok = __syncthreads_and(ok || !have) != 0;
@@ -525,9 +545,26 @@ int tc_becp_d_planes(int nk, int nb, int nproj, const cplx<double>* becp, const 
   return GWB_OK;
 }
 
+// Wait limit of the pipeline barriers (SM clock cycles) and the
+// failure-test hook (K step whose load is withheld; -1: none), read at launch.
+static std::atomic<long long> g_wait_cycles{TC_WAIT_CYCLES};
+static std::atomic<int> g_withhold{-1};
+
 }  // namespace gwb
 
 using namespace gwb;
+
+extern "C" int gwb_tc_set_wait_limit(int64_t cycles) {
+  GWB_REQUIRE(cycles > 0, "the wait limit must be positive");
+  g_wait_cycles.store((long long)cycles);
+  return GWB_OK;
+}
+
+extern "C" int gwb_tc_test_withhold(int32_t kstep) {
+  GWB_REQUIRE(kstep >= -1, "kstep must be -1 (off) or a K step index");
+  g_withhold.store((int)kstep);
+  return GWB_OK;
+}
 
 extern "C" int gwb_tc_planes(int64_t nk, int64_t rows, int64_t cols, const void* src, int64_t src_ld,
                              int64_t src_kstride, int dtype, int conj, void* planes, int64_t ld, int64_t rows_cap,
@@ -622,10 +659,12 @@ extern "C" int gwb_zgemm_tc(int opB, int64_t M, int64_t N, int64_t K, double alp
   dim3 grid((unsigned)(Mt * Nt), (unsigned)splits, (unsigned)batch);
   if (nn) {
     GWB_CUDA_TRY(allow_smem(k_zgemm_tc<true>));
-    k_zgemm_tc<true><<<grid, TC_THREADS, TC_SMEM, st>>>(mapA, mapB, (int)M, (int)N, (int)K, (int)kps, out, status);
+    k_zgemm_tc<true><<<grid, TC_THREADS, TC_SMEM, st>>>(mapA, mapB, (int)M, (int)N, (int)K, (int)kps, out, status,
+                                                       g_wait_cycles.load(), g_withhold.load());
   } else {
     GWB_CUDA_TRY(allow_smem(k_zgemm_tc<false>));
-    k_zgemm_tc<false><<<grid, TC_THREADS, TC_SMEM, st>>>(mapA, mapB, (int)M, (int)N, (int)K, (int)kps, out, status);
+    k_zgemm_tc<false><<<grid, TC_THREADS, TC_SMEM, st>>>(mapA, mapB, (int)M, (int)N, (int)K, (int)kps, out, status,
+                                                        g_wait_cycles.load(), g_withhold.load());
   }
   GWB_LAUNCH_CHECK();
   count_launches(1);

@@ -72,6 +72,8 @@ struct gwb_ham {
   gwb::cplx<float>* d_p32 = nullptr;
   double* d_d64 = nullptr;
   float* d_d32 = nullptr;
+  double* d_q64 = nullptr;  // augmentation q_pq of the overlap S (USPP/PAW), when set
+  float* d_q32 = nullptr;
   gwb::cplx<double>* d_tw64[3] = {nullptr, nullptr, nullptr};
   gwb::cplx<float>* d_tw32[3] = {nullptr, nullptr, nullptr};
   // scratch
@@ -81,6 +83,8 @@ struct gwb_ham {
   size_t part_bytes = 0;
   void* d_bd = nullptr;  // becp * D
   size_t bd_bytes = 0;
+  void* d_bq = nullptr;  // becp * q (overlap apply)
+  size_t bq_bytes = 0;
   // tensor-core nonlocal term (float32 applies of complex128 blocks)
   void* d_pplanes = nullptr;  // BF16 planes of P: (nk, 4, nproj, ldp)
   size_t pplanes_bytes = 0;
@@ -96,7 +100,7 @@ struct gwb_ham {
   int* d_tcstatus = nullptr;  // pipeline-wait timeouts of the tensor-core products
   double* d_rhok = nullptr;  // density accumulators, one box per k
   size_t rhok_bytes = 0;
-  bool have_t = false, have_v = false, have_p = false;
+  bool have_t = false, have_v = false, have_p = false, have_q = false;
 };
 
 namespace gwb {
@@ -627,6 +631,107 @@ __global__ void __launch_bounds__(256) k_nl_add(const cplx<T>* __restrict__ bd,
   }
 }
 
+// K5 of the generalized apply: one pass over the slice partials gives both
+// bd = becp D (H) and bq = becp q (S). Same fixed-order reduction as K5.
+template <typename T>
+__global__ void __launch_bounds__(128) k_becp_reduce_dq(const cplx<T>* __restrict__ part, const T* __restrict__ D,
+                                                        const T* __restrict__ Q, cplx<T>* __restrict__ bd,
+                                                        cplx<T>* __restrict__ bq, int nk, int nb, int nproj,
+                                                        int nslice) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* becp = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* grp = becp + nproj;
+  const int kb = blockIdx.x;
+  const size_t stride = (size_t)nk * nb * nproj;
+  const int ngrp = max(1, (int)blockDim.x / nproj);
+  for (int idx = threadIdx.x; idx < nproj * ngrp; idx += blockDim.x) {
+    const int p = idx % nproj, gq = idx / nproj;
+    cplx<T> a = mk<T>(0, 0);
+    for (int s = gq; s < nslice; s += ngrp) a = a + part[s * stride + (size_t)kb * nproj + p];
+    grp[gq * nproj + p] = a;
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < nproj; p += blockDim.x) {
+    cplx<T> a = mk<T>(0, 0);
+    for (int gq = 0; gq < ngrp; ++gq) a = a + grp[gq * nproj + p];
+    becp[p] = a;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < nproj; q += blockDim.x) {
+    cplx<T> a = mk<T>(0, 0), b = mk<T>(0, 0);
+    for (int p = 0; p < nproj; ++p) {
+      a = a + scale(becp[p], D[(size_t)p * nproj + q]);
+      b = b + scale(becp[p], Q[(size_t)p * nproj + q]);
+    }
+    bd[(size_t)kb * nproj + q] = a;
+    bq[(size_t)kb * nproj + q] = b;
+  }
+}
+
+// K6 of the generalized apply: each projector tile is read once for both
+// outputs, out_h += bd P and out_s = (c + bq P) on the sphere, 0 in the
+// padding (the overlap's mask).
+template <typename T, typename SIO>
+__global__ void __launch_bounds__(256) k_nl_add_hs(const cplx<T>* __restrict__ bd, const cplx<T>* __restrict__ bq,
+                                                   const cplx<T>* __restrict__ P, const SIO* __restrict__ c,
+                                                   int64_t ck, SIO* __restrict__ out_h, int64_t ohk,
+                                                   SIO* __restrict__ out_s, int64_t osk,
+                                                   const int* __restrict__ npw_k, int nk, int nb, int nproj,
+                                                   int npw_max) {
+  constexpr int TGO = 64, TQ = 16;
+  __shared__ cplx<T> sb[NL_TB][TQ];
+  __shared__ cplx<T> sq[NL_TB][TQ];
+  __shared__ cplx<T> sp[TQ][TGO];
+  const int gt = blockIdx.x, bt = blockIdx.y, k = blockIdx.z;
+  const int tid = threadIdx.x;
+  const int lg = tid % TGO, lb0 = tid / TGO;
+  const int gi_o = gt * TGO + lg;
+  const bool on_sphere = gi_o < npw_k[k];
+  cplx<T> ah[4], as[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int b = bt * NL_TB + lb0 * 4 + i;
+    const bool ok = gi_o < npw_max && b < nb;
+    ah[i] = ok ? ld<T>(out_h, (size_t)k * ohk + (size_t)b * npw_max + gi_o) : mk<T>(0, 0);
+    as[i] = (ok && on_sphere) ? ld<T>(c, (size_t)k * ck + (size_t)b * npw_max + gi_o) : mk<T>(0, 0);
+  }
+  for (int q0 = 0; q0 < nproj; q0 += TQ) {
+    for (int i = tid; i < NL_TB * TQ; i += blockDim.x) {
+      const int bb = i / TQ, qq = i % TQ;
+      const int b = bt * NL_TB + bb, q = q0 + qq;
+      const bool ok = b < nb && q < nproj;
+      sb[bb][qq] = ok ? bd[((size_t)k * nb + b) * nproj + q] : mk<T>(0, 0);
+      sq[bb][qq] = ok ? bq[((size_t)k * nb + b) * nproj + q] : mk<T>(0, 0);
+    }
+    for (int i = tid; i < TQ * TGO; i += blockDim.x) {
+      const int qq = i / TGO, gg = i % TGO;
+      const int q = q0 + qq, gi = gt * TGO + gg;
+      sp[qq][gg] = (q < nproj && gi < npw_max) ? P[((size_t)k * nproj + q) * npw_max + gi] : mk<T>(0, 0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int qq = 0; qq < TQ; ++qq) {
+      const cplx<T> pv = sp[qq][lg];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        ah[i] = ah[i] + sb[lb0 * 4 + i][qq] * pv;
+        as[i] = as[i] + sq[lb0 * 4 + i][qq] * pv;
+      }
+    }
+    __syncthreads();
+  }
+  if (gi_o < npw_max) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int b = bt * NL_TB + lb0 * 4 + i;
+      if (b < nb) {
+        st(out_h, (size_t)k * ohk + (size_t)b * npw_max + gi_o, ah[i]);
+        st(out_s, (size_t)k * osk + (size_t)b * npw_max + gi_o, on_sphere ? as[i] : mk<T>(0, 0));
+      }
+    }
+  }
+}
+
 template <typename T> __global__ void k_scale_copy(const double* src, T* dst, size_t n, double s) {
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i < n) dst[i] = (T)(src[i] * s);
@@ -775,8 +880,9 @@ static int nonlocal_tc(gwb_ham* h, const cplx<double>* c, int64_t ck, cplx<doubl
                       nk, nullptr, 0, h->d_tcstatus, st);
 }
 
+// out = T c + local(c): the kinetic and FFT local terms, band chunks sized to L2.
 template <typename T, typename SIO>
-static int apply_impl(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t ok, int nb, cudaStream_t st) {
+static int local_term(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t ok, int nb, cudaStream_t st) {
   const FftGeom& g = h->g;
   const size_t es = sizeof(cplx<T>);
   const size_t plane_elems = (size_t)g.n[1] * g.n[2];
@@ -789,7 +895,6 @@ static int apply_impl(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t ok
   if (nbc < 1) nbc = 1;
   int rc = ensure_buf(&h->d_W, &h->W_bytes, per_band * nbc);
   if (rc) return rc;
-  const bool dbl = sizeof(T) == 8;
   const size_t smA = plane_smem(g, es), smB = pencil_smem(g, es);
   const unsigned c0 = g.plan[0].code, c1 = g.plan[1].code, c2 = g.plan[2].code;
   const bool cubic = c0 == c1 && c1 == c2;
@@ -799,18 +904,33 @@ static int apply_impl(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t ok
   else if (cubic && c0 == kCode72) rcl = local_chunks<T, SIO, kCode72>(h, c, ck, out, ok, nb, nbc, st, smA, smB);
   else if (cubic && c0 == kCode96) rcl = local_chunks<T, SIO, kCode96>(h, c, ck, out, ok, nb, nbc, st, smA, smB);
   else rcl = local_chunks<T, SIO, 0u>(h, c, ck, out, ok, nb, nbc, st, smA, smB);
-  if (rcl) return rcl;
+  return rcl;
+}
+
+// The nonlocal slices: enough G slices to fill the GPU for this band count.
+template <typename T>
+static int nl_geometry(gwb_ham* h, int nb, int* gslice, int* nsl) {
+  const int ns = nl_slices(h, nb);
+  *gslice = ((h->npw_max + ns - 1) / ns + NL_TG - 1) / NL_TG * NL_TG;
+  *nsl = (h->npw_max + *gslice - 1) / *gslice;
+  const size_t es = sizeof(cplx<T>);
+  int rc = ensure_buf(&h->d_part, &h->part_bytes, (size_t)*nsl * h->nk * nb * h->nproj * es);
+  if (rc) return rc;
+  return ensure_buf(&h->d_bd, &h->bd_bytes, (size_t)h->nk * nb * h->nproj * es);
+}
+
+template <typename T, typename SIO>
+static int apply_impl(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t ok, int nb, cudaStream_t st) {
+  const size_t es = sizeof(cplx<T>);
+  const bool dbl = sizeof(T) == 8;
+  int rc = local_term<T, SIO>(h, c, ck, out, ok, nb, st);
+  if (rc) return rc;
   if constexpr (std::is_same<T, float>::value && std::is_same<SIO, cplx<double>>::value) {
     if (h->nproj > 0 && tc_nonlocal_enabled(h)) return nonlocal_tc(h, c, ck, out, ok, nb, st);
   }
   if (h->nproj > 0) {
-    const int ns = nl_slices(h, nb);
-    const int gslice = ((h->npw_max + ns - 1) / ns + NL_TG - 1) / NL_TG * NL_TG;
-    const int nsl = (h->npw_max + gslice - 1) / gslice;
-    rc = ensure_buf(&h->d_part, &h->part_bytes, (size_t)nsl * h->nk * nb * h->nproj * es);
-    if (rc) return rc;
-    rc = ensure_buf(&h->d_bd, &h->bd_bytes, (size_t)h->nk * nb * h->nproj * es);
-    if (rc) return rc;
+    int gslice = 0, nsl = 0;
+    if ((rc = nl_geometry<T>(h, nb, &gslice, &nsl))) return rc;
     const cplx<T>* P = dbl ? (const cplx<T>*)h->d_p64 : (const cplx<T>*)h->d_p32;
     const T* D = dbl ? (const T*)h->d_d64 : (const T*)h->d_d32;
     dim3 g4((h->nproj + NL_TP - 1) / NL_TP, (nb + NL_TB - 1) / NL_TB, h->nk * nsl);
@@ -826,6 +946,37 @@ static int apply_impl(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t ok
   return GWB_OK;
 }
 
+
+// Generalized apply: out_h = H c and out_s = S c = (c + sum_pq |p> q_pq <q|c>)
+// masked, from one becp contraction (CUDA cores, every precision).
+template <typename T, typename SIO>
+static int apply_hs_impl(gwb_ham* h, const SIO* c, int64_t ck, SIO* out_h, int64_t ohk, SIO* out_s, int64_t osk,
+                         int nb, cudaStream_t st) {
+  const size_t es = sizeof(cplx<T>);
+  const bool dbl = sizeof(T) == 8;
+  int rc = local_term<T, SIO>(h, c, ck, out_h, ohk, nb, st);
+  if (rc) return rc;
+  const cplx<T>* P = dbl ? (const cplx<T>*)h->d_p64 : (const cplx<T>*)h->d_p32;
+  if (h->nproj > 0) {
+    int gslice = 0, nsl = 0;
+    if ((rc = nl_geometry<T>(h, nb, &gslice, &nsl))) return rc;
+    if ((rc = ensure_buf(&h->d_bq, &h->bq_bytes, (size_t)h->nk * nb * h->nproj * es))) return rc;
+    const T* D = dbl ? (const T*)h->d_d64 : (const T*)h->d_d32;
+    const T* Q = dbl ? (const T*)h->d_q64 : (const T*)h->d_q32;
+    dim3 g4((h->nproj + NL_TP - 1) / NL_TP, (nb + NL_TB - 1) / NL_TB, h->nk * nsl);
+    k_becp_partial<T, SIO><<<g4, 256, 0, st>>>(c, P, (cplx<T>*)h->d_part, h->nk, nb, h->nproj, h->npw_max, gslice, ck);
+    const int ngrp = std::max(1, 128 / h->nproj);
+    k_becp_reduce_dq<T><<<h->nk * nb, 128, (size_t)h->nproj * (1 + ngrp) * es, st>>>(
+        (const cplx<T>*)h->d_part, D, Q, (cplx<T>*)h->d_bd, (cplx<T>*)h->d_bq, h->nk, nb, h->nproj, nsl);
+    count_launches(2);
+  }
+  dim3 g6((h->npw_max + 63) / 64, (nb + NL_TB - 1) / NL_TB, h->nk);
+  k_nl_add_hs<T, SIO><<<g6, 256, 0, st>>>((const cplx<T>*)h->d_bd, (const cplx<T>*)h->d_bq, P, c, ck, out_h, ohk,
+                                          out_s, osk, h->d_npw, h->nk, nb, h->nproj, h->npw_max);
+  GWB_LAUNCH_CHECK();
+  count_launches(1);
+  return GWB_OK;
+}
 
 // Density of nb bands (float64 FFTs): K1 per band chunk into W, then the
 // pencil kernel accumulating w |psi|^2 into rho_k, finally the k sum.
@@ -1036,7 +1187,7 @@ int gwb_ham_create(const gwb_ham_geometry* geom, int device, gwb_ham** out) {
 int gwb_ham_destroy(gwb_ham* h) {
   if (!h) return GWB_OK;
   void* ptrs[] = {h->d_npw, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos, h->d_t64, h->d_t32, h->d_v64,
-                  h->d_v32, h->d_p64, h->d_p32, h->d_d64, h->d_d32, h->d_W, h->d_part, h->d_bd,
+                  h->d_v32, h->d_p64, h->d_p32, h->d_d64, h->d_d32, h->d_q64, h->d_q32, h->d_W, h->d_part, h->d_bd, h->d_bq,
                   h->d_pplanes, h->d_cplanes, h->d_becp, h->d_bdplanes, h->d_tcwork, h->d_tcstatus, h->d_rhok,
                   h->d_tw64[0], h->d_tw64[1], h->d_tw64[2], h->d_tw32[0], h->d_tw32[1], h->d_tw32[2]};
   for (void* p : ptrs)
@@ -1126,6 +1277,56 @@ int gwb_ham_apply(gwb_ham* h, const void* c, void* out, int32_t nb, int32_t io_d
   return gwb_ham_apply_strided(h, c, ks, out, ks, nb, io_dtype, prec, stream);
 }
 
+int gwb_ham_set_overlap(gwb_ham* h, const double* q, void* stream) {
+  GWB_REQUIRE(h, "null handle");
+  GWB_REQUIRE(h->have_p, "projectors must be set before the overlap");
+  if (h->nproj == 0) {
+    h->have_q = true;
+    return GWB_OK;
+  }
+  GWB_REQUIRE(q, "null overlap pointer");
+  GWB_CUDA_TRY(cudaSetDevice(h->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t nd = (size_t)h->nproj * h->nproj;
+  if (!h->d_q64) {
+    GWB_CUDA_TRY(cudaMalloc((void**)&h->d_q64, nd * 8));
+    GWB_CUDA_TRY(cudaMalloc((void**)&h->d_q32, nd * 4));
+  }
+  GWB_CUDA_TRY(cudaMemcpyAsync(h->d_q64, q, nd * 8, cudaMemcpyDeviceToDevice, st));
+  k_scale_copy<float><<<blocks_for(nd, 256), 256, 0, st>>>(q, h->d_q32, nd, 1.0);
+  GWB_LAUNCH_CHECK();
+  h->have_q = true;
+  return GWB_OK;
+}
+
+int gwb_ham_apply_hs(gwb_ham* h, const void* c, int64_t c_kstride, void* out_h, int64_t oh_kstride, void* out_s,
+                     int64_t os_kstride, int32_t nb, int32_t io_dtype, int32_t prec, void* stream) {
+  GWB_REQUIRE(h && c && out_h && out_s, "null argument");
+  GWB_REQUIRE(nb >= 0, "nb < 0");
+  GWB_REQUIRE(h->have_t && h->have_v && h->have_p, "kinetic, potential and projectors must be set first");
+  GWB_REQUIRE(h->have_q, "the overlap (gwb_ham_set_overlap) must be set first");
+  GWB_REQUIRE(io_dtype == GWB_C64 || io_dtype == GWB_C128, "io_dtype must be GWB_C64 or GWB_C128");
+  GWB_REQUIRE(prec == GWB_FP32 || prec == GWB_FP64, "prec must be GWB_FP32 or GWB_FP64");
+  GWB_REQUIRE(c != out_h && c != out_s && out_h != out_s, "c, out_h and out_s must not overlap");
+  const int64_t row = (int64_t)nb * h->npw_max;
+  GWB_REQUIRE(c_kstride >= row && oh_kstride >= row && os_kstride >= row, "k stride smaller than nb * npw_max");
+  if (nb == 0) return GWB_OK;
+  GWB_CUDA_TRY(cudaSetDevice(h->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  if (io_dtype == GWB_C128) {
+    auto* ci = (const cplx<double>*)c;
+    auto* oh = (cplx<double>*)out_h;
+    auto* os = (cplx<double>*)out_s;
+    return prec == GWB_FP64 ? apply_hs_impl<double>(h, ci, c_kstride, oh, oh_kstride, os, os_kstride, nb, st)
+                            : apply_hs_impl<float>(h, ci, c_kstride, oh, oh_kstride, os, os_kstride, nb, st);
+  }
+  auto* ci = (const cplx<float>*)c;
+  auto* oh = (cplx<float>*)out_h;
+  auto* os = (cplx<float>*)out_s;
+  return prec == GWB_FP64 ? apply_hs_impl<double>(h, ci, c_kstride, oh, oh_kstride, os, os_kstride, nb, st)
+                          : apply_hs_impl<float>(h, ci, c_kstride, oh, oh_kstride, os, os_kstride, nb, st);
+}
+
 int gwb_ham_density(gwb_ham* h, const void* c, int64_t c_kstride, int32_t nb, int32_t io_dtype,
                     const double* weights, int64_t w_kstride, double scale, double* rho, void* stream) {
   GWB_REQUIRE(h && c && weights && rho, "null argument");
@@ -1141,7 +1342,7 @@ int gwb_ham_density(gwb_ham* h, const void* c, int64_t c_kstride, int32_t nb, in
 }
 
 size_t gwb_ham_scratch_bytes(const gwb_ham* h) {
-  return h ? h->W_bytes + h->part_bytes + h->bd_bytes + h->pplanes_bytes + h->cplanes_bytes + h->becp_bytes +
+  return h ? h->W_bytes + h->part_bytes + h->bd_bytes + h->bq_bytes + h->pplanes_bytes + h->cplanes_bytes + h->becp_bytes +
                  h->bdplanes_bytes + h->tcwork_bytes + h->rhok_bytes
            : 0;
 }

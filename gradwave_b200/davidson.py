@@ -627,38 +627,28 @@ class _Solver:
 
 def _native_solve(ham, x0, t, mask, tol, max_iter, max_dim, mode, time_applies=False, model=None
                   ) -> BatchedDavidsonResult | None:
-    """The whole solve inside libgwb.so (``gwb_davidson_solve``); None when the
-    library reports a breakdown it does not repair (the host driver retries)."""
-    import ctypes
-    nk, nb, npw = (int(s) for s in x0.shape)
-    dev = x0.device
-    p = _lib.DavidsonParams(nk, nb, npw, max_dim, int(max_iter), {"fp64": 0, "fp32exp": 1, "mixed": 2}[mode],
-                            0 if model is None else 1, 1 if time_applies else 0, float(tol), float(t.max()))
-    nbytes = ctypes.c_size_t()
-    _lib.call("gwb_davidson_workspace_bytes", ctypes.byref(p), ctypes.byref(nbytes))
-    ws = ham._native_workspace(int(nbytes.value))
-    x0c = x0.contiguous()
-    tc = t.to(dev, torch.float64).contiguous()
-    mk = mask.to(dev, torch.uint8).contiguous()
-    eig = torch.empty(nk, nb, dtype=torch.float64, device=dev)
-    vec = torch.empty(nk, nb, npw, dtype=torch.complex128, device=dev)
-    rn = torch.empty(nk, nb, dtype=torch.float64, device=dev)
-    st = _lib.DavidsonStats()
-    status = _lib.load().gwb_davidson_solve(ham._h, ctypes.byref(p), None if model is None else model.data_ptr(),
-                                            x0c.data_ptr(), tc.data_ptr(),
-                                            mk.data_ptr(), ws.data_ptr(), ws.numel(), eig.data_ptr(),
-                                            vec.data_ptr(), rn.data_ptr(), ctypes.byref(st), _lib.stream_ptr(dev))
-    if status == _lib.GWB_ERR_BREAKDOWN:
-        logger.debug("native Davidson: %s; retrying on the host driver", _lib.load().gwb_last_error().decode())
-        return None
-    _lib.check(status)
-    n_rows = st.n_apply_low + st.n_apply_full
-    ham._count_rows(n_rows)
-    info = {"n_restart": st.n_restart, "n_cert": st.n_cert, "n_repair": st.n_repair, "n_rollback": st.n_rollback,
-            "max_dim": max_dim, "native": True, "n_apply_calls": int(st.n_apply_calls)}
+    """The whole solve inside libgwb.so (``gwb_davidson_solve`` through the
+    custom op ``gwb::davidson_solve``); None when the library reports a
+    breakdown it does not repair (the host driver retries)."""
+    from .ops import SOLVE_MODES, SOLVE_STATS, SOLVE_TIME_APPLIES
+    try:
+        eig, vec, rn, stats = torch.ops.gwb.davidson_solve(
+            ham.handle, x0.contiguous(), t, mask, float(tol), int(max_iter), int(max_dim), SOLVE_MODES[mode],
+            SOLVE_TIME_APPLIES if time_applies else 0, model)
+    except Exception as e:  # the dispatcher may re-wrap the library's GwbError
+        if getattr(e, "status", None) == _lib.GWB_ERR_BREAKDOWN or f"libgwb status {_lib.GWB_ERR_BREAKDOWN} " in str(e):
+            logger.debug("native Davidson: %s; retrying on the host driver", e)
+            return None
+        raise
+    st = dict(zip(SOLVE_STATS, stats.tolist()))
+    n_low, n_full = int(st["n_apply_low"]), int(st["n_apply_full"])
+    ham._count_rows(n_low + n_full)
+    info = {"n_restart": int(st["n_restart"]), "n_cert": int(st["n_cert"]), "n_repair": int(st["n_repair"]),
+            "n_rollback": int(st["n_rollback"]), "max_dim": max_dim, "native": True,
+            "n_apply_calls": int(st["n_apply_calls"]), "n_tpa_fallback": int(st["n_tpa_fallback"])}
     if time_applies:
-        info["apply_ms"] = float(st.apply_ms)
-    return BatchedDavidsonResult(eig, vec, int(st.n_iter), rn, int(st.n_apply_low), int(st.n_apply_full), info)
+        info["apply_ms"] = float(st["apply_ms"])
+    return BatchedDavidsonResult(eig, vec, int(st["n_iter"]), rn, n_low, n_full, info)
 
 
 _TC_STEP_NAMES = ("nh", "nn", "chol")
@@ -836,6 +826,8 @@ def davidson_batched(h_apply, x0, t, mask, tol: float = 1e-9, max_iter: int = 40
                                  precond=precond)
             if res is not None:
                 return res
+        if not bool(torch.isfinite(torch.view_as_real(x0) if x0.is_complex() else x0).all()):
+            raise _lib.GwbError(_lib.GWB_ERR_NONFINITE, "the start block holds a non-finite value")
         return _Solver(h_apply, x0, t, mask, tol, max_iter, max_dim_factor, mode, precond, history_out).run()
 
 

@@ -186,7 +186,20 @@ class GammaHamiltonian:
         self.t_phi = kinetic_phi(gb).to(dev)
         self._work = None
         self.n_apply = 0
+        self.timing: list | None = None   # (start event, end event, bands, prec) per apply when a list
         assert nhalf * 2 - 1 == npw
+
+    def apply_times(self) -> dict:
+        """Totals of the applies recorded since ``timing`` was set to a list
+        (call after the stream has been synchronised): launches, milliseconds
+        and real bands, per arithmetic precision."""
+        out = {"calls": 0, "ms": 0.0, "bands": 0, "bands_fp32": 0, "bands_fp64": 0}
+        for e0, e1, nb, prec in self.timing or []:
+            out["calls"] += 1
+            out["ms"] += e0.elapsed_time(e1)
+            out["bands"] += nb
+            out["bands_fp32" if prec == _lib.GWB_FP32 else "bands_fp64"] += nb
+        return out
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -209,10 +222,17 @@ class GammaHamiltonian:
         need = int(_lib.load().gwb_gamma_work_bytes(nb, self.gb.npw))
         if self._work is None or self._work.numel() < need:
             self._work = torch.empty(need, dtype=torch.uint8, device=self.device)
+        ev = None
+        if self.timing is not None:
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            ev[0].record()
         _lib.call("gwb_gamma_apply", self._h, nb, self.gb.nhalf, self.gb.npw, phi.data_ptr(), phi.shape[1],
                   out.data_ptr(), out.shape[1], self.src_half.data_ptr(), self.conj_full.data_ptr(),
                   self.rep_full.data_ptr(), self.partner_rep.data_ptr(), prec, self._work.data_ptr(),
                   self._work.numel(), _lib.stream_ptr(self.device))
+        if ev is not None:
+            ev[1].record()
+            self.timing.append((ev[0], ev[1], nb, prec))
         nphi = 2 * self.gb.nhalf - 1
         if out.shape[1] > nphi:  # padded rows (the solver's even width) keep their pad at zero
             out[:, nphi:] = 0.0

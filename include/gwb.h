@@ -107,6 +107,20 @@ int gwb_ham_apply(gwb_ham* h, const void* c, void* out, int32_t nb, int32_t io_d
 int gwb_ham_apply_strided(gwb_ham* h, const void* c, int64_t c_kstride, void* out, int64_t out_kstride,
                           int32_t nb, int32_t io_dtype, int32_t prec, void* stream);
 
+/* Augmentation matrix q (nproj*nproj float64, real symmetric, device) of the
+ * overlap S = 1 + sum_pq |beta_p> q_pq <beta_q| (USPP/PAW). Set after the
+ * projectors. Replaces q_full of gradwave scf/uspp_batch.py:34-45
+ * (BatchedHS.__init__). */
+int gwb_ham_set_overlap(gwb_ham* h, const double* q, void* stream);
+
+/* out_h = H c and out_s = S c in one pass (the projector contraction
+ * <beta|c> is formed once and feeds both the D and the q terms; padded slots
+ * of both outputs are 0). Strides as in gwb_ham_apply_strided; c, out_h and
+ * out_s must not overlap. Replaces gradwave scf/uspp_batch.py:56-73
+ * (BatchedHS.h and BatchedHS.s applied to the same block). */
+int gwb_ham_apply_hs(gwb_ham* h, const void* c, int64_t c_kstride, void* out_h, int64_t oh_kstride, void* out_s,
+                     int64_t os_kstride, int32_t nb, int32_t io_dtype, int32_t prec, void* stream);
+
 /* Electron density on the box: rho[r] = scale * sum_k sum_b weights[k*w_kstride + b]
  * |psi_kb(r)|^2 with psi_kb(r) = sum_G c_kb(G) exp(iG.r) (the unnormalised
  * inverse FFT of the sphere coefficients; padded slots of c must be zero, as
@@ -201,6 +215,16 @@ int gwb_tc_planes(int64_t nk, int64_t rows, int64_t cols, const void* src, int64
  * expansion block, gradwave solvers/davidson.py:428-432; no counterpart in
  * the reference's precision choices (it has float64 and float32 only). */
 int64_t gwb_zgemm_tc_work_bytes(int opB, int64_t M, int64_t N, int64_t K, int64_t batch);
+/* Limit (SM clock cycles, default 4e9, about two seconds) of every mbarrier
+ * wait in the tensor-core products, read at each launch; a wait that runs out
+ * reports GWB_ERR_TIMEOUT through *status, after the CTA has waited (bounded)
+ * for its issued bulk copies and MMAs. No counterpart in the reference. */
+int gwb_tc_set_wait_limit(int64_t cycles);
+/* Failure-test hook: with kstep >= 0 every later gwb_zgemm_tc launch issues no
+ * load for K step kstep of its split, so that step's consumer wait runs out
+ * (GWB_ERR_TIMEOUT) without a fault; -1 turns it off. For the tests of the
+ * bounded waits only. No counterpart in the reference. */
+int gwb_tc_test_withhold(int32_t kstep);
 int gwb_zgemm_tc(int opB, int64_t M, int64_t N, int64_t K, double alpha_re, double alpha_im, const void* A_planes,
                  int64_t lda, int64_t a_rows_cap, const void* B_planes, int64_t ldb, int64_t b_rows_cap,
                  double beta_re, double beta_im, void* C, int64_t ldc, int64_t strideC, int64_t batch, void* work,
@@ -339,6 +363,7 @@ typedef struct {
   double max_residual;
   double apply_ms;                    /* device time of the H applies (timing flag only) */
   int64_t n_apply_calls;              /* gwb_ham_apply launches of the solve */
+  int64_t n_tpa_fallback;             /* (k, band) pairs the learned preconditioner's stall rule sent to TPA */
 } gwb_davidson_stats;
 
 /* Device workspace the solve needs (bytes, 256-byte aligned base). */

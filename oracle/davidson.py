@@ -63,8 +63,11 @@ def orthonormalize_b(v, mask, against=None):
     return q
 
 
-def davidson_batched(h_apply, x0, t, mask, tol=1e-9, max_iter=40, max_dim_factor=4,
-                     keep_history=False) -> OracleResult:
+def davidson_rounds(h_apply, x0, t, mask, tol=1e-9, max_iter=40, max_dim_factor=4, keep_history=False):
+    """The solve as a generator: yields ``(it, eig, rn)`` after every
+    Rayleigh-Ritz round (the point where the reference appends to its
+    ``history_out``, ``solvers/davidson.py:688-690``) and returns the
+    ``OracleResult``. A caller can time the rounds one by one."""
     x0 = np.asarray(x0, dtype=np.complex128)
     t = np.asarray(t, dtype=np.float64)
     mask = np.asarray(mask, dtype=bool)
@@ -89,18 +92,20 @@ def davidson_batched(h_apply, x0, t, mask, tol=1e-9, max_iter=40, max_dim_factor
         w, u = np.linalg.eigh(s)
         u = u[:, :, :nb]
         eig = w[:, :nb].real
-        x = np.einsum("kja,kjg->kag", u, v)
-        hx = np.einsum("kja,kjg->kag", u, hv)
+        ut = np.ascontiguousarray(np.swapaxes(u, 1, 2))
+        x = ut @ v                                   # x_a = sum_j u_ja v_j
+        hx = ut @ hv
         r = hx - eig[..., None] * x
         rn = np.linalg.norm(r, axis=-1)
         if keep_history:
             history.append((it, rn.copy(), eig.copy()))
+        yield it, eig, rn
         if rn.max() < tol:
             return OracleResult(eig, x, it, rn, n_apply, history)
         n_add = int((rn > tol).sum(axis=1).max())
         sel = np.argsort(-rn, axis=1, kind="stable")[:, :n_add]
         r_sel = np.take_along_axis(r, sel[..., None], axis=1)
-        t_band = np.einsum("kbg,kg,kbg->kb", np.conj(x), t, x).real
+        t_band = ((x.real ** 2 + x.imag ** 2) * t[:, None, :]).sum(axis=-1)   # <x|T|x>
         d = teter_b(r_sel, t, np.take_along_axis(t_band, sel, axis=1))
         dn = np.linalg.norm(d, axis=-1, keepdims=True)
         d = np.where(dn > 1e-300, d / np.maximum(dn, 1e-300), d)
@@ -116,6 +121,17 @@ def davidson_batched(h_apply, x0, t, mask, tol=1e-9, max_iter=40, max_dim_factor
             v = np.concatenate([v, d], axis=1)
             hv = np.concatenate([hv, H(d)], axis=1)
     return OracleResult(eig, x, max_iter, rn, n_apply, history)
+
+
+def davidson_batched(h_apply, x0, t, mask, tol=1e-9, max_iter=40, max_dim_factor=4,
+                     keep_history=False) -> OracleResult:
+    gen = davidson_rounds(h_apply, x0, t, mask, tol=tol, max_iter=max_iter, max_dim_factor=max_dim_factor,
+                          keep_history=keep_history)
+    while True:
+        try:
+            next(gen)
+        except StopIteration as stop:
+            return stop.value
 
 
 def band_energy(eig: np.ndarray, kweights: np.ndarray, nocc: int) -> float:

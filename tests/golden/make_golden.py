@@ -22,7 +22,8 @@ What is recorded, per case:
   * generalized USPP/PAW solve: ``BatchedHS.s`` and ``davidson_gen_batched``
     (``scf/uspp_batch.py``) with a synthetic augmentation matrix q.
 
-Usage: python tests/golden/make_golden.py [small|big|all|density|gamma|uspp] [--ref /path/to/gradwave/src]
+Usage: python tests/golden/make_golden.py [small|big|all|density|gamma|uspp] --ref <gradwave>/src
+       (or set GWB_REFERENCE_SRC instead of --ref)
 """
 
 from __future__ import annotations
@@ -265,8 +266,12 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("which", nargs="?", default="small",
                     choices=["small", "big", "all", "density", "gamma", "uspp"])
-    ap.add_argument("--ref", default="/root/reference/src")
+    ap.add_argument("--ref", default=os.environ.get("GWB_REFERENCE_SRC"),
+                    help="the reference's source directory (the one holding the gradwave package); "
+                         "or set GWB_REFERENCE_SRC")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give --ref or set GWB_REFERENCE_SRC")
     shim(args.ref)
     torch.set_num_threads(os.cpu_count() or 1)
     jobs = []

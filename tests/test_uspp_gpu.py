@@ -58,3 +58,23 @@ def test_generalized_davidson_matches_reference(cuda_device, name):
     d = torch.diagonal(m, dim1=-2, dim2=-1).real
     off = m - torch.diag_embed(torch.diagonal(m, dim1=-2, dim2=-1))
     assert float(off.abs().max()) < 1e-8 * float(d.max())
+
+
+@pytest.mark.parametrize("name", ["si2_fcc", "si8_cubic"])
+def test_fused_hs_apply(cuda_device, name):
+    """gwb_ham_apply_hs: H c from the fused pass equals the plain apply (the
+    same arithmetic in the same order), and S c equals the float64 oracle's
+    overlap apply; float32 arithmetic within its bar."""
+    from oracle.uspp import s_apply
+    g, ci, hs = _hs(name, cuda_device)
+    c = torch.from_numpy(random_block(int(g["seed"]) + 3, ci.bk.nk, 5, ci.bk.npw_max)).to(cuda_device)
+    c = c * hs.mask[:, None, :]
+    h_out, s_out = hs.hs(c)
+    h_ref = hs.h(c)
+    scale = float(h_ref.abs().max())
+    assert float((h_out - h_ref).abs().max()) <= 1e-14 * scale
+    s_ref = s_apply(ci.p.numpy(), g["q"], ci.bk.mask.numpy(), c.cpu().numpy())
+    assert np.abs(s_out.cpu().numpy() - s_ref).max() <= 1e-12 * np.abs(s_ref).max()
+    h32, s32 = hs.hs(c.to(torch.complex64))
+    assert float((h32.to(torch.complex128) - h_ref).abs().max()) <= 3e-6 * scale
+    assert np.abs(s32.cpu().numpy() - s_ref).max() <= 3e-6 * np.abs(s_ref).max()
