@@ -732,6 +732,64 @@ def run_tc(args):
     return 0
 
 
+def run_oz(args):
+    """Float64 products on the int8 tensor cores (Ozaki scheme, ``--slices``)
+    next to cuBLAS DGEMM at the real Davidson shapes of the 216-atom Gamma
+    cell: A B^T with K = 80,798 (subspace / projection coefficients, Gram) and
+    A B with K = the basis (Ritz vectors, projection update); ``--warmup``
+    untimed and ``--steps`` timed calls each (CUDA events), error against the
+    float64 product relative to the operands' row maxima."""
+    import torch
+    from gradwave_b200.oz import OzMatmul, check_status
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device="cpu").manual_seed(0)
+    npw = 80798
+    decay = torch.exp(-torch.linspace(0.0, 8.0, npw, dtype=torch.float64))
+    om = OzMatmul(dev, s=args.slices)
+    out = {"mode": "oz", "slices": args.slices, "shapes": {}}
+
+    def ev(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / max(args.steps, 1)
+
+    for name, (M, N, K, form) in {"nt_512x1920xnpw": (512, 1920, npw, "nt"),
+                                  "nt_gram_512x512xnpw": (512, 512, npw, "nt"),
+                                  "nn_512xnpwx1920": (512, npw, 1920, "nn")}.items():
+        if form == "nt":
+            a = (torch.randn(M, K, dtype=torch.float64, generator=g) * decay).to(dev)
+            b = (torch.randn(N, K, dtype=torch.float64, generator=g) * decay).to(dev)
+            c = torch.empty(M, N, dtype=torch.float64, device=dev)
+            t_oz = ev(lambda: om.nt(a, b, c))
+            ref = a @ b.T
+            t_d = ev(lambda: torch.matmul(a, b.T, out=ref))
+            sc = a.abs().amax(1)[:, None] * b.abs().amax(1)[None, :] * K ** 0.5
+        else:
+            a = torch.randn(M, K, dtype=torch.float64, generator=g).to(dev)
+            b = (torch.randn(K, N, dtype=torch.float64, generator=g) * decay[:N]).to(dev)
+            c = torch.empty(M, N, dtype=torch.float64, device=dev)
+            t_oz = ev(lambda: om.nn(a, b, c))
+            ref = a @ b
+            t_d = ev(lambda: torch.matmul(a, b, out=ref))
+            sc = a.abs() @ b.abs().amax(1, keepdim=True) + 1e-300
+        check_status(dev)
+        flop = 2.0 * M * N * K
+        out["shapes"][name] = {"M": M, "N": N, "K": K, "oz_ms": round(t_oz, 4), "dgemm_ms": round(t_d, 4),
+                               "speedup": round(t_d / t_oz, 3), "oz_tflops_equiv": round(flop / t_oz / 1e9, 1),
+                               "int8_tops_issued": round(flop * args.slices * (args.slices + 1) / 2 / t_oz / 1e9, 1),
+                               "err": float(((c - ref).abs() / sc).max())}
+        del a, b, c, ref
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_gamma(args):
     """The Gamma real path on a Gamma-only cell: ``--warmup`` untimed and one
     wall-timed ``davidson_gamma`` from the identity start on the lowest
@@ -749,8 +807,9 @@ def run_gamma(args):
     x0 = gamma_start(gb, ci.nbands, dev)
     mode = "mixed" if args.solver in ("mixed", "fp32exp", "learned-mixed") else "fp64"
     lock = {"auto": None, "on": True, "off": False}[args.lock]
+    _, pc = _solver_choice(args.solver, dev)
     kw = dict(tol=args.tol, max_iter=300, mode=mode, max_dim_factor=args.max_dim_factor, lock=lock,
-              n_buffer=args.n_buffer or 0)
+              n_buffer=args.n_buffer or 0, precond=pc)
     for _ in range(args.warmup):
         davidson_gamma(gh, x0, **kw)
     torch.cuda.synchronize()
@@ -764,7 +823,8 @@ def run_gamma(args):
            "tol_ev": args.tol, "n_iter": r.n_iter,
            "wall_ms": wall,
            "band_applies": gh.n_apply - n0, "max_residual_ev": float(r.residual_norms.max()),
-           "nhalf": gb.nhalf, "npw": gb.npw}
+           "nhalf": gb.nhalf, "npw": gb.npw, "precond": "teter" if isinstance(pc, str) else "learned",
+           "n_tpa_fallback": r.n_tpa_fallback, "oz": os.environ.get("GWB_OZ", "1") != "0"}
     if r.phase_ms:
         out["phase_ms"] = r.phase_ms
     gold = _golden(args.config)
@@ -810,7 +870,8 @@ def main():
                     help="--mode gamma: lock converged pairs (auto: on in the mixed mode)")
     ap.add_argument("--n-buffer", type=int, default=None,
                     help="Gamma path: buffer bands above the wanted ones (default 32 in the bench line, 0 in --mode gamma)")
-    ap.add_argument("--mode", default="solve", choices=["solve", "apply", "once", "tc", "gamma"],
+    ap.add_argument("--slices", type=int, default=8, help="--mode oz: int8 slices per float64 operand")
+    ap.add_argument("--mode", default="solve", choices=["solve", "apply", "once", "tc", "gamma", "oz"],
                     help="apply: only time Hamiltonian applies; once: a single solve (profiling)")
     ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64"], help="arithmetic of --mode apply")
     ap.add_argument("--solver", default="learned-mixed", choices=["plain", "fp32exp", "mixed", "learned-mixed"],
@@ -820,6 +881,8 @@ def main():
         return run_apply(args)
     if args.mode == "tc":
         return run_tc(args)
+    if args.mode == "oz":
+        return run_oz(args)
     if args.mode == "gamma":
         return run_gamma(args)
     if args.mode == "once":

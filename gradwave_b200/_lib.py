@@ -96,6 +96,11 @@ _SIGNATURES = {
     "gwb_tc_planes": [_I64, _I64, _I64, _P, _I64, _I64, ctypes.c_int, ctypes.c_int, _P, _I64, _I64, _I64, _P],
     "gwb_zgemm_tc_work_bytes": [ctypes.c_int, _I64, _I64, _I64, _I64],
     "gwb_tc_set_wait_limit": [_I64],
+    "gwb_oz_split_rows": [_I, _I64, _I64, _P, _I64, _P, _P, _I64, _I64, _I64, _P, _P],
+    "gwb_oz_split_cols": [_I, _I64, _I64, _P, _I64, _P, _I64, _I64, _I64, _P, _P],
+    "gwb_oz_work_bytes": [_I64, _I64, _I64],
+    "gwb_oz_gemm": [_I, _I64, _I64, _I64, _P, _I64, _I64, _I64, _P, _P, _I64, _I64, _I64, _P, _D, _D, _P, _I64, _P,
+                    _SZ, _P, _P],
     "gwb_tc_test_withhold": [_I],
     "gwb_zgemm_tc": [ctypes.c_int, _I64, _I64, _I64, _D, _D, _P, _I64, _I64, _P, _I64, _I64, _D, _D, _P, _I64, _I64,
                      _I64, _P, ctypes.c_size_t, _P, _P],
@@ -128,7 +133,7 @@ _RESTYPES = {"gwb_last_error": ctypes.c_char_p, "gwb_version": ctypes.c_char_p,
              "gwb_launch_count": ctypes.c_ulonglong,
              "gwb_ham_scratch_bytes": ctypes.c_size_t, "gwb_heev_scratch_doubles": ctypes.c_int64,
              "gwb_precond_learned_work_bytes": ctypes.c_int64, "gwb_zgemm_tc_work_bytes": ctypes.c_int64,
-             "gwb_gamma_work_bytes": ctypes.c_size_t}
+             "gwb_gamma_work_bytes": ctypes.c_size_t, "gwb_oz_work_bytes": ctypes.c_int64}
 
 
 def declared_symbols() -> list[str]:

@@ -37,7 +37,6 @@
 // GWB_ERR_TIMEOUT (4) into *status and the CTA goes to its clean-up: the
 // producer first waits (bounded) until every TMA box it issued has landed,
 // all threads wait for the committed MMAs, and the TMEM is always released.
-#include <cuda.h>  // CUtensorMap and its enums (types only; the encoder is fetched from the driver at run time)
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -45,6 +44,7 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "tcgen05.cuh"
 
 namespace gwb {
 namespace {
@@ -65,56 +65,6 @@ constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024;  // + alignment slack
 constexpr int TC_TMEM_COLS = 2 * TC_N;             // re and im accumulators
 constexpr long long TC_WAIT_CYCLES = 4000000000LL;  // default wait limit: ~2 s at 1.9 GHz
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait for the phase with the given parity to complete.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
-  const long long t0 = clock64();
-  while (!mbar_try(bar, parity)) {
-    if (clock64() - t0 > limit) return false;
-  }
-  return true;
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1,
-                                            int c2) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(
-          dst),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
-      : "memory");
-}
-
-// Shared-memory matrix descriptor (tcgen05 "version 1" format) for the
-// 64-byte swizzle: start address, leading- and stride-dimension byte offsets
-// in 16-byte units, layout type 4 (SWIZZLE_64B) in bits 61-63.
-__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46) | (4ull << 61);
-}
-
 // Instruction descriptor of kind::f16: BF16 A and B, FP32 accumulator,
 // M = 128, N = 128, A K-major, B K-major (NN = false) or MN-major (NN = true).
 __host__ __device__ constexpr uint32_t idesc(bool b_mn, bool negate_a) {
@@ -131,18 +81,9 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b
       : "memory");
 }
 
-__device__ __forceinline__ void mma_commit(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+__device__ __forceinline__ void tmem_ld16f(uint32_t taddr, float (&v)[16]) {
   uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
+  tmem_ld16(taddr, r);
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
@@ -301,8 +242,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     float re[16], im[16];
     __syncwarp();  // the TMEM loads are warp-collective
     if (have) {    // CTA-uniform
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c, re);
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + TC_N + c, im);
+      tmem_ld16f(tmem + ((uint32_t)(warp * 32) << 16) + c, re);
+      tmem_ld16f(tmem + ((uint32_t)(warp * 32) << 16) + TC_N + c, im);
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
     } else {
 #pragma unroll
@@ -468,23 +409,6 @@ __global__ void __launch_bounds__(256) k_becp_d_planes(int nk, int nb, int nproj
   }
 }
 
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(p);
-  });
-  return fn;
-}
-
 // 3-D view of a plane set: (columns, rows, 4 x batch planes); box
 // (32, box_rows, 4): 32 columns (64 B, the swizzle span) of box_rows rows of
 // all four planes of one batch entry, 64-byte swizzled in shared memory.
@@ -549,6 +473,8 @@ int tc_becp_d_planes(int nk, int nb, int nproj, const cplx<double>* becp, const 
 // failure-test hook (K step whose load is withheld; -1: none), read at launch.
 static std::atomic<long long> g_wait_cycles{TC_WAIT_CYCLES};
 static std::atomic<int> g_withhold{-1};
+long long tc_wait_cycles() { return g_wait_cycles.load(); }
+int tc_withhold() { return g_withhold.load(); }
 
 }  // namespace gwb
 

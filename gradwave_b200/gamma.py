@@ -251,6 +251,7 @@ class GammaDavidsonResult:
     n_iter: int
     residual_norms: torch.Tensor  # (nb,)
     phase_ms: dict | None = None  # CUDA-event times per step (GWB_PROFILE=1)
+    n_tpa_fallback: int = 0       # bands the learned preconditioner's stall rule sent to TPA
 
 
 def _orthonormalize(v: torch.Tensor, against: torch.Tensor | None = None) -> torch.Tensor:
@@ -306,27 +307,69 @@ class _TcProjection:
         return t
 
 
-def _project_out(t: torch.Tensor, basis: torch.Tensor) -> torch.Tensor:
-    """t -= (t basis^T) basis, in place (one float64 GEMM pair)."""
+class _Products:
+    """The float64 products of the Gamma solver: cuBLAS DGEMM (through torch)
+    or, with ``oz``, the int8 tensor-core products of ``gradwave_b200.oz``
+    (the Ozaki scheme, 8 slices: float64-level error relative to the rows'
+    maxima). ``nt(a, b)`` = a b^T, ``nn(a, b)`` = a b, ``sub_nn(t, c, b)``:
+    t -= c b in place."""
+
+    def __init__(self, dev=None, oz: bool = False):
+        self.om = None
+        if oz:
+            from .oz import OzMatmul
+            self.om = OzMatmul(dev)
+
+    @staticmethod
+    def _rows(a: torch.Tensor) -> torch.Tensor:
+        return a if a.stride(-1) == 1 else a.contiguous()
+
+    def nt(self, a: torch.Tensor, b: torch.Tensor, same: bool = False) -> torch.Tensor:
+        if self.om is None or a.shape[0] == 0 or b.shape[0] == 0:
+            return a @ b.T
+        a = self._rows(a)
+        b = a if same else self._rows(b)
+        out = torch.empty(a.shape[0], b.shape[0], dtype=torch.float64, device=a.device)
+        return self.om.nt(a, b, out, same=same)
+
+    def nn(self, a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
+        if self.om is None or a.shape[0] == 0 or b.shape[0] == 0:
+            return a @ b
+        a, b = a.contiguous(), self._rows(b)
+        out = torch.empty(a.shape[0], b.shape[1], dtype=torch.float64, device=a.device)
+        return self.om.nn(a, b, out)
+
+    def sub_nn(self, t: torch.Tensor, c: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
+        if self.om is None or t.stride(-1) != 1:
+            return t.addmm_(c, b, alpha=-1.0)
+        self.om.nn(c.contiguous(), self._rows(b), t, alpha=-1.0, beta=1.0)
+        return t
+
+
+_CUBLAS = _Products()
+
+
+def _project_out(t: torch.Tensor, basis: torch.Tensor, mm: _Products = _CUBLAS) -> torch.Tensor:
+    """t -= (t basis^T) basis, in place (one float64 product pair)."""
     if basis.shape[0]:
-        t.addmm_(t @ basis.T, basis, alpha=-1.0)
+        mm.sub_nn(t, mm.nt(t, basis), basis)
     return t
 
 
-def _cholqr(y: torch.Tensor):
+def _cholqr(y: torch.Tensor, mm: _Products = _CUBLAS):
     """Cholesky-QR of the rows of y: L = chol(y y^T), y <- L^-1 y, with the
-    triangular inverse formed once (n x n) and applied as one GEMM. Returns
+    triangular inverse formed once (n x n) and applied as one product. Returns
     None when the Gram matrix is not numerically positive definite (a row kept
     less than 1e-8 of its unit norm)."""
-    L, info = torch.linalg.cholesky_ex(y @ y.T)
+    L, info = torch.linalg.cholesky_ex(mm.nt(y, y, same=True))
     if int(info.max()) != 0 or float(torch.diagonal(L).min()) <= 1e-8:
         return None
     eye = torch.eye(L.shape[0], dtype=L.dtype, device=L.device)
-    return torch.linalg.solve_triangular(L, eye, upper=False) @ y
+    return mm.nn(torch.linalg.solve_triangular(L, eye, upper=False), y)
 
 
 def _expand(t: torch.Tensor, v: torch.Tensor, tcp: _TcProjection | None = None,
-            locked: torch.Tensor | None = None) -> torch.Tensor:
+            locked: torch.Tensor | None = None, mm: _Products = _CUBLAS) -> torch.Tensor:
     """New directions from preconditioned residuals: unit rows, two
     projections against the orthonormal basis v (and the locked rows, which
     are orthogonal to v), then Cholesky-QR; Householder QR dropping rows that
@@ -343,25 +386,25 @@ def _expand(t: torch.Tensor, v: torch.Tensor, tcp: _TcProjection | None = None,
     (it would change the rows by that much)."""
     t = t / torch.linalg.vector_norm(t, dim=1, keepdim=True).clamp_min(1e-300)
     lk = locked if locked is not None else v[:0]
-    _project_out(t, lk)
-    t = tcp.project(t, v) if tcp is not None else _project_out(t, v)
-    _project_out(_project_out(t, lk), v)
-    y = _cholqr(t)
+    _project_out(t, lk, mm)
+    t = tcp.project(t, v) if tcp is not None else _project_out(t, v, mm)
+    _project_out(_project_out(t, lk, mm), v, mm)
+    y = _cholqr(t, mm)
     if y is not None:
-        g = y @ y.T
+        g = mm.nt(y, y, same=True)
         g.diagonal().sub_(1.0)
         if float(g.abs().max()) < 1e-13:
             return y
-        y2 = _cholqr(y)
+        y2 = _cholqr(y, mm)
         if y2 is not None:
             return y2
     q, r = torch.linalg.qr(t.T, mode="reduced")
     t = q.T[r.diagonal().abs() > 1e-8]
     if t.shape[0] == 0:
         return t
-    _project_out(_project_out(t, lk), v)
+    _project_out(_project_out(t, lk, mm), v, mm)
     q, _ = torch.linalg.qr(t.T, mode="reduced")
-    return q.T
+    return q.T.contiguous()
 
 
 def _teter(residual: torch.Tensor, t_g: torch.Tensor, t_band: torch.Tensor) -> torch.Tensor:
@@ -370,6 +413,64 @@ def _teter(residual: torch.Tensor, t_g: torch.Tensor, t_band: torch.Tensor) -> t
     x2 = x * x
     num = 27.0 + 18.0 * x + 12.0 * x2 + 8.0 * x2 * x
     return residual * (num / (num + 16.0 * x2 * x2))
+
+
+def _half_rows(phi: torch.Tensor, nhalf: int) -> torch.Tensor:
+    """Embedded real rows -> half-sphere complex rows scaled by sqrt(w_G):
+    c'_0 = phi_0, c'_G = phi_2G-1 + i phi_2G (w_G = 2 off G = 0). Their plain
+    sums over the half sphere are the full-sphere sums, so a kernel that reads
+    complex rows (the band's kinetic energy, residual amplitudes) sees the
+    same numbers as on the full sphere."""
+    c = torch.empty(phi.shape[0], nhalf, dtype=torch.complex128, device=phi.device)
+    c[:, 0] = phi[:, 0]
+    c[:, 1:] = torch.complex(phi[:, 1:2 * nhalf - 1:2], phi[:, 2:2 * nhalf - 1:2])
+    return c
+
+
+def _embed_rows(c: torch.Tensor, npad: int) -> torch.Tensor:
+    """Inverse of ``_half_rows`` (zero pad column(s))."""
+    nhalf = c.shape[1]
+    phi = torch.zeros(c.shape[0], npad, dtype=torch.float64, device=c.device)
+    phi[:, 0] = c[:, 0].real
+    phi[:, 1:2 * nhalf - 1:2] = c[:, 1:].real
+    phi[:, 2:2 * nhalf - 1:2] = c[:, 1:].imag
+    return phi
+
+
+class _LearnedGamma:
+    """The learned preconditioner on the Gamma path: the network's complex-row
+    kernel (``gwb::precond_apply``) on the sqrt(w)-scaled half-sphere rows of
+    the selected bands, with the stall rule of the complex solver (a band
+    whose residual has not improved on its best by 10 % for 3 rounds keeps
+    TPA from then on; ``gwb_stall_update``). Its per-band state follows the
+    active Ritz block through locking."""
+
+    def __init__(self, model, nb: int, t_half: torch.Tensor, dev):
+        self.params = model.params.to(dev)
+        self.t_half = t_half.to(dev, torch.float64).reshape(1, -1).contiguous()
+        self.best = torch.full((nb,), float("inf"), dtype=torch.float64, device=dev)
+        self.count = torch.zeros(nb, dtype=torch.uint8, device=dev)
+        self.tpa_only = torch.zeros(nb, dtype=torch.uint8, device=dev)
+
+    def keep(self, mask: torch.Tensor) -> None:
+        self.best, self.count, self.tpa_only = self.best[mask], self.count[mask], self.tpa_only[mask]
+
+    def n_fallback(self) -> int:
+        return int(self.tpa_only.sum())
+
+    def __call__(self, x: torch.Tensor, r: torch.Tensor, rn: torch.Tensor, eig: torch.Tensor,
+                 sel: torch.Tensor, npad: int) -> torch.Tensor:
+        n_all = int(rn.shape[0])
+        rn = rn.contiguous()
+        _lib.call("gwb_stall_update", rn.data_ptr(), self.best.data_ptr(), self.count.data_ptr(),
+                  self.tpa_only.data_ptr(), n_all, 0.9, 3, _lib.stream_ptr(rn.device))
+        nhalf = int(self.t_half.shape[1])
+        xs, rs = _half_rows(x[sel], nhalf), _half_rows(r[sel], nhalf)
+        n = int(xs.shape[0])
+        idx = torch.arange(n, dtype=torch.int32, device=x.device).reshape(1, n)
+        d = torch.ops.gwb.precond_apply(xs[None], rs[None], self.t_half, idx, eig[sel].reshape(1, n),
+                                        self.params, self.tpa_only[sel].reshape(1, n))
+        return _embed_rows(d[0], npad)
 
 
 class _Locked:
@@ -406,7 +507,7 @@ class _Locked:
 @torch.no_grad()
 def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, max_iter: int = 40,
                    max_dim_factor: int = 4, mode: str = "fp64", lock: bool | None = None,
-                   n_buffer: int = 0, buffer_tol: float = 1e-2) -> GammaDavidsonResult:
+                   n_buffer: int = 0, buffer_tol: float = 1e-2, precond="teter") -> GammaDavidsonResult:
     """Real-symmetric block Davidson on the half sphere
     (``core/gamma.py:261-290``): the single-k Davidson of the reference
     (``solvers/davidson.py:330-395``: Rayleigh-Ritz on the whole subspace,
@@ -443,7 +544,12 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
     the next embedded coordinates, seeded noise where those repeat a start
     direction): they keep the wanted block's upper edge away
     from the first unwanted eigenvalue, are expanded only while their residual
-    exceeds ``buffer_tol`` (eV) and are neither tested nor returned."""
+    exceeds ``buffer_tol`` (eV) and are neither tested nor returned.
+
+    ``precond``: ``"teter"`` (TPA) or a ``learned.LearnedPreconditioner``
+    (the network on the half-sphere rows, TPA for bands whose residual
+    stalls). The float64 products run on the int8 tensor cores
+    (``gradwave_b200.oz``) unless ``GWB_OZ=0``."""
     if mode not in ("fp64", "mixed"):
         raise ValueError(f"mode must be 'fp64' or 'mixed', got {mode!r}")
     if n_buffer < 0:
@@ -480,6 +586,8 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
     t_phi = torch.nn.functional.pad(ham.t_phi, (0, npad - nphi))
     tcp = _TcProjection(rows, nb, npad, dev) if (mode == "mixed" and dev.type == "cuda"
                                                  and os.environ.get("GWB_TC_PROJECT", "1") != "0") else None
+    # float64 products on the int8 tensor cores (GWB_OZ=0: cuBLAS DGEMM)
+    mm = _Products(dev, oz=dev.type == "cuda" and os.environ.get("GWB_OZ", "1") != "0")
     v0 = _orthonormalize(phi0.clone())
     if v0.shape[0] < nb:  # degenerate start: pad with seeded noise (``:345-350``)
         gen = torch.Generator(device="cpu").manual_seed(1234)
@@ -498,6 +606,11 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
     prev = float("inf")
     HV[:m] = ham.apply_phi(V[:m], prec=f32 if low else f64)
     locked = _Locked(nwant, npad, dev)
+    learned = None
+    if not (precond is None or (isinstance(precond, str) and precond == "teter")):
+        if not hasattr(precond, "params"):
+            raise ValueError("precond must be 'teter' or a learned.LearnedPreconditioner")
+        learned = _LearnedGamma(precond, nb, gb.t_half, dev)
     # the subspace matrix grows by the new columns only (m0: rows already in it)
     S = torch.zeros(rows, rows, dtype=torch.float64, device=dev)
     m0 = 0
@@ -506,15 +619,16 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
         """Float64 apply of the Ritz block and its nb x nb Rayleigh-Ritz
         (gradwave ``solvers/davidson.py:281-308``)."""
         hx = ham.apply_phi(x, prec=f64)
-        g = x @ hx.T
+        g = mm.nt(x, hx)
         w2, u2 = torch.linalg.eigh(0.5 * (g + g.T))
-        x, hx = u2.T @ x, u2.T @ hx
+        x, hx = mm.nn(u2.T, x), mm.nn(u2.T, hx)
         r = hx - w2[:, None] * x
         return x, hx, w2, r, torch.linalg.vector_norm(r, dim=1)
 
     def finish(eig, x, rn, nw_a, it):
         e, xx, r = locked.merge(eig[:nw_a], x[:nw_a], rn[:nw_a])
-        return GammaDavidsonResult(e, unembed_real(gb, xx[:, :nphi]), it, r, prof.summary())
+        return GammaDavidsonResult(e, unembed_real(gb, xx[:, :nphi]), it, r, prof.summary(),
+                                   0 if learned is None else learned.n_fallback())
 
     it = 0
     for it in range(1, max_iter + 1):
@@ -522,7 +636,7 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
         nw_a = nwant - locked.n   # wanted pairs still in it
         v, hv = V[:m], HV[:m]
         with prof("subspace_gemm"):
-            blk = v @ hv[m0:m].T                       # (m, m - m0)
+            blk = mm.nt(v, hv[m0:m])                   # (m, m - m0)
             S[:m, m0:m] = blk
             S[m0:m, :m0] = blk[:m0].T
             S[m0:m, m0:m] = 0.5 * (blk[m0:] + blk[m0:].T)
@@ -533,8 +647,8 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
         eig = w[:nb_a]
         with prof("ritz_gemm"):
             ut = u[:, :nb_a].T
-            x = ut @ v
-            hx = ut @ hv
+            x = mm.nn(ut, v)
+            hx = mm.nn(ut, hv)
         with prof("residual"):
             r = hx - eig[:, None] * x
             rn = torch.linalg.vector_norm(r, dim=1)
@@ -563,10 +677,13 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
         if done:
             return finish(eig, x, rn, nw_a, it)
         with prof("orthonormalize"):
-            t_band = (x * x * t_phi[None, :]).sum(dim=1)
-            pr = _teter(r[unconv], t_phi, t_band[unconv])
+            if learned is not None:
+                pr = learned(x, r, rn, eig, torch.nonzero(unconv).flatten(), npad)
+            else:
+                t_band = (x * x * t_phi[None, :]).sum(dim=1)
+                pr = _teter(r[unconv], t_phi, t_band[unconv])
             pr[:, nphi:] = 0.0  # the pad column is not a coordinate of the operator
-            t = _expand(pr, v, tcp, locked.rows())
+            t = _expand(pr, v, tcp, locked.rows(), mm)
         if t.shape[0] == 0:  # no independent direction left
             if low:
                 x, hx, eig, r, rn = certify(x)
@@ -583,6 +700,8 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
                 keep = torch.ones(nb_a, dtype=torch.bool, device=dev)
                 if n_lock:
                     keep[:nw_a] = ~lockable
+                    if learned is not None:
+                        learned.keep(keep)
                     locked.add(x[:nw_a][lockable], hx[:nw_a][lockable], eig[:nw_a][lockable],
                                rn[:nw_a][lockable])
                 xk, hxk = x[keep], hx[keep]   # copies (x may alias V rows)

@@ -230,6 +230,42 @@ int gwb_zgemm_tc(int opB, int64_t M, int64_t N, int64_t K, double alpha_re, doub
                  double beta_re, double beta_im, void* C, int64_t ldc, int64_t strideC, int64_t batch, void* work,
                  size_t work_bytes, int* status, void* stream);
 
+/* Float64-accurate real products on the int8 tensor cores (tcgen05
+ * kind::i8, the Ozaki scheme). A slice set is s (6, 7 or 8) int8 planes of
+ * rows_cap x ldk (ldk a multiple of 64, 16-byte aligned base), plane p at
+ * p rows_cap ldk, with one float64 scale per row: row r is
+ * scale[r] sum_p plane_p[r] 2^-7(p+1), each plane holding 7 bits of every
+ * element (truncated; scale the power of two above the row's largest
+ * magnitude). The float64 GEMMs of the Davidson subspace, Ritz, projection
+ * and Cholesky-QR steps (gradwave solvers/davidson.py:195-222,428-432,
+ * 648-657) run on them; the reference has no counterpart.
+ *
+ * gwb_oz_split_rows: rows [row0, row0 + rows) of the set from the rows of src
+ * (K columns, row stride ld_src), each element times fold[k] when fold is
+ * not NULL; columns K..ldk-1 zeroed; scale[row0 + r] set. */
+int gwb_oz_split_rows(int32_t s, int64_t rows, int64_t K, const double* src, int64_t ld_src, const double* fold,
+                      void* slices, int64_t ldk, int64_t rows_cap, int64_t row0, double* scale, void* stream);
+/* gwb_oz_split_cols: the transposed layout. src is krows x R (row stride
+ * ld_src); row r of the set gets, in columns k0 .. k0 + krows - 1, the
+ * slices of src[k][r] / kscale[k0 + k], with kscale[k0 + k] the power of two
+ * above max_r |src[k][r]| (set here). The B operand of C = A B (B = src) is
+ * this set, with kscale folded into A's rows by gwb_oz_split_rows. */
+int gwb_oz_split_cols(int32_t s, int64_t krows, int64_t R, const double* src, int64_t ld_src, void* slices,
+                      int64_t ldk, int64_t rows_cap, int64_t k0, double* kscale, void* stream);
+/* C (M x N float64, row stride ldc) = alpha diag(a_scale) (A B^T) diag(b_scale)
+ * + beta C over K columns, for rows a_row0.. of slice set A and b_row0.. of
+ * slice set B (b_scale NULL: ones); the s(s+1)/2 slice pairs with
+ * i + j <= s + 1 as exact int8 products (int32 accumulation in tensor memory,
+ * float64 sums every 8192 columns). Columns K..ceil(K/64)*64-1 of A must be
+ * zero. Small tile grids split K, with float64 partials in `work`
+ * (gwb_oz_work_bytes; fewer splits with less). A pipeline wait that runs out
+ * ORs GWB_ERR_TIMEOUT into *status (device int). */
+int64_t gwb_oz_work_bytes(int64_t M, int64_t N, int64_t K);
+int gwb_oz_gemm(int32_t s, int64_t M, int64_t N, int64_t K, const void* A, int64_t lda, int64_t a_rows_cap,
+                int64_t a_row0, const double* a_scale, const void* B, int64_t ldb, int64_t b_rows_cap, int64_t b_row0,
+                const double* b_scale, double alpha, double beta, double* C, int64_t ldc, void* work,
+                size_t work_bytes, int* status, void* stream);
+
 /* r = hx - eig * x and rn = |r| per (k, band); eig (nk, eig_kstride) float64.
  * Replaces gradwave solvers/davidson.py:656-657. */
 int gwb_residual(int32_t nk, int32_t nb, int32_t npw, const void* x, int64_t x_kstride, const void* hx,

@@ -40,16 +40,23 @@ class OracleHamiltonian:
         self.idx_scatter = np.where(self.mask, self.flat_idx, self.n)
         self.n_apply = 0   # band*k applies, the reference's hpsi tally
 
-    def local(self, c: np.ndarray) -> np.ndarray:
+    def local(self, c: np.ndarray, chunk: int = 8) -> np.ndarray:
+        """Band chunks of ``chunk`` boxes at a time (the same arithmetic as one
+        batched transform; a chunk's boxes stay in cache)."""
         nk, nb, m = c.shape
         out = np.zeros_like(c)
+        box = np.zeros((min(chunk, max(nb, 1)), self.n + 1), dtype=np.complex128)
         for k in range(nk):
-            box = np.zeros((nb, self.n + 1), dtype=np.complex128)
-            box[:, self.idx_scatter[k]] = c[k]
-            psi = scipy.fft.ifftn(box[:, :self.n].reshape(nb, *self.shape), axes=(-3, -2, -1),
-                                  workers=_workers())
-            vg = scipy.fft.fftn(psi * self.v, axes=(-3, -2, -1), workers=_workers())
-            out[k] = vg.reshape(nb, self.n)[:, self.flat_idx[k]]
+            for b0 in range(0, nb, chunk):
+                b1 = min(nb, b0 + chunk)
+                bx = box[: b1 - b0]
+                bx[:] = 0.0
+                bx[:, self.idx_scatter[k]] = c[k, b0:b1]
+                psi = scipy.fft.ifftn(bx[:, :self.n].reshape(b1 - b0, *self.shape), axes=(-3, -2, -1),
+                                      workers=_workers(), overwrite_x=False)
+                psi *= self.v
+                vg = scipy.fft.fftn(psi, axes=(-3, -2, -1), workers=_workers(), overwrite_x=True)
+                out[k, b0:b1] = vg.reshape(b1 - b0, self.n)[:, self.flat_idx[k]]
         return out
 
     def nonlocal_(self, c: np.ndarray) -> np.ndarray:

@@ -6,9 +6,9 @@
 * Adam step vs numpy;
 * a zero output layer makes the learned step exactly TPA;
 * training on solver-logged pairs lowers the held-out loss below TPA's;
-* with the committed weights, a held-out cell converges to the reference's
-  eigenvalues and the iteration counts with and without the network are
-  recorded.
+* with the committed weights (trained on 8-atom cells), the held-out
+  64-atom cell converges to the reference's eigenvalues in fewer rounds with
+  the network than with TPA.
 """
 
 import json
@@ -20,6 +20,8 @@ import torch
 from tests.conftest import load_golden
 
 pytestmark = pytest.mark.gpu
+
+HA = 27.211386245988
 
 
 def _rand_params(seed):
@@ -132,26 +134,39 @@ def test_alignment_gradient_matches_finite_difference(cuda_device):
     assert abs(fd - float(do.sum())) <= 5e-2 * abs(fd) + 1e-6
 
 
-def test_committed_network_on_heldout_cell(cuda_device):
+def test_committed_network_gains_on_heldout_cell(cuda_device):
+    """What the trained network gains: the committed weights were trained on
+    rows logged from solves of seeded displaced and strained 8-atom cells
+    only; applied to the 64-atom cell (4 k, 160 bands, basis 640: held out),
+    the mixed solve with the network needs fewer Davidson rounds than the same
+    solve with TPA, and both end within 1e-8 Ha of the reference's float64
+    eigenvalues and 1e-6 Ha/cell in band energy."""
     from gradwave_b200 import learned
     from gradwave_b200.cells import make_cell
     from gradwave_b200.davidson import davidson_batched
     from gradwave_b200.hamiltonian import BatchedHamiltonian
     if not learned.available():
         pytest.skip("no trained weights committed")
-    g = load_golden("si8_cubic")
-    ci = make_cell("si8_cubic")
+    g = load_golden("si64_cubic")
+    ci = make_cell("si64_cubic")
     bk = ci.bk.to(cuda_device)
     h = BatchedHamiltonian(bk, ci.shape, ci.v_eff_r, ci.p)
     x0 = ci.identity_start().to(cuda_device)
     lp = learned.LearnedPreconditioner.load(device=cuda_device)
-    rl = davidson_batched(h.apply, x0, bk.t, bk.mask, tol=1e-10, max_iter=200, precond=lp)
-    rt = davidson_batched(h.apply, x0, bk.t, bk.mask, tol=1e-10, max_iter=200)
+    rl = davidson_batched(h.apply, x0, bk.t, bk.mask, tol=1e-10, max_iter=300, mode="mixed", precond=lp)
+    rt = davidson_batched(h.apply, x0, bk.t, bk.mask, tol=1e-10, max_iter=300, mode="mixed")
+    nocc = ci.nocc()
+    w = np.asarray(ci.kweights)
     for r in (rl, rt):
+        eig = r.eigenvalues.cpu().numpy()
         assert float(r.residual_norms.max()) < 1e-10
-        assert np.abs(r.eigenvalues.cpu().numpy() - g["eigenvalues"]).max() < 1e-9
+        assert np.abs(eig - g["eigenvalues"]).max() < 1e-8 * HA
+        be = 2.0 * float(np.sum(w[:, None] * (eig[:, :nocc] - g["eigenvalues"][:, :nocc])))
+        assert abs(be) < 1e-6 * HA
     print(json.dumps({"learned_iters": rl.n_iter, "tpa_iters": rt.n_iter,
-                      "learned_applies": rl.n_apply_full, "tpa_applies": rt.n_apply_full}))
+                      "learned_applies": rl.n_apply_low + rl.n_apply_full,
+                      "tpa_applies": rt.n_apply_low + rt.n_apply_full}))
+    assert rl.n_iter < rt.n_iter
 
 
 def test_tensor_core_inference_matches_reference_forward(cuda_device):
