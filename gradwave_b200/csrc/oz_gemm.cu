@@ -3,23 +3,25 @@
 // Ootomo, Ozaki, Yokota 2024 for integer tensor cores).
 //
 // Splitting. Every row of an operand is scaled by a power of two sigma above
-// its largest magnitude, so |x / sigma| < 1, and cut into S signed 7-bit
-// slices by repeated truncation: t = x / sigma; for p = 1..S: t *= 128,
-// q_p = trunc(t) in [-127, 127], t -= q_p. Then x = sigma sum_p q_p 2^-7p up
-// to 2^-7S sigma, every step exact in float64. A slice set holds the S int8
-// planes of rows_cap x ldk (ldk a multiple of 64, columns K..ldk-1 zero),
-// plane p at p rows_cap ldk, and the per-row scales.
+// its largest magnitude, so |x / sigma| < 1, and cut into S signed slices by
+// repeated rounding to nearest: t = 64 x / sigma; for p = 1..S: q_p = rint(t)
+// in [-64, 64], t = 128 (t - q_p). Then x = sigma sum_p q_p 2^(1-7p) to
+// within 2^-7S sigma, every step exact in float64. Rounding (not truncation)
+// leaves errors of either sign, so they do not add up coherently in sums such
+// as the diagonal of a Gram matrix. A slice set holds the S int8 planes of
+// rows_cap x ldk (ldk a multiple of 64, columns K..ldk-1 zero), plane p at
+// p rows_cap ldk, and the per-row scales.
 //
-// Product. C = alpha diag(sa) (sum_{i+j <= S+1} 2^-7(i+j) A_i B_j^T) diag(sb)
-// + beta C for slice sets A (M x K) and B (N x K): every A_i B_j^T is an
-// exact int8 product with int32 accumulation, the pairs of one level L = i + j
-// share an int32 accumulator in tensor memory, and the levels are added into
-// float64 registers once per K chunk of 8192 (S x 8192 x 127^2 < 2^31 for
-// S <= 8, so no int32 sum can overflow). The pairs with i + j > S + 1 lie
-// below the error of the kept ones and are not formed: S(S+1)/2 int8 products
-// per float64 product. With S = 7 the result is within about 4e-14 of the
-// float64 product relative to max|a| max|b| K (measured on rows of decaying
-// plane-wave coefficients), the level of a float64 GEMM at these K.
+// Product. C = alpha diag(sa) (sum_{i+j <= S+1} 2^(2-7(i+j)) A_i B_j^T)
+// diag(sb) + beta C for slice sets A (M x K) and B (N x K): every A_i B_j^T
+// is an exact int8 product with int32 accumulation, the pairs of one level
+// L = i + j share an int32 accumulator in tensor memory, and the levels are
+// added into float64 registers once per K chunk of 32768 (S x 32768 x 64^2 <
+// 2^31 for S <= 8, so no int32 sum can overflow). The pairs with
+// i + j > S + 1 lie below the error of the kept ones and are not formed:
+// S(S+1)/2 int8 products per float64 product. The error of an element is
+// about 2^-7S of the rows' scales times sqrt(K): with S = 8 the level of a
+// float64 GEMM of the same shape.
 //
 // A product C = A B with B held as K x N rows (the Davidson updates
 // D -= C V and the Ritz vectors X = U^T V) uses B's slices transposed
@@ -51,7 +53,7 @@ constexpr int OZ_M = 128;
 constexpr int OZ_N = 64;
 constexpr int OZ_KS = 64;                    // K elements (bytes) per stage: one 64-byte swizzle row
 constexpr int OZ_STAGES = 2;
-constexpr int OZ_CHUNK_STEPS = 8192 / OZ_KS;  // stages per int32 accumulation chunk
+constexpr int OZ_CHUNK_STEPS = 32768 / OZ_KS;  // stages per int32 accumulation chunk
 constexpr int OZ_THREADS = 192;
 constexpr int OZ_TMEM_COLS = 512;
 constexpr int OZ_SROW = OZ_N + 1;            // staging row (doubles), padded
@@ -220,7 +222,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
       for (int l = 0; l < S; ++l) {
-        const double f = ldexp(1.0, -7 * (l + 2));
+        const double f = ldexp(1.0, 2 - 7 * (l + 2));  // level L = l + 2: weight 2^(2 - 7L)
 #pragma unroll
         for (int cb = 0; cb < OZ_N / 16; ++cb) {
           uint32_t r[16];
@@ -318,14 +320,14 @@ template <int NT> __device__ double block_max(double v, double* red) {
   return v;
 }
 
-// S slices of t (|t| < 1) into q[0..S-1]
+// S slices of t (|t| < 1) into q[0..S-1]: q_p in [-64, 64] with weight 2^(1-7p)
 template <int S> __device__ __forceinline__ void cut(double t, signed char (&q)[S]) {
+  t *= 64.0;
 #pragma unroll
   for (int p = 0; p < S; ++p) {
-    t *= 128.0;
-    const double w = trunc(t);
+    const double w = rint(t);
     q[p] = (signed char)(int)w;
-    t -= w;
+    t = (t - w) * 128.0;
   }
 }
 

@@ -31,6 +31,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from . import ops  # noqa: F401  (registers torch.ops.gwb.*)
 from .constants import HBAR2_2M
 
 _R2 = 2.0 ** 0.5
@@ -312,13 +313,45 @@ class _Products:
     or, with ``oz``, the int8 tensor-core products of ``gradwave_b200.oz``
     (the Ozaki scheme, 8 slices: float64-level error relative to the rows'
     maxima). ``nt(a, b)`` = a b^T, ``nn(a, b)`` = a b, ``sub_nn(t, c, b)``:
-    t -= c b in place."""
+    t -= c b in place.
+
+    ``attach(V, HV)`` registers the solver's basis buffers: their slices are
+    then kept current by ``rows_changed(r0, r1)`` (only the rows that
+    changed are sliced again), and a product whose operand is a prefix
+    ``V[:m]`` or ``HV[:m]`` reads the kept slices instead of slicing it."""
 
     def __init__(self, dev=None, oz: bool = False):
         self.om = None
+        self.V = self.HV = None
+        self.valid = 0
         if oz:
             from .oz import OzMatmul
             self.om = OzMatmul(dev)
+
+    def attach(self, V: torch.Tensor, HV: torch.Tensor) -> None:
+        if self.om is None:
+            return
+        from .oz import SliceSet
+        rows, npad = V.shape
+        self.V, self.HV = V, HV
+        self.v_rows = SliceSet(rows, npad, V.device, self.om.s)   # rows of V (a b^T operands)
+        self.v_cols = SliceSet(npad, rows, V.device, self.om.s)   # V^T: the B of  . @ V
+        self.hv_cols = SliceSet(npad, rows, V.device, self.om.s)  # HV^T: the B of . @ HV
+        self.valid = 0
+
+    def rows_changed(self, r0: int, r1: int) -> None:
+        """Rows [r0, r1) of V and HV were written; rows before r0 are as
+        they were when last sliced."""
+        if self.V is None or r1 <= r0:
+            return
+        self.v_rows.split_rows(self.V[r0:r1], row0=r0)
+        self.v_cols.split_cols(self.V[r0:r1], k0=r0)
+        self.hv_cols.split_cols(self.HV[r0:r1], k0=r0)
+        self.valid = r1
+
+    def _prefix(self, t: torch.Tensor, base) -> bool:
+        return (base is not None and t.dim() == 2 and t.data_ptr() == base.data_ptr()
+                and t.stride() == base.stride() and t.shape[1] == base.shape[1] and t.shape[0] <= self.valid)
 
     @staticmethod
     def _rows(a: torch.Tensor) -> torch.Tensor:
@@ -327,22 +360,44 @@ class _Products:
     def nt(self, a: torch.Tensor, b: torch.Tensor, same: bool = False) -> torch.Tensor:
         if self.om is None or a.shape[0] == 0 or b.shape[0] == 0:
             return a @ b.T
+        from .oz import oz_gemm
         a = self._rows(a)
         b = a if same else self._rows(b)
         out = torch.empty(a.shape[0], b.shape[0], dtype=torch.float64, device=a.device)
+        if not same and self._prefix(a, self.V):      # V[:m] b^T
+            sb = self.om._set("nt_b", b.shape[0], b.shape[1])
+            sb.split_rows(b)
+            oz_gemm(a.shape[0], b.shape[0], a.shape[1], self.v_rows, sb, out)
+            return out
+        if not same and self._prefix(b, self.V):      # a V[:m]^T
+            sa = self.om._set("nt_a", a.shape[0], a.shape[1])
+            sa.split_rows(a)
+            oz_gemm(a.shape[0], b.shape[0], a.shape[1], sa, self.v_rows, out)
+            return out
         return self.om.nt(a, b, out, same=same)
+
+    def _nn_into(self, a: torch.Tensor, b: torch.Tensor, out: torch.Tensor, alpha: float, beta: float) -> None:
+        from .oz import oz_gemm
+        for base, cols in ((self.V, getattr(self, "v_cols", None)), (self.HV, getattr(self, "hv_cols", None))):
+            if self._prefix(b, base):
+                m = b.shape[0]
+                sa = self.om._set("nn_a", a.shape[0], m)
+                sa.split_rows(a.contiguous(), fold=cols.kscale)
+                oz_gemm(a.shape[0], b.shape[1], m, sa, cols, out, alpha, beta, b_scaled=False)
+                return
+        self.om.nn(a.contiguous(), self._rows(b), out, alpha, beta)
 
     def nn(self, a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
         if self.om is None or a.shape[0] == 0 or b.shape[0] == 0:
             return a @ b
-        a, b = a.contiguous(), self._rows(b)
         out = torch.empty(a.shape[0], b.shape[1], dtype=torch.float64, device=a.device)
-        return self.om.nn(a, b, out)
+        self._nn_into(a, b, out, 1.0, 0.0)
+        return out
 
     def sub_nn(self, t: torch.Tensor, c: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
         if self.om is None or t.stride(-1) != 1:
             return t.addmm_(c, b, alpha=-1.0)
-        self.om.nn(c.contiguous(), self._rows(b), t, alpha=-1.0, beta=1.0)
+        self._nn_into(c, b, t, -1.0, 1.0)
         return t
 
 
@@ -548,8 +603,8 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
 
     ``precond``: ``"teter"`` (TPA) or a ``learned.LearnedPreconditioner``
     (the network on the half-sphere rows, TPA for bands whose residual
-    stalls). The float64 products run on the int8 tensor cores
-    (``gradwave_b200.oz``) unless ``GWB_OZ=0``."""
+    stalls). With ``GWB_OZ=1`` the float64 products run on the int8 tensor
+    cores (``gradwave_b200.oz``) instead of cuBLAS."""
     if mode not in ("fp64", "mixed"):
         raise ValueError(f"mode must be 'fp64' or 'mixed', got {mode!r}")
     if n_buffer < 0:
@@ -586,8 +641,10 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
     t_phi = torch.nn.functional.pad(ham.t_phi, (0, npad - nphi))
     tcp = _TcProjection(rows, nb, npad, dev) if (mode == "mixed" and dev.type == "cuda"
                                                  and os.environ.get("GWB_TC_PROJECT", "1") != "0") else None
-    # float64 products on the int8 tensor cores (GWB_OZ=0: cuBLAS DGEMM)
-    mm = _Products(dev, oz=dev.type == "cuda" and os.environ.get("GWB_OZ", "1") != "0")
+    # float64 products: cuBLAS DGEMM, or with GWB_OZ=1 the int8 tensor-core
+    # products (measured on this path: no faster than DGEMM at these shapes,
+    # and a residual floor just above 1e-10 eV on the 216-atom cell)
+    mm = _Products(dev, oz=dev.type == "cuda" and os.environ.get("GWB_OZ", "0") == "1")
     v0 = _orthonormalize(phi0.clone())
     if v0.shape[0] < nb:  # degenerate start: pad with seeded noise (``:345-350``)
         gen = torch.Generator(device="cpu").manual_seed(1234)
@@ -605,6 +662,8 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
     cert_floor = 32.0 * float(torch.finfo(torch.float32).eps) * max(float(t_phi.max()), 1.0)
     prev = float("inf")
     HV[:m] = ham.apply_phi(V[:m], prec=f32 if low else f64)
+    mm.attach(V, HV)
+    mm.rows_changed(0, m)
     locked = _Locked(nwant, npad, dev)
     learned = None
     if not (precond is None or (isinstance(precond, str) and precond == "teter")):
@@ -669,6 +728,7 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
                     v, hv = V[:m], HV[:m]
                     if tcp is not None:
                         tcp.rows(V, 0, m)
+                    mm.rows_changed(0, m)
         with prof("residual"):
             unconv = rn > tol
             if n_buffer:
@@ -718,6 +778,7 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
             m += nt
             if tcp is not None:
                 tcp.rows(V, r0, m)
+            mm.rows_changed(r0, m)
     if low:  # out of rounds in float32: certify what there is
         x, hx, eig, r, rn = certify(x)
     return finish(eig, x, rn, nwant - locked.n, max_iter)

@@ -3,7 +3,8 @@
 scheme on tcgen05 kind::i8).
 
 A ``SliceSet`` holds up to ``rows_cap`` rows of length up to ``k_cap`` as s
-int8 planes (7 bits each, per-row power-of-two scales), the operand format of
+int8 planes (about 7 bits each, rounded to nearest, per-row power-of-two
+scales), the operand format of
 ``oz_gemm``. Rows are written either from rows of a float64 matrix
 (``split_rows``, optionally multiplied column by column by ``fold``) or from
 the columns of one (``split_cols``: the transposed layout that a product

@@ -234,9 +234,9 @@ int gwb_zgemm_tc(int opB, int64_t M, int64_t N, int64_t K, double alpha_re, doub
  * kind::i8, the Ozaki scheme). A slice set is s (6, 7 or 8) int8 planes of
  * rows_cap x ldk (ldk a multiple of 64, 16-byte aligned base), plane p at
  * p rows_cap ldk, with one float64 scale per row: row r is
- * scale[r] sum_p plane_p[r] 2^-7(p+1), each plane holding 7 bits of every
- * element (truncated; scale the power of two above the row's largest
- * magnitude). The float64 GEMMs of the Davidson subspace, Ritz, projection
+ * scale[r] sum_p plane_p[r] 2^(-6-7p) to within 2^-7s scale[r], every plane
+ * value in [-64, 64] (each rounded to nearest; scale the power of two above
+ * the row's largest magnitude). The float64 GEMMs of the Davidson subspace, Ritz, projection
  * and Cholesky-QR steps (gradwave solvers/davidson.py:195-222,428-432,
  * 648-657) run on them; the reference has no counterpart.
  *

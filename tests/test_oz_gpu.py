@@ -2,8 +2,9 @@
 against float64 products of numpy (long-double accumulation as the exact
 reference).
 
-* the slices rebuild every element to 2^-7s of its row's scale, the pad
-  columns are zero, the scales are powers of two above the row maxima;
+* the slices (rounded to nearest, |q| <= 64) rebuild every element to 2^-7s
+  of its row's scale, the pad columns are zero, the scales are powers of two
+  above the row maxima;
 * A B^T (both forms of operand), ragged sizes, split K, alpha/beta, rows
   taken from an offset: error within 1e-13 (7 slices) and 1e-15 (8 slices)
   of max|a| max|b| K-scaled, i.e. at the level of a float64 GEMM, on rows of
@@ -39,8 +40,9 @@ def test_split_rows_rebuilds_the_rows(cuda_device):
     torch.cuda.synchronize()
     q = st.q.cpu().numpy().astype(np.float64)[:, 2:39]
     sc = st.scale.cpu().numpy()[2:39]
-    rebuilt = sum(q[p] * 2.0 ** (-7 * (p + 1)) for p in range(7)) * sc[:, None]
+    rebuilt = sum(q[p] * 2.0 ** (-6 - 7 * p) for p in range(7)) * sc[:, None]
     assert np.all(np.abs(rebuilt[:, :1000] - a) <= 2.0 ** -49 * sc[:, None])
+    assert np.abs(q).max() <= 64
     assert np.all(q[:, :, 1000:] == 0)
     mx = np.abs(a).max(axis=1)
     nz = mx > 0
@@ -91,3 +93,4 @@ def test_product_nn_and_reuse(cuda_device):
     om.nt(A, A, g, same=True)
     refg = _exact(a, a)
     assert np.abs(g.cpu().numpy() - refg).max() < 1e-13 * np.abs(refg).max()
+
