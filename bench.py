@@ -645,6 +645,35 @@ def run_apply(args):
     return 0
 
 
+def run_apply_gamma(args):
+    """Apply-only loop of the Gamma path (for profiling its kernels under
+    ncu): K applies of the workload's whole embedded band block (nbands real
+    rows, two per complex row of the apply kernels), float32 or float64."""
+    import torch
+    from gradwave_b200.cells import make_cell
+    from gradwave_b200.gamma import GammaHamiltonian, build_gamma_basis
+    dev = torch.device("cuda", 0)
+    ci = make_cell(args.config)
+    gb = build_gamma_basis(ci.spheres[0], ci.shape)
+    gh = GammaHamiltonian(gb, ci.v_eff_r, ci.p[0], ci.bk.dij_full, device=dev)
+    g = torch.Generator().manual_seed(1)
+    phi = torch.randn(ci.nbands, 2 * gb.nhalf - 1, dtype=torch.float64, generator=g).to(dev)
+    prec = 0 if args.prec == "fp32" else 1
+    for _ in range(args.warmup):
+        gh.apply_phi(phi, prec=prec)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        gh.apply_phi(phi, prec=prec)
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"mode": "apply_gamma", "config": args.config, "prec": args.prec, "bands": ci.nbands,
+                      "complex_rows": (ci.nbands + 1) // 2, "ms_per_apply": e0.elapsed_time(e1) / args.steps}),
+          flush=True)
+    return 0
+
+
 def run_once(args):
     """``--warmup`` untimed and one wall-timed solve of the workload (for ncu
     launch lists and the larger cells): rounds, applies, eigenvalue and band
@@ -848,6 +877,9 @@ def _solver_choice(name, dev):
     if name == "mixed":
         return "mixed", "teter"
     if name == "learned-mixed":
+        w = os.environ.get("GWB_PRECOND_WEIGHTS")
+        if w:
+            return "mixed", learned.LearnedPreconditioner.load(w, device=dev)
         pc = learned.LearnedPreconditioner.load(device=dev) if learned.available() else "teter"
         return "mixed", pc
     raise ValueError(f"unknown solver {name!r}")
@@ -871,7 +903,7 @@ def main():
     ap.add_argument("--n-buffer", type=int, default=None,
                     help="Gamma path: buffer bands above the wanted ones (default 32 in the bench line, 0 in --mode gamma)")
     ap.add_argument("--slices", type=int, default=8, help="--mode oz: int8 slices per float64 operand")
-    ap.add_argument("--mode", default="solve", choices=["solve", "apply", "once", "tc", "gamma", "oz"],
+    ap.add_argument("--mode", default="solve", choices=["solve", "apply", "apply_gamma", "once", "tc", "gamma", "oz"],
                     help="apply: only time Hamiltonian applies; once: a single solve (profiling)")
     ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64"], help="arithmetic of --mode apply")
     ap.add_argument("--solver", default="learned-mixed", choices=["plain", "fp32exp", "mixed", "learned-mixed"],
@@ -879,6 +911,8 @@ def main():
     args = ap.parse_args()
     if args.mode == "apply":
         return run_apply(args)
+    if args.mode == "apply_gamma":
+        return run_apply_gamma(args)
     if args.mode == "tc":
         return run_tc(args)
     if args.mode == "oz":

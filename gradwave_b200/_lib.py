@@ -83,6 +83,7 @@ _SIGNATURES = {
     "gwb_ham_apply": [_P, _P, _P, _I, _I, _I, _P],
     "gwb_ham_apply_strided": [_P, _P, _I64, _P, _I64, _I, _I, _I, _P],
     "gwb_ham_set_overlap": [_P, _P, _P],
+    "gwb_ham_set_tuning": [_P, _I64, _I],
     "gwb_ham_apply_hs": [_P, _P, _I64, _P, _I64, _P, _I64, _I, _I, _I, _P],
     "gwb_ham_scratch_bytes": [_P],
     "gwb_ham_tc_status": [_P, _P],

@@ -101,6 +101,9 @@ struct gwb_ham {
   double* d_rhok = nullptr;  // density accumulators, one box per k
   size_t rhok_bytes = 0;
   bool have_t = false, have_v = false, have_p = false, have_q = false;
+  // tuning (gwb_ham_set_tuning; 0 = the built-in rule)
+  size_t w_budget = 0;   // bytes of FFT scratch W per band chunk
+  int nl_target = 0;     // CTAs the G-sliced becp contraction aims for
 };
 
 namespace gwb {
@@ -766,7 +769,8 @@ static size_t pencil_smem(const FftGeom& g, size_t es) {
 // with every slice at least 256 plane waves long.
 static int nl_slices(const gwb_ham* h, int nb) {
   const int tiles = ((h->nproj + NL_TP - 1) / NL_TP) * ((nb + NL_TB - 1) / NL_TB) * h->nk;
-  const int want = (4 * 148 + tiles - 1) / tiles;
+  const int target = h->nl_target > 0 ? h->nl_target : 4 * 148;
+  const int want = (target + tiles - 1) / tiles;
   const int cap = std::max(1, h->npw_max / 256);
   return std::max(1, std::min(want, cap));
 }
@@ -888,7 +892,7 @@ static int local_term(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t ok
   const size_t plane_elems = (size_t)g.n[1] * g.n[2];
   const size_t per_band = (size_t)h->nk * g.L[0] * plane_elems * es;
   // balanced chunks: as few as the L2 budget allows, all of (nearly) equal size
-  const size_t budget = std::max(w_budget_bytes(), per_band);
+  const size_t budget = std::max(h->w_budget ? h->w_budget : w_budget_bytes(), per_band);
   const size_t max_nbc = std::max<size_t>(1, budget / per_band);
   const size_t nchunks = ((size_t)nb + max_nbc - 1) / max_nbc;
   int nbc = (int)(((size_t)nb + nchunks - 1) / nchunks);
@@ -1027,7 +1031,7 @@ static int density_impl(gwb_ham* h, const SIO* c, int64_t ck, int nb, const doub
   const size_t es = sizeof(cplx<double>);
   const size_t N = (size_t)g.n[0] * g.n[1] * g.n[2];
   const size_t per_band = (size_t)h->nk * g.L[0] * g.n[1] * g.n[2] * es;
-  const size_t budget = std::max(w_budget_bytes(), per_band);
+  const size_t budget = std::max(h->w_budget ? h->w_budget : w_budget_bytes(), per_band);
   const size_t max_nbc = std::max<size_t>(1, budget / per_band);
   const size_t nchunks = ((size_t)nb + max_nbc - 1) / max_nbc;
   int nbc = (int)(((size_t)nb + nchunks - 1) / nchunks);
@@ -1275,6 +1279,14 @@ int gwb_ham_apply(gwb_ham* h, const void* c, void* out, int32_t nb, int32_t io_d
   GWB_REQUIRE(h, "null handle");
   const int64_t ks = (int64_t)nb * h->npw_max;
   return gwb_ham_apply_strided(h, c, ks, out, ks, nb, io_dtype, prec, stream);
+}
+
+int gwb_ham_set_tuning(gwb_ham* h, int64_t w_budget_bytes, int32_t nl_target_ctas) {
+  GWB_REQUIRE(h, "null handle");
+  GWB_REQUIRE(w_budget_bytes >= 0 && nl_target_ctas >= 0, "tuning values must be >= 0");
+  h->w_budget = (size_t)w_budget_bytes;
+  h->nl_target = nl_target_ctas;
+  return GWB_OK;
 }
 
 int gwb_ham_set_overlap(gwb_ham* h, const double* q, void* stream) {

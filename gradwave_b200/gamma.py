@@ -179,6 +179,8 @@ class GammaHamiltonian:
             _lib.call("gwb_ham_set_potential", self._h, self.v.data_ptr(), s)
             _lib.call("gwb_ham_set_projectors", self._h, self.p.data_ptr() if self.nproj else None,
                       self.dij.data_ptr() if self.nproj else None, s)
+        from .autotune import apply_tuning
+        self.tuning = apply_tuning(self._h, "gamma", self.shape, self.nproj)
         i32 = dict(dtype=torch.int32, device=dev)
         self.src_half = gb.src_half.to(**i32).contiguous()
         self.conj_full = gb.conj_full.to(dev, torch.uint8).contiguous()
@@ -497,11 +499,16 @@ class _LearnedGamma:
     kernel (``gwb::precond_apply``) on the sqrt(w)-scaled half-sphere rows of
     the selected bands, with the stall rule of the complex solver (a band
     whose residual has not improved on its best by 10 % for 3 rounds keeps
-    TPA from then on; ``gwb_stall_update``). Its per-band state follows the
-    active Ritz block through locking."""
+    TPA from then on; ``gwb_stall_update``; GWB_STALL_RATIO and
+    GWB_STALL_PATIENCE change the 0.9 and the 3). Its per-band state follows
+    the active Ritz block through locking."""
 
     def __init__(self, model, nb: int, t_half: torch.Tensor, dev):
+        import os
         self.params = model.params.to(dev)
+        # the stall rule's ratio and patience (GWB_STALL_RATIO, GWB_STALL_PATIENCE)
+        self.ratio = float(os.environ.get("GWB_STALL_RATIO", "0.9"))
+        self.patience = int(os.environ.get("GWB_STALL_PATIENCE", "3"))
         self.t_half = t_half.to(dev, torch.float64).reshape(1, -1).contiguous()
         self.best = torch.full((nb,), float("inf"), dtype=torch.float64, device=dev)
         self.count = torch.zeros(nb, dtype=torch.uint8, device=dev)
@@ -518,7 +525,7 @@ class _LearnedGamma:
         n_all = int(rn.shape[0])
         rn = rn.contiguous()
         _lib.call("gwb_stall_update", rn.data_ptr(), self.best.data_ptr(), self.count.data_ptr(),
-                  self.tpa_only.data_ptr(), n_all, 0.9, 3, _lib.stream_ptr(rn.device))
+                  self.tpa_only.data_ptr(), n_all, self.ratio, self.patience, _lib.stream_ptr(rn.device))
         nhalf = int(self.t_half.shape[1])
         xs, rs = _half_rows(x[sel], nhalf), _half_rows(r[sel], nhalf)
         n = int(xs.shape[0])

@@ -81,6 +81,8 @@ class BatchedHamiltonian:
             _lib.call("gwb_ham_set_potential", self._h, self.v_eff_r.data_ptr(), s)
             _lib.call("gwb_ham_set_projectors", self._h, self.p.data_ptr() if self.nproj else None,
                       self.dij.data_ptr() if self.nproj else None, s)
+        from .autotune import apply_tuning
+        self.tuning = apply_tuning(self._h, "complex", self.shape, self.nproj)
 
     def __del__(self):
         h = getattr(self, "_h", None)

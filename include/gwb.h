@@ -107,6 +107,14 @@ int gwb_ham_apply(gwb_ham* h, const void* c, void* out, int32_t nb, int32_t io_d
 int gwb_ham_apply_strided(gwb_ham* h, const void* c, int64_t c_kstride, void* out, int64_t out_kstride,
                           int32_t nb, int32_t io_dtype, int32_t prec, void* stream);
 
+/* Tuning of a handle's applies (0 keeps the built-in rule): the bytes of FFT
+ * scratch per band chunk (default 48 MiB or GWB_W_BUDGET_MB: chunks of bands
+ * whose scratch stays in L2) and the number of CTAs the G-sliced projector
+ * contraction aims for (default 4 x 148). The values are chosen per box and
+ * projector count by gradwave_b200.autotune from timed applies. No
+ * counterpart in the reference. */
+int gwb_ham_set_tuning(gwb_ham* h, int64_t w_budget_bytes, int32_t nl_target_ctas);
+
 /* Augmentation matrix q (nproj*nproj float64, real symmetric, device) of the
  * overlap S = 1 + sum_pq |beta_p> q_pq <beta_q| (USPP/PAW). Set after the
  * projectors. Replaces q_full of gradwave scf/uspp_batch.py:34-45
