@@ -405,15 +405,21 @@ def _apply_roofline(tm: dict, rows_per_band: float, npw: float, n_box: float, np
             "launches": tm["calls"], "avg_launch_ms": round(tm["ms"] / max(1, tm["calls"]), 4),
             "share_of_step": round(tm["ms"] / max(1e-9, ms_step), 4),
             "bytes_per_row": bytes_per_row, "bytes_per_launch": per_launch, "rows_per_step": rows}
-    # DRAM bytes per complex row from the committed ncu capture of the same
-    # apply (cold cache, one launch), scaled to this run's rows per launch
+    # DRAM bytes per complex row of the float32 and float64 applies from the
+    # committed ncu capture of the same apply kernels (one whole-block apply
+    # of the workload; the figure per row is independent of the block size),
+    # times this run's rows of each precision, per launch
     summary = ROOT / "profiles" / f"{traffic_key}.md"
     if summary.exists() and tm["calls"]:
         import re
-        m = re.search(r"dram_bytes_per_row:\s*([0-9.eE+]+)", summary.read_text())
-        if m:
-            roof["traffic"] = round(float(m.group(1)) * rows / tm["calls"])
-            roof["traffic_source"] = f"profiles/{traffic_key}.md (ncu dram__bytes_read.sum + dram__bytes_write.sum)"
+        txt = summary.read_text()
+        m32 = re.search(r"dram_bytes_per_row_fp32:\s*([0-9.eE+]+)", txt)
+        m64 = re.search(r"dram_bytes_per_row_fp64:\s*([0-9.eE+]+)", txt)
+        if m32 and m64:
+            b = (float(m32.group(1)) * tm.get("bands_fp32", 0) + float(m64.group(1)) * tm.get("bands_fp64", 0))
+            roof["traffic"] = round(b * rows_per_band / tm["calls"])
+            roof["traffic_source"] = (f"profiles/{traffic_key}.md: ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                      "per complex row of each precision, times this run's rows")
     return roof
 
 

@@ -25,6 +25,7 @@ the reference's ``davidson_gamma`` runs the single-k ``davidson``
 from __future__ import annotations
 
 import ctypes
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -181,6 +182,29 @@ class GammaHamiltonian:
                       self.dij.data_ptr() if self.nproj else None, s)
         from .autotune import apply_tuning
         self.tuning = apply_tuning(self._h, "gamma", self.shape, self.nproj)
+        # float64 applies from 128 projectors: the nonlocal term in the real
+        # embedding as two float64 GEMMs (a second handle without projectors
+        # gives T + V_loc). At k = 0 the projectors are Hermitian-symmetric
+        # (P(-G) = conj P(G): real functions in real space), so their embedded
+        # rows pi_p give <P_p|c> = pi_p . phi for every real band and the term
+        # sum_pq P_p D_pq <P_q|c> embeds as (becp D) Pi: one real product per
+        # real band where the complex row costs a complex one per band pair.
+        self._h_loc = None
+        self.pi = None
+        if self.nproj >= 128 and os.environ.get("GWB_GAMMA_REAL_NL", "1") != "0":
+            geom.nproj = 0
+            hl = ctypes.c_void_p()
+            _lib.call("gwb_ham_create", ctypes.byref(geom), int(dev.index or 0), ctypes.byref(hl))
+            self._h_loc = hl
+            with torch.cuda.device(dev):
+                s = _lib.stream_ptr(dev)
+                _lib.call("gwb_ham_set_kinetic", hl, self.t.data_ptr(), s)
+                _lib.call("gwb_ham_set_potential", hl, self.v.data_ptr(), s)
+                _lib.call("gwb_ham_set_projectors", hl, None, None, s)
+            if self.tuning is not None:
+                _lib.call("gwb_ham_set_tuning", hl, int(self.tuning["w_budget_mb"]) << 20, 0)
+            rep = gb.rep_full_idx.to(dev)
+            self.pi = embed_real(gb, p[0][:, rep]).contiguous()     # (nproj, 2 nhalf - 1)
         i32 = dict(dtype=torch.int32, device=dev)
         self.src_half = gb.src_half.to(**i32).contiguous()
         self.conj_full = gb.conj_full.to(dev, torch.uint8).contiguous()
@@ -205,14 +229,15 @@ class GammaHamiltonian:
         return out
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            try:
-                torch.cuda.synchronize(self.device)
-                _lib.load().gwb_ham_destroy(h)
-            except Exception:
-                pass
-            self._h = None
+        for name in ("_h", "_h_loc"):
+            h = getattr(self, name, None)
+            if h is not None and h.value:
+                try:
+                    torch.cuda.synchronize(self.device)
+                    _lib.load().gwb_ham_destroy(h)
+                except Exception:
+                    pass
+                setattr(self, name, None)
 
     def apply_phi(self, phi: torch.Tensor, prec: int = _lib.GWB_FP64) -> torch.Tensor:
         """H on real embedded rows (nb, 2 nhalf - 1) float64 -> same shape."""
@@ -229,14 +254,18 @@ class GammaHamiltonian:
         if self.timing is not None:
             ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
             ev[0].record()
-        _lib.call("gwb_gamma_apply", self._h, nb, self.gb.nhalf, self.gb.npw, phi.data_ptr(), phi.shape[1],
-                  out.data_ptr(), out.shape[1], self.src_half.data_ptr(), self.conj_full.data_ptr(),
-                  self.rep_full.data_ptr(), self.partner_rep.data_ptr(), prec, self._work.data_ptr(),
-                  self._work.numel(), _lib.stream_ptr(self.device))
+        real_nl = prec == _lib.GWB_FP64 and self._h_loc is not None
+        _lib.call("gwb_gamma_apply", self._h_loc if real_nl else self._h, nb, self.gb.nhalf, self.gb.npw,
+                  phi.data_ptr(), phi.shape[1], out.data_ptr(), out.shape[1], self.src_half.data_ptr(),
+                  self.conj_full.data_ptr(), self.rep_full.data_ptr(), self.partner_rep.data_ptr(), prec,
+                  self._work.data_ptr(), self._work.numel(), _lib.stream_ptr(self.device))
+        nphi = 2 * self.gb.nhalf - 1
+        if real_nl:
+            becp = phi[:, :nphi] @ self.pi.T
+            out[:, :nphi].addmm_(becp @ self.dij, self.pi)
         if ev is not None:
             ev[1].record()
             self.timing.append((ev[0], ev[1], nb, prec))
-        nphi = 2 * self.gb.nhalf - 1
         if out.shape[1] > nphi:  # padded rows (the solver's even width) keep their pad at zero
             out[:, nphi:] = 0.0
         self.n_apply += nb

@@ -114,3 +114,19 @@ def test_bench_reference_arm_contract():
     assert line["impl"] == "reference" and line["higher_is_better"] is False and line["value"] > 0
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def test_autotune_records_and_lookup(tmp_path, monkeypatch):
+    """The autotuner's table: keys by apply kind, box and projector count; a
+    recorded choice is found, a missing one is None (built-in rules)."""
+    import json
+    from gradwave_b200 import autotune
+    p = tmp_path / "tuning.json"
+    k = autotune.key("gamma", (96, 96, 96), 864)
+    assert k == "gamma:96x96x96:p864"
+    p.write_text(json.dumps({"entries": {k: {"choice": {"w_budget_mb": 32, "nl_target": 296}}}}))
+    monkeypatch.setattr(autotune, "TUNING", p)
+    monkeypatch.setattr(autotune, "_CACHE", None)
+    assert autotune.lookup("gamma", (96, 96, 96), 864) == {"w_budget_mb": 32, "nl_target": 296}
+    assert autotune.lookup("complex", (96, 96, 96), 864) is None
+    monkeypatch.setattr(autotune, "_CACHE", None)
