@@ -12,8 +12,9 @@ seeded Gaussian vacancies. Our arm reports:
 
 * ``value``       device-timed ms per solve with the inputs resident in HBM
                   (CUDA events on the launching stream, max over ranks) of the
-                  product's fast form: on a Gamma-only cell the real
-                  (half-sphere) path with float32 expansion applies, float64
+                  product's fast form (``--solver``, default learned-mixed):
+                  on a Gamma-only cell the real (half-sphere) path with the
+                  learned preconditioner, float32 expansion applies, float64
                   certification and polish, locking and buffer bands; on a
                   multi-k cell the batched complex solver in its mixed mode
                   with the learned preconditioner;
@@ -73,6 +74,9 @@ sys.path.insert(0, str(ROOT))
 HA = 27.211386245988
 EIG_TOL_EV = 1e-8 * HA
 METRIC = "ms per converged band solve (eig err ≤1e-8 Ha): learned+mixed vs plain, 1 B200"
+# buffer bands of the Gamma headline form (measured on si216: 16 gives the
+# least time with the learned preconditioner)
+GAMMA_BUFFERS = 16
 GOLDEN = {"si2_fcc": "si2_fcc", "si8_cubic": "si8_cubic", "si64_cubic": "si64_cubic",
           "si216_vacancy": "si216_vacancy"}
 
@@ -436,10 +440,12 @@ def _gamma_line(args, ci, gold, dev, flush, ws, rank) -> dict:
     gh = GammaHamiltonian(gb, ci.v_eff_r, ci.p[0], ci.bk.dij_full, device=dev)
     x0_host = gamma_start(gb, ci.nbands, "cpu").pin_memory()
     x0_dev = x0_host.to(dev)
-    nbuf = 32 if args.n_buffer is None else args.n_buffer
+    nbuf = GAMMA_BUFFERS if args.n_buffer is None else args.n_buffer
+    mode, pc = _solver_choice(args.solver, dev)
+    mode = "mixed" if mode in ("mixed", "fp32exp") else "fp64"
 
     def fast(x0):
-        return davidson_gamma(gh, x0, tol=args.tol, max_iter=300, mode="mixed", n_buffer=nbuf)
+        return davidson_gamma(gh, x0, tol=args.tol, max_iter=300, mode=mode, n_buffer=nbuf, precond=pc)
 
     with ClockSampler(dev.index) as clk:
         for _ in range(args.warmup):
@@ -498,7 +504,9 @@ def _gamma_line(args, ci, gold, dev, flush, ws, rank) -> dict:
                        "npw": [int(gb.npw)], "nhalf": gb.nhalf, "tol_ev": args.tol,
                        "l2": "flushed (256 MiB write) between timed steps; basis 2 GB > L2",
                        "parallelism": f"replicas{ws}" if ws > 1 else "single"},
-            "solver": f"gamma-mixed (locking, {nbuf} buffer bands, TPA)",
+            "solver": f"gamma-{mode} (locking, {nbuf} buffer bands, "
+                      f"{'TPA' if isinstance(pc, str) else 'learned preconditioner'})",
+            "n_tpa_fallback": res.n_tpa_fallback,
             "eig_err_ev": err_fast, "eig_err_ha": None if err_fast is None else err_fast / HA,
             "n_iter": res.n_iter, "band_applies": {"fp32": tm["bands_fp32"], "fp64": tm["bands_fp64"]},
             "plain_fp64": {"value": round(ms_plain, 3), "unit": "ms", "n_iter": n_iter_plain,
