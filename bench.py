@@ -408,7 +408,8 @@ def _apply_roofline(tm: dict, rows_per_band: float, npw: float, n_box: float, np
             "frac": round(achieved / hbm_peak, 4), "peak_kind": peak_kind, "traffic": None,
             "launches": tm["calls"], "avg_launch_ms": round(tm["ms"] / max(1, tm["calls"]), 4),
             "share_of_step": round(tm["ms"] / max(1e-9, ms_step), 4),
-            "bytes_per_row": bytes_per_row, "bytes_per_launch": per_launch, "rows_per_step": rows}
+            "bytes_per_row": bytes_per_row, "fixed_bytes_per_launch": per_launch,
+            "alg_bytes_per_launch": round(alg / max(1, tm["calls"])), "rows_per_step": rows}
     # DRAM bytes per complex row of the float32 and float64 applies from the
     # committed ncu capture of the same apply kernels (one whole-block apply
     # of the workload; the figure per row is independent of the block size),
@@ -776,20 +777,27 @@ def run_tc(args):
 
 
 def run_oz(args):
-    """Float64 products on the int8 tensor cores (Ozaki scheme, ``--slices``)
-    next to cuBLAS DGEMM at the real Davidson shapes of the 216-atom Gamma
-    cell: A B^T with K = 80,798 (subspace / projection coefficients, Gram) and
-    A B with K = the basis (Ritz vectors, projection update); ``--warmup``
-    untimed and ``--steps`` timed calls each (CUDA events), error against the
-    float64 product relative to the operands' row maxima."""
+    """Float64 products on the int8 tensor cores next to cuBLAS DGEMM at the
+    real Davidson shapes of the 216-atom Gamma cell: A B^T with K = 80,798
+    (subspace / projection coefficients, Gram) and A B with K = the basis
+    (Ritz vectors, projection update). ``--oz-scheme slices``: the Ozaki
+    scheme's first form with ``--slices`` int8 slices; ``crt``: its second
+    form with ``--moduli`` residues. ``--warmup`` untimed and ``--steps``
+    timed calls each (CUDA events): the whole call (operands split on every
+    call) and the product alone on split operands; error against the float64
+    product relative to the operands' row maxima times sqrt(K) (``err``) and
+    relative to |A||B| (``err_abs_prod``)."""
     import torch
-    from gradwave_b200.oz import OzMatmul, check_status
+    from gradwave_b200.oz import CrtMatmul, OzMatmul, check_status
     dev = torch.device("cuda", 0)
     g = torch.Generator(device="cpu").manual_seed(0)
     npw = 80798
     decay = torch.exp(-torch.linspace(0.0, 8.0, npw, dtype=torch.float64))
-    om = OzMatmul(dev, s=args.slices)
-    out = {"mode": "oz", "slices": args.slices, "shapes": {}}
+    crt = args.oz_scheme == "crt"
+    om = CrtMatmul(dev, n=args.moduli) if crt else OzMatmul(dev, s=args.slices)
+    n_products = args.moduli if crt else args.slices * (args.slices + 1) // 2
+    out = {"mode": "oz", "scheme": args.oz_scheme, "moduli" if crt else "slices": args.moduli if crt else args.slices,
+           "int8_products": n_products, "shapes": {}}
 
     def ev(fn):
         for _ in range(args.warmup):
@@ -811,24 +819,35 @@ def run_oz(args):
             b = (torch.randn(N, K, dtype=torch.float64, generator=g) * decay).to(dev)
             c = torch.empty(M, N, dtype=torch.float64, device=dev)
             t_oz = ev(lambda: om.nt(a, b, c))
+            sa, sb = om._set("nt_a", M, K), om._set("nt_b", N, K)
+            t_prod = ev(lambda: om.gemm(M, N, K, sa, sb, c))
             ref = a @ b.T
             t_d = ev(lambda: torch.matmul(a, b.T, out=ref))
             sc = a.abs().amax(1)[:, None] * b.abs().amax(1)[None, :] * K ** 0.5
+            sabs = a.abs() @ b.abs().T
         else:
             a = torch.randn(M, K, dtype=torch.float64, generator=g).to(dev)
             b = (torch.randn(K, N, dtype=torch.float64, generator=g) * decay[:N]).to(dev)
             c = torch.empty(M, N, dtype=torch.float64, device=dev)
             t_oz = ev(lambda: om.nn(a, b, c))
+            sa, sb = om._set("nn_a", M, K), om._set("nn_b", N, K)
+            t_prod = ev(lambda: om.gemm(M, N, K, sa, sb, c, b_scaled=False))
             ref = a @ b
             t_d = ev(lambda: torch.matmul(a, b, out=ref))
             sc = a.abs() @ b.abs().amax(1, keepdim=True) + 1e-300
+            sabs = a.abs() @ b.abs()
+        om.nt(a, b, c) if form == "nt" else om.nn(a, b, c)
         check_status(dev)
         flop = 2.0 * M * N * K
-        out["shapes"][name] = {"M": M, "N": N, "K": K, "oz_ms": round(t_oz, 4), "dgemm_ms": round(t_d, 4),
-                               "speedup": round(t_d / t_oz, 3), "oz_tflops_equiv": round(flop / t_oz / 1e9, 1),
-                               "int8_tops_issued": round(flop * args.slices * (args.slices + 1) / 2 / t_oz / 1e9, 1),
-                               "err": float(((c - ref).abs() / sc).max())}
-        del a, b, c, ref
+        d = (c - ref).abs()
+        out["shapes"][name] = {"M": M, "N": N, "K": K, "oz_ms": round(t_oz, 4), "product_ms": round(t_prod, 4),
+                               "dgemm_ms": round(t_d, 4), "speedup": round(t_d / t_oz, 3),
+                               "speedup_product": round(t_d / t_prod, 3),
+                               "oz_tflops_equiv": round(flop / t_oz / 1e9, 1),
+                               "int8_tops_issued": round(flop * n_products / t_prod / 1e9, 1),
+                               "err": float((d / sc).max()),
+                               "err_abs_prod": float((d / (sabs + 1e-300)).max())}
+        del a, b, c, ref, sabs, d
     print(json.dumps(out), flush=True)
     return 0
 
@@ -867,7 +886,7 @@ def run_gamma(args):
            "wall_ms": wall,
            "band_applies": gh.n_apply - n0, "max_residual_ev": float(r.residual_norms.max()),
            "nhalf": gb.nhalf, "npw": gb.npw, "precond": "teter" if isinstance(pc, str) else "learned",
-           "n_tpa_fallback": r.n_tpa_fallback, "oz": os.environ.get("GWB_OZ", "0") == "1"}
+           "n_tpa_fallback": r.n_tpa_fallback, "oz": os.environ.get("GWB_OZ", "0")}
     if r.phase_ms:
         out["phase_ms"] = r.phase_ms
     gold = _golden(args.config)
@@ -917,6 +936,8 @@ def main():
     ap.add_argument("--n-buffer", type=int, default=None,
                     help="Gamma path: buffer bands above the wanted ones (default 32 in the bench line, 0 in --mode gamma)")
     ap.add_argument("--slices", type=int, default=8, help="--mode oz: int8 slices per float64 operand")
+    ap.add_argument("--oz-scheme", default="slices", choices=["slices", "crt"], help="--mode oz: Ozaki scheme form")
+    ap.add_argument("--moduli", type=int, default=18, help="--mode oz --oz-scheme crt: residues per operand")
     ap.add_argument("--mode", default="solve", choices=["solve", "apply", "apply_gamma", "once", "tc", "gamma", "oz"],
                     help="apply: only time Hamiltonian applies; once: a single solve (profiling)")
     ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64"], help="arithmetic of --mode apply")

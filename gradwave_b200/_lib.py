@@ -103,6 +103,13 @@ _SIGNATURES = {
     "gwb_oz_gemm": [_I, _I64, _I64, _I64, _P, _I64, _I64, _I64, _P, _P, _I64, _I64, _I64, _P, _D, _D, _P, _I64, _P,
                     _SZ, _P, _P],
     "gwb_tc_test_withhold": [_I],
+    "gwb_crt_bits": [_I],
+    "gwb_crt_constants": [_I, _P, _P, _P, _P, _P],
+    "gwb_crt_split_rows": [_I, _I64, _I64, _P, _I64, _P, _P, _I64, _I64, _I64, _P, _P],
+    "gwb_crt_split_cols": [_I, _I64, _I64, _P, _I64, _P, _I64, _I64, _I64, _P, _P, _P],
+    "gwb_crt_work_bytes": [_I, _I64, _I64, _I64],
+    "gwb_crt_gemm": [_I, _I64, _I64, _I64, _P, _I64, _I64, _I64, _P, _P, _I64, _I64, _I64, _P, _D, _D, _P, _I64,
+                     _P, _SZ, _P, _P],
     "gwb_zgemm_tc": [ctypes.c_int, _I64, _I64, _I64, _D, _D, _P, _I64, _I64, _P, _I64, _I64, _D, _D, _P, _I64, _I64,
                      _I64, _P, ctypes.c_size_t, _P, _P],
     "gwb_residual": [_I, _I, _I, _P, _I64, _P, _I64, _P, _I64, _P, _I64, _P, _P],
@@ -134,7 +141,8 @@ _RESTYPES = {"gwb_last_error": ctypes.c_char_p, "gwb_version": ctypes.c_char_p,
              "gwb_launch_count": ctypes.c_ulonglong,
              "gwb_ham_scratch_bytes": ctypes.c_size_t, "gwb_heev_scratch_doubles": ctypes.c_int64,
              "gwb_precond_learned_work_bytes": ctypes.c_int64, "gwb_zgemm_tc_work_bytes": ctypes.c_int64,
-             "gwb_gamma_work_bytes": ctypes.c_size_t, "gwb_oz_work_bytes": ctypes.c_int64}
+             "gwb_gamma_work_bytes": ctypes.c_size_t, "gwb_oz_work_bytes": ctypes.c_int64,
+             "gwb_crt_bits": ctypes.c_int32, "gwb_crt_work_bytes": ctypes.c_int64}
 
 
 def declared_symbols() -> list[str]:

@@ -274,6 +274,52 @@ int gwb_oz_gemm(int32_t s, int64_t M, int64_t N, int64_t K, const void* A, int64
                 const double* b_scale, double alpha, double beta, double* C, int64_t ldc, void* work,
                 size_t work_bytes, int* status, void* stream);
 
+/* Float64-accurate real products on the int8 tensor cores through residues
+ * (the Ozaki scheme's second form: the Chinese remainder theorem). A residue
+ * set is n (16, 18 or 20) int8 planes of rows_cap x ldk (ldk a multiple of 64,
+ * 16-byte aligned base), plane t at t rows_cap ldk, with one float64 scale
+ * per row: row r is scale[r] x_r with x_r an integer vector, |x_r| < 2^p
+ * (p = gwb_crt_bits(n): 52, 60, 67), plane t holding x_r mod m_t, centred
+ * (m_t = 256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211,
+ * 199, 197, 193, 191, 181, 179, 173: the first n). The float64 GEMMs of the
+ * Davidson subspace, Ritz, projection and Cholesky-QR steps (gradwave
+ * solvers/davidson.py:195-222,428-432,648-657) run on them; the reference
+ * has no counterpart.
+ *
+ * gwb_crt_bits: p for n moduli (-1 for an unsupported n).
+ * gwb_crt_constants: the moduli m_t, y_t = (M / m_t)^-1 mod m_t, 1/m_t as a
+ * double-double (inv_hi + inv_lo) and M = prod m_t as a double-double
+ * (M_hl[0] + M_hl[1]); host only, for inspection and tests. */
+int32_t gwb_crt_bits(int32_t n);
+int gwb_crt_constants(int32_t n, uint32_t* m, uint32_t* y, double* inv_hi, double* inv_lo, double* M_hl);
+/* gwb_crt_split_rows: rows [row0, row0 + rows) of the set from the rows of
+ * src (K columns, row stride ld_src), each element times fold[k] when fold is
+ * not NULL: scale[row0 + r] = 2^(e - p) with 2^e the power of two above the
+ * row's largest magnitude (NaN for a row with a non-finite value), x = the
+ * nearest integers to the row / scale; columns K..ldk-1 zeroed. */
+int gwb_crt_split_rows(int32_t n, int64_t rows, int64_t K, const double* src, int64_t ld_src, const double* fold,
+                       void* planes, int64_t ldk, int64_t rows_cap, int64_t row0, double* scale, void* stream);
+/* gwb_crt_split_cols: the transposed layout. src is krows x R (row stride
+ * ld_src); row r of the set gets, in columns k0 .. k0 + krows - 1, the
+ * residues of the nearest integer to 2^p src[k][r] / kscale[k0 + k], with
+ * kscale[k0 + k] the power of two above max_r |src[k][r]| (set here), and
+ * scale[r] = 2^-p. The B operand of C = A B (B = src) is this set, with kscale
+ * folded into A's rows by gwb_crt_split_rows. */
+int gwb_crt_split_cols(int32_t n, int64_t krows, int64_t R, const double* src, int64_t ld_src, void* planes,
+                       int64_t ldk, int64_t rows_cap, int64_t k0, double* kscale, double* scale, void* stream);
+/* C (M x N float64, row stride ldc) = alpha diag(a_scale) (A B^T) diag(b_scale)
+ * + beta C over K <= 2^19 columns, for rows a_row0.. of residue set A and
+ * b_row0.. of residue set B: n exact int8 products (int32 sums in tensor
+ * memory), each reduced modulo its m_t into a byte of `work`
+ * (gwb_crt_work_bytes), then the Chinese remainder reconstruction in
+ * double-double. Columns K..ceil(K/64)*64-1 of A must be zero. A pipeline
+ * wait that runs out ORs GWB_ERR_TIMEOUT into *status (device int). */
+int64_t gwb_crt_work_bytes(int32_t n, int64_t M, int64_t N, int64_t K);
+int gwb_crt_gemm(int32_t n, int64_t M, int64_t N, int64_t K, const void* A, int64_t lda, int64_t a_rows_cap,
+                 int64_t a_row0, const double* a_scale, const void* B, int64_t ldb, int64_t b_rows_cap,
+                 int64_t b_row0, const double* b_scale, double alpha, double beta, double* C, int64_t ldc, void* work,
+                 size_t work_bytes, int* status, void* stream);
+
 /* r = hx - eig * x and rn = |r| per (k, band); eig (nk, eig_kstride) float64.
  * Replaces gradwave solvers/davidson.py:656-657. */
 int gwb_residual(int32_t nk, int32_t nb, int32_t npw, const void* x, int64_t x_kstride, const void* hx,

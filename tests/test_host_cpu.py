@@ -16,7 +16,7 @@ def test_library_exports_every_declared_symbol():
     from gradwave_b200 import _lib
     lib = _lib.load()
     header = (ROOT / "include" / "gwb.h").read_text()
-    declared = set(re.findall(r"^\s*(?:int|int64_t|const char\*|size_t|unsigned long long)\s+(gwb_\w+)\(", header, re.M))
+    declared = set(re.findall(r"^\s*(?:int|int32_t|int64_t|const char\*|size_t|unsigned long long)\s+(gwb_\w+)\(", header, re.M))
     assert declared, "no declarations parsed"
     for name in declared:
         assert hasattr(lib, name), f"libgwb.so does not export {name}"
