@@ -886,7 +886,7 @@ def run_gamma(args):
            "wall_ms": wall,
            "band_applies": gh.n_apply - n0, "max_residual_ev": float(r.residual_norms.max()),
            "nhalf": gb.nhalf, "npw": gb.npw, "precond": "teter" if isinstance(pc, str) else "learned",
-           "n_tpa_fallback": r.n_tpa_fallback, "oz": os.environ.get("GWB_OZ", "0")}
+           "n_tpa_fallback": r.n_tpa_fallback, "oz": os.environ.get("GWB_OZ", "0"), "rounds": r.info}
     if r.phase_ms:
         out["phase_ms"] = r.phase_ms
     gold = _golden(args.config)

@@ -284,6 +284,7 @@ class GammaDavidsonResult:
     residual_norms: torch.Tensor  # (nb,)
     phase_ms: dict | None = None  # CUDA-event times per step (GWB_PROFILE=1)
     n_tpa_fallback: int = 0       # bands the learned preconditioner's stall rule sent to TPA
+    info: dict | None = None      # rounds per phase, hand-off residual
 
 
 def _orthonormalize(v: torch.Tensor, against: torch.Tensor | None = None) -> torch.Tensor:
@@ -298,35 +299,49 @@ def _orthonormalize(v: torch.Tensor, against: torch.Tensor | None = None) -> tor
 
 
 class _TcProjection:
-    """First projection pass of the expansion block on the tensor cores, for
-    the mixed schedule. The solver keeps its real rows at an even width, so a
-    row is also a complex row of half the length, and for such rows
-    Re(A B^H) is exactly the real product A B^T: the split-BF16 complex
-    kernels (``gradwave_b200.tc``) then compute the coefficients D V^T and the
-    update D -= C V (C real, imaginary part zero). The BF16 planes of the
-    basis are kept current row block by row block. A row that keeps less than
-    1e-2 of its unit norm would be dominated by the products' ~1e-6 error, so
-    then the block is redone in float64 (the complex path's rule)."""
+    """Products of the float32 phase of the mixed schedule on the tensor
+    cores. The solver keeps its real rows at an even width, so a row is also
+    a complex row of half the length, and for such rows Re(A B^H) is exactly
+    the real product A B^T, and a real coefficient matrix times complex rows
+    gives the real product's even and odd columns as its real and imaginary
+    parts: the split-BF16 complex kernels (``gradwave_b200.tc``, error about
+    1e-6 of sum_k |a||b|) then compute
+
+    * ``project``: the coefficients D V^T and the update D -= C V;
+    * ``subspace``: the new columns V HV_new^T of the subspace matrix;
+    * ``ritz``: the Ritz vectors U^T V and their images U^T HV.
+
+    The BF16 planes of the basis and of its images are kept current row block
+    by row block. In the float32 phase the applies themselves carry ~1e-7
+    relative error, and every convergence decision is made after a float64
+    certification of a re-orthonormalised block. A row that keeps less than
+    1e-2 of its unit norm in ``project`` would be dominated by the products'
+    error, so then the block is redone in float64 (the complex path's rule)."""
 
     def __init__(self, max_dim: int, nb: int, npad: int, dev):
         from .tc import PlaneSet
         self.nc = npad // 2
         self.pv = PlaneSet(1, max_dim, self.nc, dev)
+        self.ph = PlaneSet(1, max_dim, self.nc, dev)
         self.pt = PlaneSet(1, nb, self.nc, dev)
         self.pc = PlaneSet(1, nb, max_dim, dev)
         self.n_fallback = 0
 
-    def rows(self, v: torch.Tensor, r0: int, r1: int) -> None:
+    def _cx(self, t: torch.Tensor) -> torch.Tensor:
+        return torch.view_as_complex(t.view(t.shape[0], self.nc, 2))
+
+    def rows(self, v: torch.Tensor, hv: torch.Tensor | None, r0: int, r1: int) -> None:
         if r1 > r0:
-            vc = torch.view_as_complex(v.view(v.shape[0], self.nc, 2))
-            self.pv.write(vc, r1 - r0, row0=r0, src_ld=self.nc, src_kstride=0, offset=r0 * self.nc)
+            self.pv.write(self._cx(v), r1 - r0, row0=r0, src_ld=self.nc, src_kstride=0, offset=r0 * self.nc)
+            if hv is not None:
+                self.ph.write(self._cx(hv), r1 - r0, row0=r0, src_ld=self.nc, src_kstride=0, offset=r0 * self.nc)
 
     def project(self, t: torch.Tensor, v: torch.Tensor) -> torch.Tensor:
         from .tc import OP_H, OP_N, zgemm_tc
         n, m = t.shape[0], v.shape[0]
         t = t.contiguous()
         keep = t.clone()
-        tc = torch.view_as_complex(t.view(n, self.nc, 2))
+        tc = self._cx(t)
         self.pt.write(tc, n, src_ld=self.nc, src_kstride=0)
         c = torch.empty(n, m, dtype=torch.complex128, device=t.device)
         zgemm_tc(OP_H, n, m, self.nc, self.pt, self.pv, c, m, n * m)
@@ -337,6 +352,32 @@ class _TcProjection:
             self.n_fallback += 1
             return keep - (keep @ v.T) @ v
         return t
+
+    def subspace(self, hv_new: torch.Tensor, m: int, m0: int) -> torch.Tensor:
+        """V[:m] HV[m0:m]^T (m x (m - m0)); hv_new = HV[m0:m]. From m0 = 0
+        (after a restart) the kept planes of both serve directly."""
+        from .tc import OP_H, zgemm_tc
+        if m0 == 0:
+            c = torch.empty(m, m, dtype=torch.complex128, device=hv_new.device)
+            zgemm_tc(OP_H, m, m, self.nc, self.pv, self.ph, c, m, m * m)
+            return c.real
+        n = hv_new.shape[0]
+        self.pt.write(self._cx(hv_new.contiguous()), n, src_ld=self.nc, src_kstride=0)
+        c = torch.empty(n, m, dtype=torch.complex128, device=hv_new.device)
+        zgemm_tc(OP_H, n, m, self.nc, self.pt, self.pv, c, m, n * m)
+        return c.real.T
+
+    def ritz(self, ut: torch.Tensor, m: int):
+        """(U^T V[:m], U^T HV[:m]) for the real coefficients ut (n x m)."""
+        from .tc import OP_N, zgemm_tc
+        n = ut.shape[0]
+        self.pc.write(ut.to(torch.complex128), n, src_ld=m, src_kstride=0, cols=m)
+        out = []
+        for planes in (self.pv, self.ph):
+            o = torch.empty(n, 2 * self.nc, dtype=torch.float64, device=ut.device)
+            zgemm_tc(OP_N, n, self.nc, m, self.pc, planes, self._cx(o), self.nc, n * self.nc)
+            out.append(o)
+        return out[0], out[1]
 
 
 class _Products:
@@ -351,23 +392,25 @@ class _Products:
     changed are sliced again), and a product whose operand is a prefix
     ``V[:m]`` or ``HV[:m]`` reads the kept slices instead of slicing it."""
 
-    def __init__(self, dev=None, oz: bool = False):
+    def __init__(self, dev=None, oz: bool | str = False):
         self.om = None
         self.V = self.HV = None
         self.valid = 0
-        if oz:
+        if oz == "crt":
+            from .oz import CrtMatmul
+            self.om = CrtMatmul(dev)
+        elif oz:
             from .oz import OzMatmul
             self.om = OzMatmul(dev)
 
     def attach(self, V: torch.Tensor, HV: torch.Tensor) -> None:
         if self.om is None:
             return
-        from .oz import SliceSet
         rows, npad = V.shape
         self.V, self.HV = V, HV
-        self.v_rows = SliceSet(rows, npad, V.device, self.om.s)   # rows of V (a b^T operands)
-        self.v_cols = SliceSet(npad, rows, V.device, self.om.s)   # V^T: the B of  . @ V
-        self.hv_cols = SliceSet(npad, rows, V.device, self.om.s)  # HV^T: the B of . @ HV
+        self.v_rows = self.om.new_set(rows, npad)   # rows of V (a b^T operands)
+        self.v_cols = self.om.new_set(npad, rows)   # V^T: the B of  . @ V
+        self.hv_cols = self.om.new_set(npad, rows)  # HV^T: the B of . @ HV
         self.valid = 0
 
     def rows_changed(self, r0: int, r1: int) -> None:
@@ -391,30 +434,28 @@ class _Products:
     def nt(self, a: torch.Tensor, b: torch.Tensor, same: bool = False) -> torch.Tensor:
         if self.om is None or a.shape[0] == 0 or b.shape[0] == 0:
             return a @ b.T
-        from .oz import oz_gemm
         a = self._rows(a)
         b = a if same else self._rows(b)
         out = torch.empty(a.shape[0], b.shape[0], dtype=torch.float64, device=a.device)
         if not same and self._prefix(a, self.V):      # V[:m] b^T
             sb = self.om._set("nt_b", b.shape[0], b.shape[1])
             sb.split_rows(b)
-            oz_gemm(a.shape[0], b.shape[0], a.shape[1], self.v_rows, sb, out)
+            self.om.gemm(a.shape[0], b.shape[0], a.shape[1], self.v_rows, sb, out)
             return out
         if not same and self._prefix(b, self.V):      # a V[:m]^T
             sa = self.om._set("nt_a", a.shape[0], a.shape[1])
             sa.split_rows(a)
-            oz_gemm(a.shape[0], b.shape[0], a.shape[1], sa, self.v_rows, out)
+            self.om.gemm(a.shape[0], b.shape[0], a.shape[1], sa, self.v_rows, out)
             return out
         return self.om.nt(a, b, out, same=same)
 
     def _nn_into(self, a: torch.Tensor, b: torch.Tensor, out: torch.Tensor, alpha: float, beta: float) -> None:
-        from .oz import oz_gemm
         for base, cols in ((self.V, getattr(self, "v_cols", None)), (self.HV, getattr(self, "hv_cols", None))):
             if self._prefix(b, base):
                 m = b.shape[0]
                 sa = self.om._set("nn_a", a.shape[0], m)
                 sa.split_rows(a.contiguous(), fold=cols.kscale)
-                oz_gemm(a.shape[0], b.shape[1], m, sa, cols, out, alpha, beta, b_scaled=False)
+                self.om.gemm(a.shape[0], b.shape[1], m, sa, cols, out, alpha, beta, b_scaled=False)
                 return
         self.om.nn(a.contiguous(), self._rows(b), out, alpha, beta)
 
@@ -454,8 +495,24 @@ def _cholqr(y: torch.Tensor, mm: _Products = _CUBLAS):
     return mm.nn(torch.linalg.solve_triangular(L, eye, upper=False), y)
 
 
+def _cholqr_images(x: torch.Tensor, hx: torch.Tensor, mm: _Products = _CUBLAS):
+    """Cholesky-QR of the rows of x in float64 (twice; Householder QR if that
+    breaks down), with the same triangular transform applied to their images
+    hx, so that the pair stays (block, H block)."""
+    for _ in range(2):
+        L, info = torch.linalg.cholesky_ex(mm.nt(x, x, same=True))
+        if int(info.max()) != 0 or float(torch.diagonal(L).min()) <= 1e-8:
+            q, r = torch.linalg.qr(x.T, mode="reduced")
+            rinv = torch.linalg.solve_triangular(r, torch.eye(r.shape[0], dtype=r.dtype, device=r.device),
+                                                 upper=True)
+            return q.T.contiguous(), mm.nn(rinv.T.contiguous(), hx)
+        li = torch.linalg.solve_triangular(L, torch.eye(L.shape[0], dtype=L.dtype, device=L.device), upper=False)
+        x, hx = mm.nn(li, x), mm.nn(li, hx)
+    return x, hx
+
+
 def _expand(t: torch.Tensor, v: torch.Tensor, tcp: _TcProjection | None = None,
-            locked: torch.Tensor | None = None, mm: _Products = _CUBLAS) -> torch.Tensor:
+            locked: torch.Tensor | None = None, mm: _Products = _CUBLAS, low: bool = False) -> torch.Tensor:
     """New directions from preconditioned residuals: unit rows, two
     projections against the orthonormal basis v (and the locked rows, which
     are orthogonal to v), then Cholesky-QR; Householder QR dropping rows that
@@ -469,9 +526,23 @@ def _expand(t: torch.Tensor, v: torch.Tensor, tcp: _TcProjection | None = None,
     rounds). Unit rows and a relative threshold, as the batched Davidson does
     (``:406-457``), remove that floor. The second Cholesky-QR round is skipped
     when the first already left the Gram matrix within 1e-13 of the identity
-    (it would change the rows by that much)."""
+    (it would change the rows by that much).
+
+    ``low`` (the float32 phase, with ``tcp``): both projection passes on the
+    tensor cores, each followed by a float64 Cholesky-QR. The first leaves
+    components along v of ~1e-6 that the Cholesky-QR may amplify by the
+    block's condition number; the second pass brings them back to ~1e-6 of
+    unit rows, and the second Cholesky-QR (of a nearly orthonormal block)
+    restores orthonormality among the new rows. The basis of the float32
+    phase is thus orthonormal to ~1e-6, the level of its float32 applies."""
     t = t / torch.linalg.vector_norm(t, dim=1, keepdim=True).clamp_min(1e-300)
     lk = locked if locked is not None else v[:0]
+    if low and tcp is not None and lk.shape[0] == 0:
+        y = _cholqr(tcp.project(t, v), mm)
+        if y is not None:
+            y2 = _cholqr(tcp.project(y, v), mm)
+            if y2 is not None:
+                return y2
     _project_out(t, lk, mm)
     t = tcp.project(t, v) if tcp is not None else _project_out(t, v, mm)
     _project_out(_project_out(t, lk, mm), v, mm)
@@ -677,10 +748,21 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
     t_phi = torch.nn.functional.pad(ham.t_phi, (0, npad - nphi))
     tcp = _TcProjection(rows, nb, npad, dev) if (mode == "mixed" and dev.type == "cuda"
                                                  and os.environ.get("GWB_TC_PROJECT", "1") != "0") else None
-    # float64 products: cuBLAS DGEMM, or with GWB_OZ=1 the int8 tensor-core
-    # products (measured on this path: no faster than DGEMM at these shapes,
+    # float64 products: cuBLAS DGEMM; with GWB_OZ=crt the int8 tensor-core
+    # products through residues (18 moduli), with GWB_OZ=1 through 8 int8
+    # slices (measured on this path: no faster than DGEMM at these shapes,
     # and a residual floor just above 1e-10 eV on the 216-atom cell)
-    mm = _Products(dev, oz=dev.type == "cuda" and os.environ.get("GWB_OZ", "0") == "1")
+    oz_mode = os.environ.get("GWB_OZ", "0")
+    mm = _Products(dev, oz=("crt" if oz_mode == "crt" else oz_mode == "1") if dev.type == "cuda" else False)
+    # the float32 phase's subspace, Ritz and projection products on the
+    # tensor cores (GWB_TC_LOW=0: only the first projection pass there) while
+    # the largest residual stays above GWB_TC_SWITCH (default 30) times the
+    # float32 floor; below it the basis collapses to the Ritz block made
+    # orthonormal in float64 and the float32 phase continues on float64
+    # products, so that the hand-off block is as good as without them
+    tc_low_on = tcp is not None and os.environ.get("GWB_TC_LOW", "1") != "0"
+    tc_switch = float(os.environ.get("GWB_TC_SWITCH", "30"))
+    info = {"rounds_tc": 0, "rounds_f32": 0, "rounds_f64": 0, "handoff_rn_ev": None, "m": []}
     v0 = _orthonormalize(phi0.clone())
     if v0.shape[0] < nb:  # degenerate start: pad with seeded noise (``:345-350``)
         gen = torch.Generator(device="cpu").manual_seed(1234)
@@ -691,13 +773,13 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
     HV = torch.empty(rows, npad, dtype=torch.float64, device=dev)
     m = nb
     V[:m] = v0
-    if tcp is not None:
-        tcp.rows(V, 0, m)
     low = mode == "mixed"
     f32, f64 = _lib.GWB_FP32, _lib.GWB_FP64
     cert_floor = 32.0 * float(torch.finfo(torch.float32).eps) * max(float(t_phi.max()), 1.0)
     prev = float("inf")
     HV[:m] = ham.apply_phi(V[:m], prec=f32 if low else f64)
+    if tcp is not None:
+        tcp.rows(V, HV, 0, m)
     mm.attach(V, HV)
     mm.rows_changed(0, m)
     locked = _Locked(nwant, npad, dev)
@@ -712,7 +794,16 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
 
     def certify(x):
         """Float64 apply of the Ritz block and its nb x nb Rayleigh-Ritz
-        (gradwave ``solvers/davidson.py:281-308``)."""
+        (gradwave ``solvers/davidson.py:281-308``). After a float32 phase on
+        the tensor cores the block is first made orthonormal in float64
+        (Cholesky-QR twice; Householder QR if that breaks down)."""
+        if tc_low_on and tc_active:
+            y = _cholqr(x, mm)
+            y = _cholqr(y, mm) if y is not None else None
+            if y is None:
+                q, _ = torch.linalg.qr(x.T, mode="reduced")
+                y = q.T.contiguous()
+            x = y
         hx = ham.apply_phi(x, prec=f64)
         g = mm.nt(x, hx)
         w2, u2 = torch.linalg.eigh(0.5 * (g + g.T))
@@ -723,31 +814,58 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
     def finish(eig, x, rn, nw_a, it):
         e, xx, r = locked.merge(eig[:nw_a], x[:nw_a], rn[:nw_a])
         return GammaDavidsonResult(e, unembed_real(gb, xx[:, :nphi]), it, r, prof.summary(),
-                                   0 if learned is None else learned.n_fallback())
+                                   0 if learned is None else learned.n_fallback(), info)
 
+    def phase(name):
+        """Phase timer; the float32 phase's share is reported as name/f32."""
+        return prof(name + ("/f32" if low else ""))
+
+    tc_active = tc_low_on and low
     it = 0
     for it in range(1, max_iter + 1):
         nb_a = nb - locked.n      # active Ritz block
         nw_a = nwant - locked.n   # wanted pairs still in it
         v, hv = V[:m], HV[:m]
-        with prof("subspace_gemm"):
-            blk = mm.nt(v, hv[m0:m])                   # (m, m - m0)
+        tc_low = low and tc_active
+        info["rounds_tc" if tc_low else ("rounds_f32" if low else "rounds_f64")] += 1
+        info["m"].append(m)
+        with phase("subspace_gemm"):
+            blk = tcp.subspace(hv[m0:m], m, m0) if tc_low else mm.nt(v, hv[m0:m])  # (m, m - m0)
             S[:m, m0:m] = blk
             S[m0:m, :m0] = blk[:m0].T
             S[m0:m, m0:m] = 0.5 * (blk[m0:] + blk[m0:].T)
             m0 = m
             s = S[:m, :m]
-        with prof("eigh"):
+        with phase("eigh"):
             w, u = torch.linalg.eigh(s)
         eig = w[:nb_a]
-        with prof("ritz_gemm"):
+        with phase("ritz_gemm"):
             ut = u[:, :nb_a].T
-            x = mm.nn(ut, v)
-            hx = mm.nn(ut, hv)
-        with prof("residual"):
+            if tc_low:
+                x, hx = tcp.ritz(ut.contiguous(), m)
+            else:
+                x = mm.nn(ut, v)
+                hx = mm.nn(ut, hv)
+        with phase("residual"):
             r = hx - eig[:, None] * x
             rn = torch.linalg.vector_norm(r, dim=1)
             rmax = float(rn[:nw_a].max())
+        if tc_low and rmax < tc_switch * cert_floor:
+            # leave the tensor-core products: the Ritz block, orthonormal in
+            # float64, becomes the basis (its float32 images transformed alike)
+            with phase("restart"):
+                xo, hxo = _cholqr_images(x.contiguous(), hx.contiguous(), mm)
+                V[:nb_a] = xo
+                HV[:nb_a] = hxo
+                m, m0 = nb_a, 0
+                x, hx = V[:nb_a], HV[:nb_a]
+                v, hv = V[:m], HV[:m]
+                r = hx - eig[:, None] * x
+                rn = torch.linalg.vector_norm(r, dim=1)
+                rmax = float(rn[:nw_a].max())
+                tcp.rows(V, None, 0, m)
+                mm.rows_changed(0, m)
+                tc_active = False
         if low:
             stalled = it > 1 and rmax > 0.7 * prev and rmax < 100.0 * cert_floor
             prev = rmax
@@ -755,38 +873,41 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
                 with prof("certify"):
                     x, hx, eig, r, rn = certify(x)
                     rmax = float(rn[:nw_a].max())
+                info["handoff_rn_ev"] = rmax
                 if rmax >= tol:  # hand-off: float64 from the certified block on
                     low = False
+                    tc_active = False
                     V[:nb_a] = x
                     HV[:nb_a] = hx
                     m, m0 = nb_a, 0
                     x, hx = V[:nb_a], HV[:nb_a]
                     v, hv = V[:m], HV[:m]
                     if tcp is not None:
-                        tcp.rows(V, 0, m)
+                        tcp.rows(V, HV, 0, m)
                     mm.rows_changed(0, m)
-        with prof("residual"):
+        with phase("residual"):
             unconv = rn > tol
             if n_buffer:
                 unconv[nw_a:] = rn[nw_a:] > max(tol, buffer_tol)
             done = rmax <= tol
         if done:
             return finish(eig, x, rn, nw_a, it)
-        with prof("orthonormalize"):
+        with phase("precondition"):
             if learned is not None:
                 pr = learned(x, r, rn, eig, torch.nonzero(unconv).flatten(), npad)
             else:
                 t_band = (x * x * t_phi[None, :]).sum(dim=1)
                 pr = _teter(r[unconv], t_phi, t_band[unconv])
             pr[:, nphi:] = 0.0  # the pad column is not a coordinate of the operator
-            t = _expand(pr, v, tcp, locked.rows(), mm)
+        with phase("orthonormalize"):
+            t = _expand(pr, v, tcp, locked.rows(), mm, low=low and tc_active)
         if t.shape[0] == 0:  # no independent direction left
             if low:
                 x, hx, eig, r, rn = certify(x)
             return finish(eig, x, rn, nw_a, it)
-        with prof("apply"):
+        with phase("apply"):
             ht = ham.apply_phi(t, prec=f32 if low else f64)
-        with prof("restart"):
+        with phase("restart"):
             nt = int(t.shape[0])
             lockable = (rn[:nw_a] <= tol) if (lock and not low) else None
             n_lock = int(lockable.sum()) if lockable is not None else 0
@@ -813,7 +934,7 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
             HV[m:m + nt] = ht
             m += nt
             if tcp is not None:
-                tcp.rows(V, r0, m)
+                tcp.rows(V, HV if (low and tc_active) else None, r0, m)
             mm.rows_changed(r0, m)
     if low:  # out of rounds in float32: certify what there is
         x, hx, eig, r, rn = certify(x)

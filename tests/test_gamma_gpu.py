@@ -77,8 +77,9 @@ def test_gamma_davidson_si2_matches_reference(cuda_device):
                                            ("mixed", 1e-10, 32)])
 def test_gamma_davidson_si216_matches_complex_reference(cuda_device, mode, tol, nbuf):
     """si216 on the Gamma path, float64 and mixed (float32 expansion applies,
-    float64 certification and hand-off, converged pairs locked), with and
-    without buffer bands, to 1e-6 and 1e-10 eV."""
+    its first rounds on split-BF16 tensor-core products, float64
+    certification and hand-off, converged pairs locked), with and without
+    buffer bands, to 1e-6 and 1e-10 eV."""
     from gradwave_b200.gamma import davidson_gamma, gamma_start
     gc = load_golden("si216_vacancy")
     ci, gb, gh = _gamma("si216_vacancy", cuda_device)
@@ -87,6 +88,10 @@ def test_gamma_davidson_si216_matches_complex_reference(cuda_device, mode, tol, 
     eig = res.eigenvalues.cpu().numpy()
     assert float(res.residual_norms.max()) < tol
     assert np.abs(eig - gc["eigenvalues"][0]).max() < 1e-8 * HA
+    if mode == "mixed":
+        # the float32 phase ran its first rounds on the tensor-core products
+        # and handed a float64-orthonormal block to the float64 phase
+        assert res.info["rounds_tc"] > 0 and res.info["rounds_f64"] > 0
 
 
 def test_gamma_apply_accepts_transposed_blocks(cuda_device):
