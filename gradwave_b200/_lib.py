@@ -103,6 +103,7 @@ _SIGNATURES = {
     "gwb_oz_gemm": [_I, _I64, _I64, _I64, _P, _I64, _I64, _I64, _P, _P, _I64, _I64, _I64, _P, _D, _D, _P, _I64, _P,
                     _SZ, _P, _P],
     "gwb_tc_test_withhold": [_I],
+    "gwb_ham_set_fft_threads": [_P, _I, _I],
     "gwb_crt_bits": [_I],
     "gwb_crt_constants": [_I, _P, _P, _P, _P, _P],
     "gwb_crt_split_rows": [_I, _I64, _I64, _P, _I64, _P, _P, _I64, _I64, _I64, _P, _P],

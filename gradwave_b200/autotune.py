@@ -9,7 +9,10 @@ projector count and the GPU:
   chunks mean fewer, larger launches;
 * the number of CTAs the G-sliced projector contraction aims for
   (``nl_target``): more slices fill the SMs, more partial sums cost a
-  reduction.
+  reduction;
+* the threads per block of the shared-memory FFT kernels of the 72^3 and
+  96^3 boxes, per precision (``fft_threads``): a float64 96^3 plane fills an
+  SM's shared memory, so its block's warps are all the latency hiding there is.
 
 ``tune(config)`` times whole-block applies of a workload (float32 and float64
 arithmetic, CUDA events, several repetitions) over a grid of both values and
@@ -51,10 +54,18 @@ def lookup(kind: str, shape, nproj: int) -> dict | None:
 
 
 def apply_tuning(handle, kind: str, shape, nproj: int) -> dict | None:
-    """Set the recorded choice (if any) on a libgwb handle; returns it."""
+    """Set the recorded choice (if any) on a libgwb handle; returns it.
+    ``GWB_FFT_THREADS=fp32,fp64`` overrides the FFT block threads."""
+    import os
     ch = lookup(kind, shape, nproj)
     if ch is not None:
         _lib.call("gwb_ham_set_tuning", handle, int(ch["w_budget_mb"]) << 20, int(ch["nl_target"]))
+    nt = os.environ.get("GWB_FFT_THREADS")
+    if nt:
+        n32, n64 = (int(x) for x in nt.split(","))
+        _lib.call("gwb_ham_set_fft_threads", handle, n32, n64)
+    elif ch is not None and "fft_threads" in ch:
+        _lib.call("gwb_ham_set_fft_threads", handle, int(ch["fft_threads"][0]), int(ch["fft_threads"][1]))
     return ch
 
 
@@ -113,11 +124,23 @@ def tune(config: str, budgets_mb=(16, 24, 32, 48, 64, 96, 128), targets=(148, 29
     _lib.call("gwb_ham_set_tuning", handle, 0, 0)
     base = {"fp32_ms": round(timed(_lib.GWB_FP32), 4), "fp64_ms": round(timed(_lib.GWB_FP64), 4)}
     best = min(rows, key=lambda r: r["fp32_ms"] + r["fp64_ms"])
+    _lib.call("gwb_ham_set_tuning", handle, int(best["w_budget_mb"]) << 20, int(best["nl_target"]))
+    threads = []
+    for nt in (256, 512, 1024):
+        _lib.call("gwb_ham_set_fft_threads", handle, nt, nt)
+        threads.append({"threads": nt, "fp32_ms": round(timed(_lib.GWB_FP32), 4),
+                        "fp64_ms": round(timed(_lib.GWB_FP64), 4)})
+    _lib.call("gwb_ham_set_fft_threads", handle, 0, 0)
+    n32 = min(threads, key=lambda r: r["fp32_ms"])["threads"]
+    n64 = min(threads, key=lambda r: r["fp64_ms"])["threads"]
+    t32 = min(r["fp32_ms"] for r in threads)
+    t64 = min(r["fp64_ms"] for r in threads)
     entry = {"config": config, "kind": kind, "bands": int(ci.nbands), "gpu": torch.cuda.get_device_name(dev),
              "timing": f"CUDA events, {steps} applies after {warmup}", "built_in_rule": base,
-             "choice": {"w_budget_mb": best["w_budget_mb"], "nl_target": best["nl_target"]},
-             "gain": round((base["fp32_ms"] + base["fp64_ms"]) / (best["fp32_ms"] + best["fp64_ms"]), 4),
-             "table": rows}
+             "choice": {"w_budget_mb": best["w_budget_mb"], "nl_target": best["nl_target"],
+                        "fft_threads": [n32, n64]},
+             "gain": round((base["fp32_ms"] + base["fp64_ms"]) / (t32 + t64), 4),
+             "table": rows, "fft_threads_table": threads}
     return key(kind, ci.shape, nproj), entry
 
 

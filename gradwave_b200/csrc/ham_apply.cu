@@ -104,6 +104,7 @@ struct gwb_ham {
   // tuning (gwb_ham_set_tuning; 0 = the built-in rule)
   size_t w_budget = 0;   // bytes of FFT scratch W per band chunk
   int nl_target = 0;     // CTAs the G-sliced becp contraction aims for
+  int fft_nt[2] = {0, 0};  // threads of the shared-memory FFT blocks (float32, float64); 0: the built-in rule
 };
 
 namespace gwb {
@@ -141,8 +142,15 @@ static size_t w_budget_bytes() {
 
 // ---------------------------------------------------------------------------
 // K1: sphere scatter + inverse FFT along axes 2 and 1, one plane per CTA.
-template <typename T, typename SIO, unsigned C1, unsigned C2>
-__global__ void __launch_bounds__(256, (C1 && C2) ? 3 : 1) k_plane_inverse(FftGeom g, const int* __restrict__ plane_ptr,
+// Blocks per SM the shared-memory FFT kernels are compiled for: three 256-thread
+// blocks (the 72^3 and 96^3 planes of float32 fit three per SM), one block of
+// 512 or 1024 threads (float64 planes fill the shared memory with one).
+template <typename T, int NT, bool CT> constexpr int fft_minb() {
+  return !CT ? 1 : (NT == 256 ? 3 : (NT == 512 && sizeof(T) == 4 ? 2 : 1));
+}
+
+template <typename T, typename SIO, unsigned C1, unsigned C2, int NT = 256>
+__global__ void __launch_bounds__(NT, (fft_minb<T, NT, (C1 && C2)>())) k_plane_inverse(FftGeom g, const int* __restrict__ plane_ptr,
                                                        const int* __restrict__ plane_g,
                                                        const int* __restrict__ plane_pos,
                                                        const SIO* __restrict__ c, cplx<T>* __restrict__ W,
@@ -170,8 +178,8 @@ __global__ void __launch_bounds__(256, (C1 && C2) ? 3 : 1) k_plane_inverse(FftGe
 }
 
 // K2: pencils along axis 0 for one (i1, band, k): inverse FFT, x v(r)/N, forward FFT.
-template <typename T, unsigned C0>
-__global__ void __launch_bounds__(256, C0 ? 3 : 1) k_pencil_vloc(FftGeom g, cplx<T>* __restrict__ W,
+template <typename T, unsigned C0, int NT = 256>
+__global__ void __launch_bounds__(NT, (fft_minb<T, NT, (C0 != 0)>())) k_pencil_vloc(FftGeom g, cplx<T>* __restrict__ W,
                                                      const T* __restrict__ v,
                                                      const cplx<T>* __restrict__ tw0, int nbc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -452,8 +460,8 @@ __global__ void __launch_bounds__(PLR * N) k_plane_forward_reg(
 }
 
 // K3: forward FFT along axes 1 and 2, sphere gather, + t c, padding zeroed.
-template <typename T, typename SIO, unsigned C1, unsigned C2>
-__global__ void __launch_bounds__(256, (C1 && C2) ? 3 : 1) k_plane_forward(
+template <typename T, typename SIO, unsigned C1, unsigned C2, int NT = 256>
+__global__ void __launch_bounds__(NT, (fft_minb<T, NT, (C1 && C2)>())) k_plane_forward(
     FftGeom g, const int* __restrict__ plane_ptr, const int* __restrict__ plane_g,
     const int* __restrict__ plane_pos, const int* __restrict__ npw, const SIO* __restrict__ c,
     SIO* __restrict__ out, const cplx<T>* __restrict__ W, const T* __restrict__ t,
@@ -780,6 +788,24 @@ static int nl_slices(const gwb_ham* h, int nb) {
 // runtime-plan kernels.
 constexpr unsigned kCode24 = 0x38u, kCode36 = 0x334u, kCode72 = 0x338u, kCode96 = 0x348u;
 
+// The shared-memory kernels of one band chunk (K1, K2, K3) with NT threads per block.
+template <typename T, typename SIO, unsigned C, int NT>
+static int local_shared(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t ok, cplx<T>* W, const T* v,
+                        const T* t, const cplx<T>* tw0, const cplx<T>* tw1, const cplx<T>* tw2, int b0, int cb,
+                        cudaStream_t st, size_t smA, size_t smB) {
+  const FftGeom& g = h->g;
+  GWB_CUDA_TRY(allow_smem(k_plane_inverse<T, SIO, C, C, NT>));
+  GWB_CUDA_TRY(allow_smem(k_plane_forward<T, SIO, C, C, NT>));
+  GWB_CUDA_TRY(allow_smem(k_pencil_vloc<T, C, NT>));
+  dim3 gA(g.L[0], cb, h->nk), gB(g.n[1], cb, h->nk);
+  k_plane_inverse<T, SIO, C, C, NT><<<gA, NT, smA, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos, c, W, tw1,
+                                                        tw2, ck, b0, cb, h->npw_max);
+  k_pencil_vloc<T, C, NT><<<gB, NT, smB, st>>>(g, W, v, tw0, cb);
+  k_plane_forward<T, SIO, C, C, NT><<<gA, NT, smA, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos, h->d_npw,
+                                                        c, out, W, t, tw1, tw2, ck, ok, b0, cb, h->npw_max);
+  return GWB_OK;
+}
+
 template <typename T, typename SIO, unsigned C>
 static int local_chunks(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t ok, int nb, int nbc,
                         cudaStream_t st, size_t smA, size_t smB) {
@@ -790,9 +816,6 @@ static int local_chunks(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t 
   const cplx<T>* tw2 = dbl ? (const cplx<T>*)h->d_tw64[2] : (const cplx<T>*)h->d_tw32[2];
   const T* v = dbl ? (const T*)h->d_v64 : (const T*)h->d_v32;
   const T* t = dbl ? (const T*)h->d_t64 : (const T*)h->d_t32;
-  GWB_CUDA_TRY(allow_smem(k_plane_inverse<T, SIO, C, C>));
-  GWB_CUDA_TRY(allow_smem(k_plane_forward<T, SIO, C, C>));
-  GWB_CUDA_TRY(allow_smem(k_pencil_vloc<T, C>));
   cplx<T>* W = (cplx<T>*)h->d_W;
   const bool cubic = g.n[0] == g.n[1] && g.n[1] == g.n[2];
   const int nreg = (cubic && g.n[0] == 36 && C == kCode36) ? 36 : ((cubic && g.n[0] == 24 && C == kCode24) ? 24 : 0);
@@ -821,12 +844,21 @@ static int local_chunks(gwb_ham* h, const SIO* c, int64_t ck, SIO* out, int64_t 
       k_plane_forward_reg<T, SIO, 24><<<gP, PLR * 24, smR, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos,
                                                                  h->d_npw, c, out, W, t, ck, ok, b0, cb, h->npw_max);
     } else {
-      k_plane_inverse<T, SIO, C, C><<<gA, 256, smA, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos, c, W,
-                                                         tw1, tw2, ck, b0, cb, h->npw_max);
-      k_pencil_vloc<T, C><<<gB, 256, smB, st>>>(g, W, v, tw0, cb);
-      k_plane_forward<T, SIO, C, C><<<gA, 256, smA, st>>>(g, h->d_plane_ptr, h->d_plane_g, h->d_plane_pos,
-                                                         h->d_npw, c, out, W, t, tw1, tw2, ck, ok, b0, cb,
-                                                         h->npw_max);
+      // threads per block of the large compile-time boxes (72^3, 96^3):
+      // gwb_ham_set_fft_threads, else 512 (float32: two 73 KB planes per SM)
+      // and 1024 (float64: one 147 KB plane per SM). Measured on the 96^3
+      // box of si216, 480 bands: float32 6.35 -> 6.26 ms, float64 16.7 ->
+      // 12.0 ms against 256 threads.
+      const int nt = h->fft_nt[dbl ? 1 : 0] ? h->fft_nt[dbl ? 1 : 0] : (dbl ? 1024 : 512);
+      int rc = GWB_OK;
+      if constexpr (C == kCode96 || C == kCode72) {
+        if (nt == 1024) rc = local_shared<T, SIO, C, 1024>(h, c, ck, out, ok, W, v, t, tw0, tw1, tw2, b0, cb, st, smA, smB);
+        else if (nt == 512) rc = local_shared<T, SIO, C, 512>(h, c, ck, out, ok, W, v, t, tw0, tw1, tw2, b0, cb, st, smA, smB);
+        else rc = local_shared<T, SIO, C, 256>(h, c, ck, out, ok, W, v, t, tw0, tw1, tw2, b0, cb, st, smA, smB);
+      } else {
+        rc = local_shared<T, SIO, C, 256>(h, c, ck, out, ok, W, v, t, tw0, tw1, tw2, b0, cb, st, smA, smB);
+      }
+      if (rc != GWB_OK) return rc;
     }
     GWB_LAUNCH_CHECK();
     count_launches(3);
@@ -1286,6 +1318,15 @@ int gwb_ham_set_tuning(gwb_ham* h, int64_t w_budget_bytes, int32_t nl_target_cta
   GWB_REQUIRE(w_budget_bytes >= 0 && nl_target_ctas >= 0, "tuning values must be >= 0");
   h->w_budget = (size_t)w_budget_bytes;
   h->nl_target = nl_target_ctas;
+  return GWB_OK;
+}
+
+int gwb_ham_set_fft_threads(gwb_ham* h, int32_t threads_fp32, int32_t threads_fp64) {
+  GWB_REQUIRE(h, "null handle");
+  auto ok = [](int32_t n) { return n == 0 || n == 256 || n == 512 || n == 1024; };
+  GWB_REQUIRE(ok(threads_fp32) && ok(threads_fp64), "FFT block threads must be 0, 256, 512 or 1024");
+  h->fft_nt[0] = threads_fp32;
+  h->fft_nt[1] = threads_fp64;
   return GWB_OK;
 }
 

@@ -201,8 +201,7 @@ class GammaHamiltonian:
                 _lib.call("gwb_ham_set_kinetic", hl, self.t.data_ptr(), s)
                 _lib.call("gwb_ham_set_potential", hl, self.v.data_ptr(), s)
                 _lib.call("gwb_ham_set_projectors", hl, None, None, s)
-            if self.tuning is not None:
-                _lib.call("gwb_ham_set_tuning", hl, int(self.tuning["w_budget_mb"]) << 20, 0)
+            apply_tuning(hl, "gamma", self.shape, self.nproj)
             rep = gb.rep_full_idx.to(dev)
             self.pi = embed_real(gb, p[0][:, rep]).contiguous()     # (nproj, 2 nhalf - 1)
         i32 = dict(dtype=torch.int32, device=dev)
@@ -762,6 +761,7 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
     # products, so that the hand-off block is as good as without them
     tc_low_on = tcp is not None and os.environ.get("GWB_TC_LOW", "1") != "0"
     tc_switch = float(os.environ.get("GWB_TC_SWITCH", "30"))
+    eig32 = os.environ.get("GWB_TC_EIG32", "0") == "1"
     info = {"rounds_tc": 0, "rounds_f32": 0, "rounds_f64": 0, "handoff_rn_ev": None, "m": []}
     v0 = _orthonormalize(phi0.clone())
     if v0.shape[0] < nb:  # degenerate start: pad with seeded noise (``:345-350``)
@@ -837,7 +837,13 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
             m0 = m
             s = S[:m, :m]
         with phase("eigh"):
-            w, u = torch.linalg.eigh(s)
+            if tc_low and eig32:
+                # the tensor-core rounds carry ~1e-6 errors: a float32
+                # eigensolve (6-11 % faster in cuSOLVER) is accurate enough
+                w, u = torch.linalg.eigh(s.float())
+                w, u = w.double(), u.double()
+            else:
+                w, u = torch.linalg.eigh(s)
         eig = w[:nb_a]
         with phase("ritz_gemm"):
             ut = u[:, :nb_a].T

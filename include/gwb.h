@@ -114,6 +114,12 @@ int gwb_ham_apply_strided(gwb_ham* h, const void* c, int64_t c_kstride, void* ou
  * projector count by gradwave_b200.autotune from timed applies. No
  * counterpart in the reference. */
 int gwb_ham_set_tuning(gwb_ham* h, int64_t w_budget_bytes, int32_t nl_target_ctas);
+/* Threads per block of the shared-memory FFT kernels of the 72^3 and 96^3
+ * boxes, per arithmetic precision: 256, 512 or 1024 (0: the built-in 512 for
+ * float32, 1024 for float64). One block of a float64 96^3 plane fills the
+ * shared memory of an SM, so more threads per block means more warps to hide
+ * the latency of its barrier-separated passes. */
+int gwb_ham_set_fft_threads(gwb_ham* h, int32_t threads_fp32, int32_t threads_fp64);
 
 /* Augmentation matrix q (nproj*nproj float64, real symmetric, device) of the
  * overlap S = 1 + sum_pq |beta_p> q_pq <beta_q| (USPP/PAW). Set after the
