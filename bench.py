@@ -852,6 +852,74 @@ def run_oz(args):
     return 0
 
 
+def run_eigh(args):
+    """The subspace eigensolver on random symmetric matrices of the Davidson
+    sizes (``--eigh-sizes``; diagonal -5..80 eV plus 0.05 noise, like the
+    216-atom subspace matrices): ``gwb_sy_lowest`` (lowest 496) and its
+    tridiagonalisation ``gwb_sytrd`` against ``torch.linalg.eigh``
+    (cuSOLVER), ``--warmup`` untimed and ``--steps`` timed calls (CUDA
+    events); with ``--eigh-trace`` the per-phase cycles of the
+    tridiagonalisation (``gwb_sytrd_set_trace``)."""
+    import torch
+    from gradwave_b200 import _lib
+    dev = torch.device("cuda", 0)
+    lib = _lib.load()
+    for m in (int(x) for x in args.eigh_sizes.split(",")):
+        nev = min(m, 496)
+        g = torch.Generator().manual_seed(m)
+        a = torch.randn(m, m, dtype=torch.float64, generator=g)
+        a = (0.5 * (a + a.T) * 0.05 + torch.diag(torch.linspace(-5, 80, m, dtype=torch.float64))).to(dev)
+        A = torch.empty_like(a)
+        w = torch.empty(nev, dtype=torch.float64, device=dev)
+        ut = torch.empty(nev, m, dtype=torch.float64, device=dev)
+        wk = torch.empty(int(lib.gwb_sy_lowest_work_bytes(m, nev)), dtype=torch.uint8, device=dev)
+        d = torch.empty(m, dtype=torch.float64, device=dev)
+        e = torch.empty(m, dtype=torch.float64, device=dev)
+        tau = torch.empty(m, dtype=torch.float64, device=dev)
+        wt = torch.empty(int(lib.gwb_sytrd_work_bytes(m)), dtype=torch.uint8, device=dev)
+        st = torch.zeros(1, dtype=torch.int32, device=dev)
+        s = _lib.stream_ptr(dev)
+
+        def own():
+            A.copy_(a)
+            _lib.call("gwb_sy_lowest", m, nev, A.data_ptr(), m, w.data_ptr(), ut.data_ptr(), m, wk.data_ptr(),
+                      wk.numel(), st.data_ptr(), s)
+
+        def trd():
+            A.copy_(a)
+            _lib.call("gwb_sytrd", m, A.data_ptr(), m, d.data_ptr(), e.data_ptr(), tau.data_ptr(), wt.data_ptr(),
+                      wt.numel(), st.data_ptr(), s)
+
+        def ev(fn):
+            for _ in range(args.warmup):
+                fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(args.steps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / max(args.steps, 1)
+
+        out = {"mode": "eigh", "m": m, "nev": nev, "own_ms": round(ev(own), 3), "sytrd_ms": round(ev(trd), 3),
+               "torch_eigh_ms": round(ev(lambda: torch.linalg.eigh(a)), 3)}
+        own()
+        ref = torch.linalg.eigvalsh(a)[:nev]
+        out["eig_err_rel"] = float((w - ref).abs().max() / ref.abs().max())
+        if args.eigh_trace:
+            tr = torch.zeros(6, dtype=torch.int64, device=dev)
+            _lib.call("gwb_sytrd_set_trace", tr.data_ptr())
+            trd()
+            torch.cuda.synchronize()
+            _lib.call("gwb_sytrd_set_trace", None)
+            names = ["reflector", "row_products", "barrier_1", "w_and_next_column", "barrier_2", "trailing_update"]
+            out["us_per_column"] = {n: round(c / 1.9e3 / (m - 1), 3) for n, c in zip(names, tr.cpu().tolist())}
+        out["status"] = int(st.item())
+        print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_gamma(args):
     """The Gamma real path on a Gamma-only cell: ``--warmup`` untimed and one
     wall-timed ``davidson_gamma`` from the identity start on the lowest
@@ -938,7 +1006,9 @@ def main():
     ap.add_argument("--slices", type=int, default=8, help="--mode oz: int8 slices per float64 operand")
     ap.add_argument("--oz-scheme", default="slices", choices=["slices", "crt"], help="--mode oz: Ozaki scheme form")
     ap.add_argument("--moduli", type=int, default=18, help="--mode oz --oz-scheme crt: residues per operand")
-    ap.add_argument("--mode", default="solve", choices=["solve", "apply", "apply_gamma", "once", "tc", "gamma", "oz"],
+    ap.add_argument("--eigh-sizes", default="993,1488,1984", help="--mode eigh: matrix sizes")
+    ap.add_argument("--eigh-trace", action="store_true", help="--mode eigh: per-phase cycles of the tridiagonalisation")
+    ap.add_argument("--mode", default="solve", choices=["solve", "apply", "apply_gamma", "once", "tc", "gamma", "oz", "eigh"],
                     help="apply: only time Hamiltonian applies; once: a single solve (profiling)")
     ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64"], help="arithmetic of --mode apply")
     ap.add_argument("--solver", default="learned-mixed", choices=["plain", "fp32exp", "mixed", "learned-mixed"],
@@ -952,6 +1022,8 @@ def main():
         return run_tc(args)
     if args.mode == "oz":
         return run_oz(args)
+    if args.mode == "eigh":
+        return run_eigh(args)
     if args.mode == "gamma":
         return run_gamma(args)
     if args.mode == "once":

@@ -104,6 +104,12 @@ _SIGNATURES = {
                     _SZ, _P, _P],
     "gwb_tc_test_withhold": [_I],
     "gwb_ham_set_fft_threads": [_P, _I, _I],
+    "gwb_sytrd_work_bytes": [_I],
+    "gwb_sytrd_set_blocks": [_I],
+    "gwb_sytrd_set_trace": [_P],
+    "gwb_sytrd": [_I, _P, _I64, _P, _P, _P, _P, _SZ, _P, _P],
+    "gwb_sy_lowest_work_bytes": [_I, _I],
+    "gwb_sy_lowest": [_I, _I, _P, _I64, _P, _P, _I64, _P, _SZ, _P, _P],
     "gwb_crt_bits": [_I],
     "gwb_crt_constants": [_I, _P, _P, _P, _P, _P],
     "gwb_crt_split_rows": [_I, _I64, _I64, _P, _I64, _P, _P, _I64, _I64, _I64, _P, _P],
@@ -143,7 +149,8 @@ _RESTYPES = {"gwb_last_error": ctypes.c_char_p, "gwb_version": ctypes.c_char_p,
              "gwb_ham_scratch_bytes": ctypes.c_size_t, "gwb_heev_scratch_doubles": ctypes.c_int64,
              "gwb_precond_learned_work_bytes": ctypes.c_int64, "gwb_zgemm_tc_work_bytes": ctypes.c_int64,
              "gwb_gamma_work_bytes": ctypes.c_size_t, "gwb_oz_work_bytes": ctypes.c_int64,
-             "gwb_crt_bits": ctypes.c_int32, "gwb_crt_work_bytes": ctypes.c_int64}
+             "gwb_crt_bits": ctypes.c_int32, "gwb_crt_work_bytes": ctypes.c_int64,
+             "gwb_sytrd_work_bytes": ctypes.c_size_t, "gwb_sy_lowest_work_bytes": ctypes.c_size_t}
 
 
 def declared_symbols() -> list[str]:

@@ -20,7 +20,7 @@ namespace gwb {
 // time must not share one.
 static thread_local std::unordered_map<int, cublasHandle_t> g_blas;
 
-static int blas_handle(cublasHandle_t* out) {
+int blas_handle(cublasHandle_t* out) {
   int dev = 0;
   GWB_CUDA_TRY(cudaGetDevice(&dev));
   auto it = g_blas.find(dev);

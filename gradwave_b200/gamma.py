@@ -286,6 +286,38 @@ class GammaDavidsonResult:
     info: dict | None = None      # rounds per phase, hand-off residual
 
 
+class _OwnEigh:
+    """The lowest eigenpairs of the subspace matrix by libgwb's own
+    eigensolver (``gwb_sy_lowest``: tridiagonalisation across the GPU,
+    multisection, inverse iteration, back-transform), with its workspace kept
+    between calls. ``lowest(s, n)`` returns (w, ut): n ascending eigenvalues
+    and the eigenvectors as the rows of ut (n x m). A bounded wait that ran
+    out is reported by ``check()`` (one read per solve)."""
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.work = None
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def lowest(self, s: torch.Tensor, n: int):
+        m = int(s.shape[0])
+        a = s.contiguous().clone()  # symmetric: row-major is column-major; overwritten
+        need = int(_lib.load().gwb_sy_lowest_work_bytes(m, n))
+        if self.work is None or self.work.numel() < need:
+            self.work = torch.empty(need, dtype=torch.uint8, device=self.dev)
+        w = torch.empty(n, dtype=torch.float64, device=self.dev)
+        ut = torch.empty(n, m, dtype=torch.float64, device=self.dev)
+        _lib.call("gwb_sy_lowest", m, n, a.data_ptr(), m, w.data_ptr(), ut.data_ptr(), m, self.work.data_ptr(),
+                  self.work.numel(), self.status.data_ptr(), _lib.stream_ptr(self.dev))
+        return w, ut
+
+    def check(self) -> None:
+        v = int(self.status.item())
+        if v != 0:
+            self.status.zero_()
+            raise _lib.GwbError(v, "subspace eigensolver: a bounded grid barrier ran out")
+
+
 def _orthonormalize(v: torch.Tensor, against: torch.Tensor | None = None) -> torch.Tensor:
     """Two projection passes against ``against``, Householder QR of the rows,
     rows with |R_ii| <= 1e-10 dropped (gradwave ``solvers/davidson.py:319-326``)."""
@@ -762,6 +794,11 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
     tc_low_on = tcp is not None and os.environ.get("GWB_TC_LOW", "1") != "0"
     tc_switch = float(os.environ.get("GWB_TC_SWITCH", "30"))
     eig32 = os.environ.get("GWB_TC_EIG32", "0") == "1"
+    # the subspace eigensolves from m = 128 on libgwb's own eigensolver
+    # (GWB_OWN_EIGH=0: cuSOLVER through torch.linalg.eigh). Measured on the
+    # 216-atom cell: 378 ms of eigensolves against cuSOLVER's 376 ms, 23
+    # rounds each.
+    own_eigh = _OwnEigh(dev) if dev.type == "cuda" and os.environ.get("GWB_OWN_EIGH", "1") != "0" else None
     info = {"rounds_tc": 0, "rounds_f32": 0, "rounds_f64": 0, "handoff_rn_ev": None, "m": []}
     v0 = _orthonormalize(phi0.clone())
     if v0.shape[0] < nb:  # degenerate start: pad with seeded noise (``:345-350``)
@@ -806,12 +843,18 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
             x = y
         hx = ham.apply_phi(x, prec=f64)
         g = mm.nt(x, hx)
-        w2, u2 = torch.linalg.eigh(0.5 * (g + g.T))
-        x, hx = mm.nn(u2.T, x), mm.nn(u2.T, hx)
+        if own_eigh is not None and g.shape[0] >= 128:
+            w2, u2t = own_eigh.lowest(0.5 * (g + g.T), g.shape[0])
+        else:
+            w2, u2 = torch.linalg.eigh(0.5 * (g + g.T))
+            u2t = u2.T
+        x, hx = mm.nn(u2t, x), mm.nn(u2t, hx)
         r = hx - w2[:, None] * x
         return x, hx, w2, r, torch.linalg.vector_norm(r, dim=1)
 
     def finish(eig, x, rn, nw_a, it):
+        if own_eigh is not None:
+            own_eigh.check()
         e, xx, r = locked.merge(eig[:nw_a], x[:nw_a], rn[:nw_a])
         return GammaDavidsonResult(e, unembed_real(gb, xx[:, :nphi]), it, r, prof.summary(),
                                    0 if learned is None else learned.n_fallback(), info)
@@ -837,16 +880,19 @@ def davidson_gamma(ham: GammaHamiltonian, x0: torch.Tensor, tol: float = 1e-9, m
             m0 = m
             s = S[:m, :m]
         with phase("eigh"):
-            if tc_low and eig32:
-                # the tensor-core rounds carry ~1e-6 errors: a float32
-                # eigensolve (6-11 % faster in cuSOLVER) is accurate enough
-                w, u = torch.linalg.eigh(s.float())
-                w, u = w.double(), u.double()
+            if own_eigh is not None and m >= 128:
+                eig, ut = own_eigh.lowest(s, nb_a)
             else:
-                w, u = torch.linalg.eigh(s)
-        eig = w[:nb_a]
+                if tc_low and eig32:
+                    # the tensor-core rounds carry ~1e-6 errors: a float32
+                    # eigensolve (6-11 % faster in cuSOLVER) is accurate enough
+                    w, u = torch.linalg.eigh(s.float())
+                    w, u = w.double(), u.double()
+                else:
+                    w, u = torch.linalg.eigh(s)
+                eig = w[:nb_a]
+                ut = u[:, :nb_a].T
         with phase("ritz_gemm"):
-            ut = u[:, :nb_a].T
             if tc_low:
                 x, hx = tcp.ritz(ut.contiguous(), m)
             else:

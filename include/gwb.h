@@ -326,6 +326,40 @@ int gwb_crt_gemm(int32_t n, int64_t M, int64_t N, int64_t K, const void* A, int6
                  int64_t b_row0, const double* b_scale, double alpha, double beta, double* C, int64_t ldc, void* work,
                  size_t work_bytes, int* status, void* stream);
 
+/* Householder tridiagonalisation of a real symmetric m x m matrix across the
+ * whole GPU (one cooperative launch, a block per SM, m <= 4096): the
+ * reduction step of the subspace eigensolve torch.linalg.eigh (gradwave
+ * solvers/davidson.py:66-75,650) for subspaces too large for
+ * gwb_heev_lowest. A (column-major, lda; both triangles) is overwritten with
+ * LAPACK's dsytrd lower-storage output: d = diag(T), e = the subdiagonal,
+ * tau, and reflector j's vector below the subdiagonal of column j
+ * (Q = H_0 ... H_{m-2}, H_j = I - tau_j v_j v_j^T, v_j[j+1] = 1). work:
+ * gwb_sytrd_work_bytes(m). A grid barrier that waits longer than the
+ * gwb_tc_set_wait_limit cycle count ORs GWB_ERR_TIMEOUT into *status. */
+size_t gwb_sytrd_work_bytes(int32_t m);
+/* Blocks of gwb_sytrd's cooperative launch (0: one per SM): fewer blocks make
+ * the grid barrier cheaper and leave less bandwidth for the products. */
+int gwb_sytrd_set_blocks(int32_t blocks);
+/* Phase trace of gwb_sytrd (NULL: off): later launches add the SM cycles of
+ * block 0 to cycles6[0..5] = before the product, the product y = A v, the
+ * barrier after it, the column's w and the next column's update, the
+ * barrier after that, the trailing updates. For tuning. */
+int gwb_sytrd_set_trace(long long* cycles6);
+int gwb_sytrd(int32_t m, double* A, int64_t lda, double* d, double* e, double* tau, void* work, size_t work_bytes,
+              int* status, void* stream);
+/* The nev lowest eigenpairs of a real symmetric m x m matrix (m <= 4096):
+ * gwb_sytrd, then multisection on Sturm counts for the eigenvalues of T,
+ * inverse iteration for its eigenvectors (clusters within 1e-9 |T|
+ * orthogonalised in turn and rotated by a Rayleigh-Ritz of T), Newton-Schulz
+ * orthonormalisation and the back-transform U = Q Z in blocks of 256
+ * reflectors. A (column-major, lda, both triangles) is overwritten. w: nev
+ * ascending; U: m x nev, column-major, ldu. work: gwb_sy_lowest_work_bytes.
+ * Replaces torch.linalg.eigh of gradwave solvers/davidson.py:66-75,650 for
+ * the lowest Ritz pairs. */
+size_t gwb_sy_lowest_work_bytes(int32_t m, int32_t nev);
+int gwb_sy_lowest(int32_t m, int32_t nev, double* A, int64_t lda, double* w, double* U, int64_t ldu, void* work,
+                  size_t work_bytes, int* status, void* stream);
+
 /* r = hx - eig * x and rn = |r| per (k, band); eig (nk, eig_kstride) float64.
  * Replaces gradwave solvers/davidson.py:656-657. */
 int gwb_residual(int32_t nk, int32_t nb, int32_t npw, const void* x, int64_t x_kstride, const void* hx,
