@@ -904,19 +904,97 @@ def run_eigh(args):
 
         out = {"mode": "eigh", "m": m, "nev": nev, "own_ms": round(ev(own), 3), "sytrd_ms": round(ev(trd), 3),
                "torch_eigh_ms": round(ev(lambda: torch.linalg.eigh(a)), 3)}
+        # the cooperative launch alone (no cluster part), for comparison
+        _lib.call("gwb_sytrd_set_cluster", 0)
+        out["sytrd_coop_only_ms"] = round(ev(trd), 3)
+        _lib.call("gwb_sytrd_set_cluster", -1)
         own()
         ref = torch.linalg.eigvalsh(a)[:nev]
         out["eig_err_rel"] = float((w - ref).abs().max() / ref.abs().max())
         if args.eigh_trace:
+            # the trace covers the cooperative launch: run it over all columns
             tr = torch.zeros(6, dtype=torch.int64, device=dev)
+            _lib.call("gwb_sytrd_set_cluster", 0)
             _lib.call("gwb_sytrd_set_trace", tr.data_ptr())
             trd()
             torch.cuda.synchronize()
             _lib.call("gwb_sytrd_set_trace", None)
+            _lib.call("gwb_sytrd_set_cluster", -1)
             names = ["reflector", "row_products", "barrier_1", "w_and_next_column", "barrier_2", "trailing_update"]
             out["us_per_column"] = {n: round(c / 1.9e3 / (m - 1), 3) for n, c in zip(names, tr.cpu().tolist())}
         out["status"] = int(st.item())
         print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_precond(args):
+    """The learned preconditioner at the 216-atom Gamma shape (``--precond-rows``
+    selected bands of 496, 40,399 half-sphere slots, random rows and
+    network): ``gwb_precond_learned_gamma`` on the embedded real rows
+    (tcgen05), and the complex-row ``gwb_precond_learned`` on the same rows as
+    half-sphere rows with each inference kernel (tcgen05, mma.sync), the
+    gather and repacking of the half rows included (the previous Gamma form).
+    CUDA events over ``--steps`` calls after ``--warmup``."""
+    import torch
+    from gradwave_b200 import _lib, learned
+    from gradwave_b200.gamma import _embed_rows, _half_rows
+    dev = torch.device("cuda", 0)
+    lib = _lib.load()
+    nb, nhalf, n = 496, 40399, args.precond_rows
+    nphi = 2 * nhalf - 1
+    npad = nphi + 1
+    g = torch.Generator(device="cpu").manual_seed(3)
+    x = torch.randn(nb, npad, generator=g, dtype=torch.float64).to(dev)
+    r = torch.randn(nb, npad, generator=g, dtype=torch.float64).to(dev)
+    x[:, nphi:] = 0.0
+    r[:, nphi:] = 0.0
+    th = (torch.rand(nhalf, generator=g, dtype=torch.float64) * 60).to(dev)
+    eig = torch.randn(nb, generator=g, dtype=torch.float64).to(dev)
+    sel = torch.randperm(nb, generator=g)[:n].sort().values.to(torch.int32).to(dev)
+    tpa = torch.zeros(nb, dtype=torch.uint8, device=dev)
+    P = torch.from_numpy(learned.init_params(1)).to(dev)
+    P[-65:] = 0.05 * torch.randn(65, generator=g, dtype=torch.float32).to(dev)
+    d = torch.empty(n, npad, dtype=torch.float64, device=dev)
+    wk = torch.empty(int(lib.gwb_precond_learned_gamma_work_bytes(n, nhalf)), dtype=torch.uint8, device=dev)
+    s = _lib.stream_ptr(dev)
+
+    def gamma_rows():
+        _lib.call("gwb_precond_learned_gamma", P.data_ptr(), nb, n, nhalf, npad, x.data_ptr(), npad, r.data_ptr(),
+                  npad, th.data_ptr(), eig.data_ptr(), sel.data_ptr(), tpa.data_ptr(), d.data_ptr(), npad,
+                  wk.data_ptr(), wk.numel(), s)
+
+    idx = torch.arange(n, dtype=torch.int32, device=dev).reshape(1, n)
+    sl = sel.long()
+
+    def half_rows():
+        xs, rs = _half_rows(x[sl], nhalf), _half_rows(r[sl], nhalf)
+        dd = torch.ops.gwb.precond_apply(xs[None], rs[None], th.reshape(1, -1), idx, eig[sl].reshape(1, n), P,
+                                         tpa[sl].reshape(1, n))
+        return _embed_rows(dd[0], npad)
+
+    def ev(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / max(args.steps, 1)
+
+    out = {"mode": "precond", "rows": n, "nhalf": nhalf, "gamma_rows_ms": round(ev(gamma_rows), 3)}
+    ref = half_rows()
+    gamma_rows()
+    torch.cuda.synchronize()
+    out["max_abs_diff_vs_half_rows"] = float((d - ref).abs().max())
+    for name, kern in (("half_rows_tcgen05_ms", 1), ("half_rows_mma_sync_ms", 0)):
+        _lib.call("gwb_precond_set_kernel", kern)
+        out[name] = round(ev(half_rows), 3)
+    _lib.call("gwb_precond_set_kernel", 1)
+    out["plane_waves_per_s_gamma_rows"] = n * nhalf / (out["gamma_rows_ms"] * 1e-3)
+    print(json.dumps(out), flush=True)
     return 0
 
 
@@ -1008,7 +1086,9 @@ def main():
     ap.add_argument("--moduli", type=int, default=18, help="--mode oz --oz-scheme crt: residues per operand")
     ap.add_argument("--eigh-sizes", default="993,1488,1984", help="--mode eigh: matrix sizes")
     ap.add_argument("--eigh-trace", action="store_true", help="--mode eigh: per-phase cycles of the tridiagonalisation")
-    ap.add_argument("--mode", default="solve", choices=["solve", "apply", "apply_gamma", "once", "tc", "gamma", "oz", "eigh"],
+    ap.add_argument("--precond-rows", type=int, default=400, help="--mode precond: selected bands")
+    ap.add_argument("--mode", default="solve", choices=["solve", "apply", "apply_gamma", "once", "tc", "gamma", "oz", "eigh",
+                                                       "precond"],
                     help="apply: only time Hamiltonian applies; once: a single solve (profiling)")
     ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64"], help="arithmetic of --mode apply")
     ap.add_argument("--solver", default="learned-mixed", choices=["plain", "fp32exp", "mixed", "learned-mixed"],
@@ -1022,6 +1102,8 @@ def main():
         return run_tc(args)
     if args.mode == "oz":
         return run_oz(args)
+    if args.mode == "precond":
+        return run_precond(args)
     if args.mode == "eigh":
         return run_eigh(args)
     if args.mode == "gamma":

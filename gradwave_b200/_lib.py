@@ -107,6 +107,10 @@ _SIGNATURES = {
     "gwb_sytrd_work_bytes": [_I],
     "gwb_sytrd_set_blocks": [_I],
     "gwb_sytrd_set_trace": [_P],
+    "gwb_sytrd_set_cluster": [_I],
+    "gwb_precond_set_kernel": [_I],
+    "gwb_precond_learned_gamma_work_bytes": [_I, _I],
+    "gwb_precond_learned_gamma": [_P, _I, _I, _I, _I, _P, _I64, _P, _I64, _P, _P, _P, _P, _P, _I64, _P, _SZ, _P],
     "gwb_sytrd": [_I, _P, _I64, _P, _P, _P, _P, _SZ, _P, _P],
     "gwb_sy_lowest_work_bytes": [_I, _I],
     "gwb_sy_lowest": [_I, _I, _P, _I64, _P, _P, _I64, _P, _SZ, _P, _P],
@@ -147,7 +151,7 @@ _SIGNATURES = {
 _RESTYPES = {"gwb_last_error": ctypes.c_char_p, "gwb_version": ctypes.c_char_p,
              "gwb_launch_count": ctypes.c_ulonglong,
              "gwb_ham_scratch_bytes": ctypes.c_size_t, "gwb_heev_scratch_doubles": ctypes.c_int64,
-             "gwb_precond_learned_work_bytes": ctypes.c_int64, "gwb_zgemm_tc_work_bytes": ctypes.c_int64,
+             "gwb_precond_learned_work_bytes": ctypes.c_int64, "gwb_precond_learned_gamma_work_bytes": ctypes.c_int64, "gwb_zgemm_tc_work_bytes": ctypes.c_int64,
              "gwb_gamma_work_bytes": ctypes.c_size_t, "gwb_oz_work_bytes": ctypes.c_int64,
              "gwb_crt_bits": ctypes.c_int32, "gwb_crt_work_bytes": ctypes.c_int64,
              "gwb_sytrd_work_bytes": ctypes.c_size_t, "gwb_sy_lowest_work_bytes": ctypes.c_size_t}

@@ -21,6 +21,7 @@
 #include <cmath>
 
 #include "common.cuh"
+#include "tcgen05.cuh"
 
 namespace gwb {
 
@@ -562,6 +563,319 @@ __global__ void k_precond_normalize(int npw, int n_add, int chunks, const double
   for (int gi = threadIdx.x; gi < npw; gi += blockDim.x) dr[gi] = scale(dr[gi], inv);
 }
 
+// ---------------------------------------------------------------------------
+// Inference on the tcgen05 tensor cores. A tile is 128 plane waves of one
+// selected row, one per thread. Layers 1-3 are M = 128, N = 64 BF16 MMAs
+// (kind::f16, FP32 accumulator in 64 TMEM columns): A = the tile's inputs
+// (K = 16: the four features, a constant 1, zeros; K = 80: the 64 SiLU
+// outputs of the layer before, a constant 1, zeros), B = the layer's weights
+// with its bias as the column that meets the constant 1 (the forward pass
+// rounds biases to BF16, so the product by 1 adds them exactly). Between the
+// MMAs each thread reads its row of the accumulator (tcgen05.ld), applies
+// SiLU and writes the BF16 row of the next A; layer 4 (64 -> 1) is a dot
+// product on the CUDA cores. Operands are K-major without swizzle: 8-row x
+// 16-byte core matrices, consecutive along K (leading byte offset 128), row
+// groups kw * 16 bytes apart (stride byte offset).
+//
+// Rows come in two forms: complex rows (GAMMA = false, as
+// k_precond_learned_tc), or the Gamma path's embedded real rows (GAMMA =
+// true): half-sphere coefficient c_G = phi[2G-1] + i phi[2G] (c_0 = phi[0]),
+// which are the sqrt(w)-scaled half rows, so sums over them are full-sphere
+// sums; the output is written back in the same embedding.
+constexpr int PU_THREADS = 128;
+constexpr int PU_TILE = 128;
+constexpr int PU_K1 = 16, PU_K = 80;
+constexpr int PU_A = PU_TILE * PU_K * 2;   // 20480 B
+constexpr int PU_A1 = PU_TILE * PU_K1 * 2;  // 4096 B
+constexpr int PU_B1 = HID * PU_K1 * 2;      // 2048 B
+constexpr int PU_B = HID * PU_K * 2;        // 10240 B
+constexpr int PU_SMEM = PU_A + PU_A1 + PU_B1 + 2 * PU_B + 16;
+constexpr int PU_TMEM_COLS = 64;
+// kind::f16 instruction descriptor: F32 accumulator, BF16 A and B, both
+// K-major, N = 64, M = 128
+constexpr uint32_t PU_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(HID >> 3) << 17) |
+                              ((uint32_t)(PU_TILE >> 4) << 24);
+
+__host__ __device__ constexpr int pu_off(int row, int k, int kw) {
+  return (row >> 3) * (kw * 16) + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2;
+}
+
+// tcgen05 shared-memory descriptor, no swizzle (layout type 0)
+__device__ __forceinline__ uint64_t pu_desc(uint32_t addr, int kw) {
+  const uint32_t lbo = 128, sbo = (uint32_t)kw * 16;
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) |
+         (1ull << 46);
+}
+
+__device__ __forceinline__ void pu_mma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %3, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %4, p;\n\t}" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(accumulate), "r"(PU_IDESC)
+      : "memory");
+}
+
+struct PuArgs {
+  const float* P;
+  int nb, n_add, npw;  // npw: plane waves per row (Gamma: half-sphere slots)
+  const void* r;       // complex: (nk, nb, npw) with k stride rk; Gamma: nb embedded rows, row stride r_row
+  int64_t rk, r_row;
+  const double* t;     // (nk, npw) kinetic diagonal
+  const double* eig;   // (nk, nb)
+  const int* sel;      // (nk, n_add)
+  const unsigned char* tpa_only;
+  const double* stats;  // per row: t_b, r_rms
+  void* d;              // complex: (nk, n_add, npw) with k stride dk; Gamma: n_add embedded rows, row stride d_row
+  int64_t dk, d_row;
+  double* partial;      // per (row, tile): sum of |d|^2
+  int tiles, total;     // tiles per row, rows * tiles
+  int* status;
+  long long wait_cycles;
+};
+
+// This warp's 32 rows of the 64 accumulator columns -> SiLU -> (unless
+// keep) the BF16 row of the next A.
+__device__ __forceinline__ void pu_hidden(uint32_t taddr, uint8_t* sA, int row, float* h, bool keep) {
+  uint32_t r[4][16];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) tmem_ld16(taddr + 16 * q, r[q]);
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int i = 0; i < 16; ++i) h[16 * q + i] = silu_fast(__uint_as_float(r[q][i]));
+  if (!keep) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      uint4 v;
+      v.x = pack_bf16(h[8 * c + 0], h[8 * c + 1]);
+      v.y = pack_bf16(h[8 * c + 2], h[8 * c + 3]);
+      v.z = pack_bf16(h[8 * c + 4], h[8 * c + 5]);
+      v.w = pack_bf16(h[8 * c + 6], h[8 * c + 7]);
+      *reinterpret_cast<uint4*>(sA + pu_off(row, 8 * c, PU_K)) = v;
+    }
+  }
+}
+
+template <bool GAMMA>
+__global__ void __launch_bounds__(PU_THREADS) k_precond_learned_umma(PuArgs a) {
+  extern __shared__ uint8_t pu_raw[];
+  __shared__ float sW4[HID];
+  __shared__ float sB4;
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ double red[PU_THREADS / 32];
+  __shared__ int abort_f;
+  uint8_t* sA = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(pu_raw) + 15) & ~(uintptr_t)15);
+  uint8_t* sA1 = sA + PU_A;
+  uint8_t* sB1 = sA1 + PU_A1;
+  uint8_t* sB2 = sB1 + PU_B1;
+  uint8_t* sB3 = sB2 + PU_B;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const float* P = a.P;
+  for (int i = tid; i < HID * PU_K1; i += PU_THREADS) {
+    const int n = i / PU_K1, k = i % PU_K1;
+    const float v = k < NIN ? P[O_W1 + n * NIN + k] : (k == NIN ? P[O_B1 + n] : 0.f);
+    *reinterpret_cast<__nv_bfloat16*>(sB1 + pu_off(n, k, PU_K1)) = __float2bfloat16_rn(v);
+  }
+  for (int i = tid; i < HID * PU_K; i += PU_THREADS) {
+    const int n = i / PU_K, k = i % PU_K;
+    const float v2 = k < HID ? P[O_W2 + n * HID + k] : (k == HID ? P[O_B2 + n] : 0.f);
+    const float v3 = k < HID ? P[O_W3 + n * HID + k] : (k == HID ? P[O_B3 + n] : 0.f);
+    *reinterpret_cast<__nv_bfloat16*>(sB2 + pu_off(n, k, PU_K)) = __float2bfloat16_rn(v2);
+    *reinterpret_cast<__nv_bfloat16*>(sB3 + pu_off(n, k, PU_K)) = __float2bfloat16_rn(v3);
+  }
+  for (int i = tid; i < HID; i += PU_THREADS) sW4[i] = bf(P[O_W4 + i]);
+  if (tid == 0) sB4 = bf(P[O_B4]);
+  // the constant columns of this thread's A rows: k = 64 (A) and k = 4 (A1) hold 1
+  {
+    const uint32_t one = 0x3F80u;  // BF16 1.0
+    *reinterpret_cast<uint4*>(sA + pu_off(tid, 64, PU_K)) = make_uint4(one, 0u, 0u, 0u);
+    *reinterpret_cast<uint4*>(sA + pu_off(tid, 72, PU_K)) = make_uint4(0u, 0u, 0u, 0u);
+    *reinterpret_cast<uint4*>(sA1 + pu_off(tid, 8, PU_K1)) = make_uint4(0u, 0u, 0u, 0u);
+  }
+  if (tid == 0) {
+    mbar_init(smem_u32(&bar), 1);
+    abort_f = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"((uint32_t)PU_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16);  // this warp's 32 lanes
+  const uint32_t bar_a = smem_u32(&bar);
+  const uint64_t dA1 = pu_desc(smem_u32(sA1), PU_K1), dB1 = pu_desc(smem_u32(sB1), PU_K1);
+  const uint32_t aA = smem_u32(sA), aB2 = smem_u32(sB2), aB3 = smem_u32(sB3);
+  uint32_t parity = 0;
+
+  // one layer's MMA (issued by thread 0 after every thread's A row is in
+  // place), then every thread waits for the accumulator
+  auto layer = [&](int which) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (which == 1) {
+        pu_mma(tmem, dA1, dB1, 0u);
+      } else {
+        const uint32_t aB = which == 2 ? aB2 : aB3;
+#pragma unroll
+        for (int s = 0; s < PU_K / 16; ++s)
+          pu_mma(tmem, pu_desc(aA + 256 * s, PU_K), pu_desc(aB + 256 * s, PU_K), s > 0 ? 1u : 0u);
+      }
+      mma_commit(bar_a);
+    }
+    if (!mbar_wait(bar_a, parity, a.wait_cycles)) {
+      atomicOr(a.status, GWB_ERR_TIMEOUT);
+      abort_f = 1;
+    }
+    parity ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  };
+
+  for (int w = blockIdx.x; w < a.total; w += gridDim.x) {
+    const int row = w / a.tiles, tile = w - row * a.tiles;
+    const int k = row / a.n_add, s = row - k * a.n_add;
+    const int b = a.sel[(int64_t)k * a.n_add + s];
+    const bool plain = a.tpa_only && a.tpa_only[(int64_t)k * a.nb + b];
+    const double tbv = a.stats[2 * row], rrms = a.stats[2 * row + 1], eps = a.eig[(int64_t)k * a.nb + b];
+    const int gi = tile * PU_TILE + tid;
+    const bool valid = gi < a.npw;
+    cplx<double> rv = mk<double>(0.0, 0.0);
+    double tg = 0.0;
+    if (valid) {
+      tg = a.t[(int64_t)k * a.npw + gi];
+      if (GAMMA) {
+        const double* rr = static_cast<const double*>(a.r) + (int64_t)b * a.r_row;
+        rv = gi == 0 ? mk<double>(rr[0], 0.0) : mk<double>(rr[2 * gi - 1], rr[2 * gi]);
+      } else {
+        rv = static_cast<const cplx<double>*>(a.r)[k * a.rk + (int64_t)b * a.npw + gi];
+      }
+    }
+    double c = tpa_coeff(tg, tbv);
+    if (!plain) {
+      float u[NIN] = {0.f, 0.f, 0.f, 0.f};
+      if (valid) features(tg, tbv, eps, sqrt(norm2(rv)), rrms, u);
+      *reinterpret_cast<uint4*>(sA1 + pu_off(tid, 0, PU_K1)) =
+          make_uint4(pack_bf16(u[0], u[1]), pack_bf16(u[2], u[3]), pack_bf16(1.f, 0.f), 0u);
+      float h[HID];
+      layer(1);
+      pu_hidden(taddr, sA, tid, h, false);
+      layer(2);
+      pu_hidden(taddr, sA, tid, h, false);
+      layer(3);
+      pu_hidden(taddr, sA, tid, h, true);
+      float o = sB4;
+#pragma unroll
+      for (int i = 0; i < HID; ++i) o = fmaf(bf(h[i]), sW4[i], o);
+      if (rv.x != 0.0 || rv.y != 0.0) c *= (double)__expf(fminf(fmaxf(o, -3.f), 3.f));
+    }
+    double nn = 0.0;
+    if (valid) {
+      const cplx<double> v = scale(rv, c);
+      nn = norm2(v);
+      if (GAMMA) {
+        double* dr = static_cast<double*>(a.d) + (int64_t)s * a.d_row;
+        if (gi == 0) {
+          dr[0] = v.x;
+        } else {
+          dr[2 * gi - 1] = v.x;
+          dr[2 * gi] = v.y;
+        }
+      } else {
+        static_cast<cplx<double>*>(a.d)[k * a.dk + (int64_t)s * a.npw + gi] = v;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) nn += __shfl_xor_sync(0xffffffffu, nn, o);
+    __syncthreads();  // red from the previous tile is read
+    if (lane == 0) red[warp] = nn;
+    __syncthreads();
+    if (tid == 0) a.partial[(int64_t)row * a.tiles + tile] = red[0] + red[1] + red[2] + red[3];
+    if (abort_f) break;
+  }
+  // after a wait that ran out, the MMA it waited for may still run: give it
+  // one more bounded wait before the accumulator's columns are freed
+  if (abort_f && tid == 0) mbar_wait(bar_a, parity ^ 1u, a.wait_cycles);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)PU_TMEM_COLS)
+                 : "memory");
+  }
+}
+
+// Per selected row of the Gamma path's embedded real rows: t_b = sum_G t_G
+// |c_G|^2 and the rms of the residual's half-sphere coefficients (as
+// k_precond_row_stats on the half rows).
+__global__ void __launch_bounds__(256) k_precond_row_stats_gamma(int nhalf, int n_add, const double* __restrict__ x,
+                                                                 int64_t x_row, const double* __restrict__ r,
+                                                                 int64_t r_row, const double* __restrict__ t_,
+                                                                 const int* __restrict__ sel,
+                                                                 double* __restrict__ stats) {
+  __shared__ double red[2][8];
+  const int s = blockIdx.x;
+  const int b = sel[s];
+  const double* xr = x + (int64_t)b * x_row;
+  const double* rr = r + (int64_t)b * r_row;
+  double tb = 0.0, r2 = 0.0;
+  for (int g = threadIdx.x; g < nhalf; g += blockDim.x) {
+    double xa, xb = 0.0, ra, rb = 0.0;
+    if (g == 0) {
+      xa = xr[0];
+      ra = rr[0];
+    } else {
+      xa = xr[2 * g - 1];
+      xb = xr[2 * g];
+      ra = rr[2 * g - 1];
+      rb = rr[2 * g];
+    }
+    tb += t_[g] * (xa * xa + xb * xb);
+    r2 += ra * ra + rb * rb;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    tb += __shfl_xor_sync(0xffffffffu, tb, o);
+    r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = tb;
+    red[1][threadIdx.x >> 5] = r2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double p = 0.0, q = 0.0;
+    for (int w = 0; w < 8; ++w) {
+      p += red[0][w];
+      q += red[1][w];
+    }
+    stats[2 * s] = p;
+    stats[2 * s + 1] = sqrt(q / nhalf);
+  }
+}
+
+// Embedded rows: d <- d / |d| over the 2 nhalf - 1 coordinates, the norm
+// summed from the tile partials in order; pad columns set to zero.
+__global__ void k_precond_normalize_gamma(int nhalf, int npad, int tiles, const double* __restrict__ partial,
+                                          double* __restrict__ d, int64_t d_row) {
+  const int s = blockIdx.x;
+  double a = 0.0;
+  for (int c = 0; c < tiles; ++c) a += partial[(int64_t)s * tiles + c];
+  const double inv = a > 0.0 ? 1.0 / sqrt(a) : 1.0;
+  double* dr = d + (int64_t)s * d_row;
+  const int nphi = 2 * nhalf - 1;
+  for (int i = threadIdx.x; i < npad; i += blockDim.x) dr[i] = i < nphi ? dr[i] * inv : 0.0;
+}
+
 // Stall rule of the learned preconditioner: a band whose residual has not
 // dropped below ratio * (its best so far) for `patience` consecutive rounds
 // reverts to TPA for the rest of the solve (tpa_only is sticky).
@@ -578,6 +892,45 @@ __global__ void k_stall_update(const double* __restrict__ rn, double* __restrict
     if (count[i] >= patience) tpa_only[i] = 1;
     rn_best[i] = fmin(rn_best[i], v);
   }
+}
+
+// The tcgen05 inference kernel over all (row, tile) items: a persistent grid
+// of up to four CTAs per SM (47 KB of shared memory and 64 TMEM columns each).
+template <bool GAMMA>
+int precond_umma(const float* params, int nb, int n_add, int npw, const void* r, int64_t rk, int64_t r_row,
+                 const double* t, const double* eig, const int* sel, const uint8_t* tpa_only, const double* stats,
+                 void* d, int64_t dk, int64_t d_row, double* partial, int rows, int* status, cudaStream_t st) {
+  int dev = 0, sms = 0;
+  GWB_CUDA_TRY(cudaGetDevice(&dev));
+  GWB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  PuArgs a;
+  a.P = params;
+  a.nb = nb;
+  a.n_add = n_add;
+  a.npw = npw;
+  a.r = r;
+  a.rk = rk;
+  a.r_row = r_row;
+  a.t = t;
+  a.eig = eig;
+  a.sel = sel;
+  a.tpa_only = tpa_only;
+  a.stats = stats;
+  a.d = d;
+  a.dk = dk;
+  a.d_row = d_row;
+  a.partial = partial;
+  a.tiles = (npw + PU_TILE - 1) / PU_TILE;
+  a.total = rows * a.tiles;
+  a.status = status;
+  a.wait_cycles = tc_wait_cycles();
+  GWB_CUDA_TRY(cudaFuncSetAttribute(k_precond_learned_umma<GAMMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    PU_SMEM));
+  GWB_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), st));
+  const int grid = std::min(a.total, 4 * sms);
+  k_precond_learned_umma<GAMMA><<<grid, PU_THREADS, PU_SMEM, st>>>(a);
+  GWB_LAUNCH_CHECK();
+  return GWB_OK;
 }
 
 }  // namespace gwb
@@ -651,10 +1004,19 @@ int gwb_precond_features(int32_t nk, int32_t nb, int32_t n_add, int32_t npw, con
   return GWB_OK;
 }
 
+// inference kernel of gwb_precond_learned: 1 tcgen05 (default), 0 mma.sync
+static int g_precond_kernel = 1;
+
+int gwb_precond_set_kernel(int32_t which) {
+  GWB_REQUIRE(which == 0 || which == 1, "kernel must be 0 (mma.sync) or 1 (tcgen05)");
+  g_precond_kernel = which;
+  return GWB_OK;
+}
+
 int64_t gwb_precond_learned_work_bytes(int32_t nk, int32_t n_add, int32_t npw) {
   if (nk <= 0 || n_add <= 0 || npw <= 0) return 0;
-  const int64_t rows = (int64_t)nk * n_add, chunks = (npw + PL_CHUNK - 1) / PL_CHUNK;
-  return rows * (2 + chunks) * (int64_t)sizeof(double);
+  const int64_t rows = (int64_t)nk * n_add, tiles = (npw + PU_TILE - 1) / PU_TILE;
+  return (rows * (2 + tiles) + 1) * (int64_t)sizeof(double);
 }
 
 int gwb_precond_learned(const float* params, int32_t nk, int32_t nb, int32_t n_add, int32_t npw, const void* x,
@@ -665,16 +1027,56 @@ int gwb_precond_learned(const float* params, int32_t nk, int32_t nb, int32_t n_a
   GWB_REQUIRE(x && r && t && eig && sel && d && work, "null pointer");
   GWB_REQUIRE((int64_t)work_bytes >= gwb_precond_learned_work_bytes(nk, n_add, npw),
               "work smaller than gwb_precond_learned_work_bytes");
-  const int rows = nk * n_add, chunks = (npw + PL_CHUNK - 1) / PL_CHUNK;
+  const int rows = nk * n_add;
   double* stats = static_cast<double*>(work);
   double* partial = stats + 2 * (int64_t)rows;
   const cudaStream_t st = (cudaStream_t)stream;
   k_precond_row_stats<<<rows, 256, 0, st>>>(npw, nb, n_add, (const cplx<double>*)x, x_kstride,
                                             (const cplx<double>*)r, r_kstride, t, sel, stats);
-  k_precond_learned_tc<<<dim3(chunks, rows), PL_THREADS, 0, st>>>(params, npw, nb, n_add, (const cplx<double>*)r,
-                                                                  r_kstride, t, eig, sel, tpa_only, stats,
-                                                                  (cplx<double>*)d, d_kstride, partial);
-  k_precond_normalize<<<rows, 256, 0, st>>>(npw, n_add, chunks, partial, (cplx<double>*)d, d_kstride);
+  if (g_precond_kernel == 0) {
+    const int chunks = (npw + PL_CHUNK - 1) / PL_CHUNK;
+    k_precond_learned_tc<<<dim3(chunks, rows), PL_THREADS, 0, st>>>(params, npw, nb, n_add, (const cplx<double>*)r,
+                                                                    r_kstride, t, eig, sel, tpa_only, stats,
+                                                                    (cplx<double>*)d, d_kstride, partial);
+    k_precond_normalize<<<rows, 256, 0, st>>>(npw, n_add, chunks, partial, (cplx<double>*)d, d_kstride);
+  } else {
+    const int64_t tiles = (npw + PU_TILE - 1) / PU_TILE;
+    int* status = reinterpret_cast<int*>(partial + (int64_t)rows * tiles);
+    int rc = precond_umma<false>(params, nb, n_add, npw, r, r_kstride, 0, t, eig, sel, tpa_only, stats, d, d_kstride,
+                                 0, partial, rows, status, st);
+    if (rc) return rc;
+    k_precond_normalize<<<rows, 256, 0, st>>>(npw, n_add, (int)tiles, partial, (cplx<double>*)d, d_kstride);
+  }
+  GWB_LAUNCH_CHECK();
+  count_launches(3);
+  return GWB_OK;
+}
+
+int64_t gwb_precond_learned_gamma_work_bytes(int32_t n_add, int32_t nhalf) {
+  if (n_add <= 0 || nhalf <= 0) return 0;
+  return ((int64_t)n_add * (2 + (nhalf + PU_TILE - 1) / PU_TILE) + 1) * (int64_t)sizeof(double);
+}
+
+int gwb_precond_learned_gamma(const float* params, int32_t nb, int32_t n_add, int32_t nhalf, int32_t npad,
+                              const double* x, int64_t x_row, const double* r, int64_t r_row, const double* t_half,
+                              const double* eig, const int32_t* sel, const uint8_t* tpa_only, double* d,
+                              int64_t d_row, void* work, size_t work_bytes, void* stream) {
+  GWB_REQUIRE(params && nb > 0 && n_add > 0 && n_add <= nb && nhalf > 0, "bad sizes");
+  GWB_REQUIRE(npad >= 2 * nhalf - 1 && x_row >= 2 * nhalf - 1 && r_row >= 2 * nhalf - 1 && d_row >= npad,
+              "rows shorter than the embedding");
+  GWB_REQUIRE(x && r && t_half && eig && sel && d && work, "null pointer");
+  GWB_REQUIRE((int64_t)work_bytes >= gwb_precond_learned_gamma_work_bytes(n_add, nhalf),
+              "work smaller than gwb_precond_learned_gamma_work_bytes");
+  double* stats = static_cast<double*>(work);
+  double* partial = stats + 2 * (int64_t)n_add;
+  const int tiles = (nhalf + PU_TILE - 1) / PU_TILE;
+  int* status = reinterpret_cast<int*>(partial + (int64_t)n_add * tiles);
+  const cudaStream_t st = (cudaStream_t)stream;
+  k_precond_row_stats_gamma<<<n_add, 256, 0, st>>>(nhalf, n_add, x, x_row, r, r_row, t_half, sel, stats);
+  int rc = precond_umma<true>(params, nb, n_add, nhalf, r, 0, r_row, t_half, eig, sel, tpa_only, stats, d, 0, d_row,
+                              partial, n_add, status, st);
+  if (rc) return rc;
+  k_precond_normalize_gamma<<<n_add, 256, 0, st>>>(nhalf, npad, tiles, partial, d, d_row);
   GWB_LAUNCH_CHECK();
   count_launches(3);
   return GWB_OK;

@@ -29,11 +29,13 @@
 // block (the last arrival flips bit 31 of the counter) and a spin bounded by
 // gwb_tc_set_wait_limit's cycle count; a spin that runs out sets
 // GWB_ERR_TIMEOUT and every block leaves at its next barrier.
+#include <cooperative_groups.h>
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "common.cuh"
 #include "sturm.cuh"
@@ -50,6 +52,7 @@ constexpr int TD_MMAX = 4096;
 
 struct TdArgs {
   int m;
+  int kend;  // panels start below kend (the cluster kernel reduces the rest)
   double* A;  // column-major, lda
   int64_t lda;
   double *d, *e, *tau;
@@ -138,7 +141,7 @@ __global__ void __launch_bounds__(TD_THREADS, 1) k_sytrd_coop(TdArgs a) {
   }
   long long td_t = clock64();
 
-  for (int k0 = 0; k0 < m - 1; k0 += TD_NB) {
+  for (int k0 = 0; k0 < min(m - 1, a.kend); k0 += TD_NB) {
     const int nbk = min(TD_NB, m - 1 - k0);
 #pragma unroll
     for (int i = 0; i < TD_NB; ++i) vreg[i] = wreg[i] = 0.0;
@@ -391,9 +394,198 @@ __global__ void __launch_bounds__(TD_THREADS, 1) k_sytrd_coop(TdArgs a) {
     }
     TD_MARK(5);
   }
-  // d[m-1]: the last diagonal element after the final panel's update
-  if (gt == 0) a.d[m - 1] = A[(m - 1) + (int64_t)(m - 1) * lda];
+  // d[m-1]: the last diagonal element after the final panel's update (when
+  // the cluster kernel does not take over the trailing part)
+  if (gt == 0 && a.kend >= m - 1) a.d[m - 1] = A[(m - 1) + (int64_t)(m - 1) * lda];
 }
+
+// ---------------------------------------------------------------------------
+// The trailing part inside one thread-block cluster. Once the trailing
+// matrix (n = m - t0 rows, fully updated, both triangles) fits in the
+// cluster's distributed shared memory, the rest of the reduction runs there:
+// CTA c of the cluster keeps rows c, c + CS, c + 2 CS, ... (full rows), and a
+// column costs two cluster barriers and one pass over the local rows instead
+// of two grid barriers and several L2 round trips.
+//
+// Unblocked form (LAPACK dsytd2: p = tau A v, w = p - (tau/2)(p.v) v,
+// A <- A - v w^T - w v^T), with the rank-2 update of column j deferred into
+// the pass that forms the product of column j + 1:
+//   entry of column j: every CTA holds column j, fully updated, in abuf (its
+//     rows were broadcast by their owners) and forms the reflector from it
+//     with the same arithmetic, so all CTAs hold identical v_j and tau_j;
+//   pass F(j): own rows i > j, columns k > j: A_ik -= v_i w_k + w_i v_k with
+//     reflector j - 1, and y_i = sum_k A_ik v_j[k] on the updated values;
+//     p_i = tau_j y_i and the CTA's part of p.v go to every CTA;
+//   barrier; step O(j): every CTA forms w_j from the gathered p; each owner
+//     brings its rows' element of column j + 1 up to date with reflector j
+//     and sends it to every CTA's abuf; barrier.
+// Sums that every CTA needs (|x|^2, p.v) are formed in the same fixed order
+// in every CTA. The cluster barriers are hardware barriers that every thread
+// of every CTA reaches the same number of times.
+constexpr int TK_THREADS = 1024;
+constexpr int TK_WARPS = TK_THREADS / 32;
+constexpr int TK_SEG = 128;    // columns per warp item of the pass (4 per lane)
+constexpr int TK_NSEG = 8;     // segments per row at most (n <= 1024)
+
+struct TkArgs {
+  int m, t0;  // the trailing part A[t0:, t0:], n = m - t0 rows
+  double* A;
+  int64_t lda;
+  double *d, *e, *tau;
+};
+
+__host__ __device__ inline size_t tk_smem_doubles(int n, int cs) {
+  const int nl = (n + cs - 1) / cs;
+  return (size_t)nl * n + 6 * (size_t)n + (size_t)nl * TK_NSEG;
+}
+
+// Sum over the block, formed in one fixed order (every thread gets it).
+__device__ __forceinline__ double tk_block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.0;
+#pragma unroll 8
+  for (int w = 0; w < TK_WARPS; ++w) s += red[w];
+  return s;
+}
+
+template <int CS>
+__global__ void __launch_bounds__(TK_THREADS, 1) k_sytrd_cluster(TkArgs a) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ __align__(16) double tk_smem[];
+  __shared__ double part[CS];
+  __shared__ double red[TK_WARPS];
+  const int c = (int)cl.block_rank();
+  const int n = a.m - a.t0, t0 = a.t0;
+  const int nl = (n + CS - 1) / CS;
+  const int64_t lda = a.lda;
+  double* A = a.A + t0 + (int64_t)t0 * lda;  // the trailing block's origin
+  double* Al = tk_smem;                       // local row li = trailing row c + li CS, n columns
+  double* abuf = Al + (size_t)nl * n;         // [2][n]: column j, fully updated
+  double* vbuf = abuf + 2 * (size_t)n;        // [2][n]: v_j
+  double* wbuf = vbuf + 2 * (size_t)n;        // w_j
+  double* pbuf = wbuf + n;                    // p_j, gathered
+  double* ypart = pbuf + n;                   // [nl][TK_NSEG] row partial products
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+  for (int t = tid; t < nl * n; t += TK_THREADS) {
+    const int li = t / n, k = t - li * n, i = c + li * CS;
+    Al[t] = i < n ? A[k + (int64_t)i * lda] : 0.0;  // column i = row i
+  }
+  for (int k = tid; k < n; k += TK_THREADS) abuf[k] = A[k];
+  cl.sync();  // every CTA of the cluster runs: shared windows are valid
+
+  for (int j = 0; j + 1 < n; ++j) {
+    const double* aj = abuf + (size_t)(j & 1) * n;
+    double* vj = vbuf + (size_t)(j & 1) * n;
+    const double* vq = vbuf + (size_t)((j + 1) & 1) * n;  // v_{j-1}
+    // ---- reflector j from column j (identical in every CTA) ----
+    double s = 0.0;
+    for (int k = j + 2 + tid; k < n; k += TK_THREADS) s += aj[k] * aj[k];
+    s = tk_block_sum(s, red);
+    const double alpha = aj[j + 1];
+    double tau = 0.0, beta = alpha, scl = 0.0;
+    if (s > 0.0) {
+      beta = -copysign(sqrt(alpha * alpha + s), alpha);
+      tau = (beta - alpha) / beta;
+      scl = 1.0 / (alpha - beta);
+    }
+    for (int k = j + 1 + tid; k < n; k += TK_THREADS) vj[k] = k == j + 1 ? 1.0 : aj[k] * scl;
+    if (c == 0) {
+      for (int k = j + 2 + tid; k < n; k += TK_THREADS) A[k + (int64_t)j * lda] = aj[k] * scl;
+      if (tid == 0) {
+        a.d[t0 + j] = aj[j];
+        a.e[t0 + j] = beta;
+        a.tau[t0 + j] = tau;
+        A[j + (int64_t)j * lda] = aj[j];
+        A[j + 1 + (int64_t)j * lda] = beta;
+      }
+    }
+    __syncthreads();
+    // ---- pass F(j): update with reflector j - 1, product with v_j ----
+    const int kb = j + 1, ncol = n - kb;
+    const int nseg = (ncol + TK_SEG - 1) / TK_SEG;
+    const int wps = TK_WARPS / nseg;  // warps per segment
+    const int li0 = kb > c ? (kb - c + CS - 1) / CS : 0;
+    if (warp < nseg * wps) {
+      const int sg = warp / wps, wr = warp - sg * wps;
+      const int klo = kb + sg * TK_SEG, khi = min(n, klo + TK_SEG);
+      double vk[4], wk[4], qk[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int k = klo + lane + 32 * u;
+        const bool in = k < khi;
+        vk[u] = in ? vj[k] : 0.0;
+        wk[u] = (in && j > 0) ? wbuf[k] : 0.0;
+        qk[u] = (in && j > 0) ? vq[k] : 0.0;
+      }
+      for (int li = li0 + wr; li < nl; li += wps) {
+        const int i = c + li * CS;
+        if (i >= n) break;
+        double* row = Al + (size_t)li * n;
+        const double vi = j > 0 ? vq[i] : 0.0, wi = j > 0 ? wbuf[i] : 0.0;
+        double y = 0.0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int k = klo + lane + 32 * u;
+          if (k < khi) {
+            double x = row[k];
+            if (j > 0) {
+              x -= vi * wk[u] + wi * qk[u];
+              row[k] = x;
+            }
+            y += x * vk[u];
+          }
+        }
+        for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+        if (lane == 0) ypart[(size_t)li * TK_NSEG + sg] = y;
+      }
+    }
+    __syncthreads();
+    // p_i = tau y_i for own rows into the local gather; the CTA's part of p.v
+    double pv = 0.0;
+    for (int li = li0 + tid; li < nl; li += TK_THREADS) {
+      const int i = c + li * CS;
+      if (i < n) {
+        double y = 0.0;
+        for (int sg = 0; sg < nseg; ++sg) y += ypart[(size_t)li * TK_NSEG + sg];
+        const double p = tau * y;
+        pbuf[i] = p;
+        pv += p * vj[i];
+      }
+    }
+    pv = tk_block_sum(pv, red);
+    const int nown = nl - li0;
+    for (int t = tid; t < nown * CS; t += TK_THREADS) {
+      const int li = li0 + t / CS, r = t % CS, i = c + li * CS;
+      if (i < n && r != c) *cl.map_shared_rank(pbuf + i, r) = pbuf[i];
+    }
+    if (tid < CS) *cl.map_shared_rank(part + c, tid) = pv;
+    cl.sync();
+    // ---- step O(j): w_j, and the own rows of column j + 1 to every CTA ----
+    double K = 0.0;
+    for (int r = 0; r < CS; ++r) K += part[r];
+    K *= 0.5 * tau;
+    for (int k = kb + tid; k < n; k += TK_THREADS) wbuf[k] = pbuf[k] - K * vj[k];
+    __syncthreads();
+    double* an = abuf + (size_t)((j + 1) & 1) * n;
+    const double wn = wbuf[kb], vn = vj[kb];
+    for (int t = tid; t < nown * CS; t += TK_THREADS) {
+      const int li = li0 + t / CS, r = t % CS, i = c + li * CS;
+      if (i < n) *cl.map_shared_rank(an + i, r) = Al[(size_t)li * n + kb] - vj[i] * wn - wbuf[i] * vn;
+    }
+    cl.sync();
+  }
+  if (c == 0 && tid == 0) {
+    const double dl = abuf[(size_t)((n - 1) & 1) * n + (n - 1)];
+    a.d[t0 + n - 1] = dl;
+    A[(n - 1) + (int64_t)(n - 1) * lda] = dl;
+  }
+}
+
 
 // ---------------------------------------------------------------------------
 // The lowest nev eigenpairs of the tridiagonal (d, e), then of A.
@@ -783,6 +975,80 @@ using namespace gwb;
 
 static int g_sytrd_blocks = 0;
 static long long* g_sytrd_trace = nullptr;
+static int g_sytrd_cluster = -1;  // cluster size of the trailing part: -1 largest that fits, 0 none
+
+extern "C" int gwb_sytrd_set_cluster(int32_t size) {
+  GWB_REQUIRE(size == -1 || size == 0 || size == 8 || size == 16, "cluster size must be -1, 0, 8 or 16");
+  g_sytrd_cluster = size;
+  return GWB_OK;
+}
+
+namespace {
+// The cluster kernel's size on this device: the cluster size and the largest
+// trailing part that fits its distributed shared memory (0, 0: none).
+struct TkChoice {
+  int cs, nmax;
+};
+
+template <int CS>
+int tk_try(int dev, TkChoice* out) {
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, k_sytrd_cluster<CS>) != cudaSuccess) return 0;
+  int nmax = 0;
+  for (int n = TK_NSEG * TK_SEG; n >= 2; --n)
+    if (tk_smem_doubles(n, CS) * 8 + fa.sharedSizeBytes <= (size_t)optin) {
+      nmax = n;
+      break;
+    }
+  if (nmax < 2) return 0;
+  const int bytes = (int)(tk_smem_doubles(nmax, CS) * 8);
+  if (cudaFuncSetAttribute(k_sytrd_cluster<CS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
+    return 0;
+  if (CS > 8 && cudaFuncSetAttribute(k_sytrd_cluster<CS>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                    cudaSuccess)
+    return 0;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(CS);
+  cfg.blockDim = dim3(TK_THREADS);
+  cfg.dynamicSmemBytes = bytes;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = CS;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int nc = 0;
+  if (cudaOccupancyMaxActiveClusters(&nc, k_sytrd_cluster<CS>, &cfg) != cudaSuccess || nc < 1) {
+    cudaGetLastError();
+    return 0;
+  }
+  *out = TkChoice{CS, nmax};
+  return 1;
+}
+
+TkChoice tk_choice(int dev, int want) {
+  static std::mutex mu;
+  static TkChoice cache[64][3];
+  static bool done[64][3];
+  const int slot = want == 8 ? 1 : (want == 16 ? 2 : 0);
+  std::lock_guard<std::mutex> g(mu);
+  if (dev < 0 || dev >= 64) return TkChoice{0, 0};
+  if (!done[dev][slot]) {
+    TkChoice ch{0, 0};
+    if (want != 8 && tk_try<16>(dev, &ch)) {
+    } else if (want != 16) {
+      tk_try<8>(dev, &ch);
+    }
+    cache[dev][slot] = ch;
+    done[dev][slot] = true;
+  }
+  return cache[dev][slot];
+}
+}  // namespace
+
 
 extern "C" int gwb_sytrd_set_trace(long long* cycles6) {
   g_sytrd_trace = cycles6;
@@ -825,8 +1091,18 @@ extern "C" int gwb_sytrd(int32_t m, double* A, int64_t lda, double* d, double* e
   // blocks of the cooperative launch: one per SM, or fewer (a cheaper grid
   // barrier against less bandwidth for the products; gwb_sytrd_set_blocks)
   const int nblk = std::max((m + TD_THREADS - 1) / TD_THREADS, g_sytrd_blocks > 0 ? std::min(g_sytrd_blocks, sms) : sms);
+  // the trailing part that fits one cluster's shared memory goes to the
+  // cluster kernel; the cooperative kernel reduces whole panels before it
+  const TkChoice ch = (g_sytrd_cluster != 0 && m > 1) ? tk_choice(dev, g_sytrd_cluster) : TkChoice{0, 0};
+  int kend = m;
+  if (ch.cs > 0) kend = m <= ch.nmax ? 0 : (m - ch.nmax + TD_NB - 1) / TD_NB * TD_NB;
+  if (m > 1) GWB_CUDA_TRY(cudaMemsetAsync(tau + (m - 1), 0, sizeof(double), st));
+  if (kend < m - 1) {
+    GWB_REQUIRE(m - kend <= ch.nmax, "internal: trailing part larger than the cluster holds");
+  }
   TdArgs args;
   args.m = m;
+  args.kend = kend;
   args.A = A;
   args.lda = lda;
   args.d = d;
@@ -842,14 +1118,33 @@ extern "C" int gwb_sytrd(int32_t m, double* A, int64_t lda, double* d, double* e
   args.status = status;
   args.wait_cycles = tc_wait_cycles();
   args.trace = g_sytrd_trace;
-  // V and W start at zero (entries above a reflector's row are read as zeros)
-  GWB_CUDA_TRY(cudaMemsetAsync(w, 0, need, st));
-  if (m > 1) GWB_CUDA_TRY(cudaMemsetAsync(tau + (m - 1), 0, sizeof(double), st));
-  const size_t smem = (size_t)std::max(m, TD_WARPS * 2 * 32 * TD_NB) * 8;
-  GWB_CUDA_TRY(cudaFuncSetAttribute(k_sytrd_coop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  void* kargs[] = {&args};
-  GWB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sytrd_coop, dim3(nblk), dim3(TD_THREADS), kargs, smem, st));
-  count_launches(1);
+  if (kend > 0) {
+    // V and W start at zero (entries above a reflector's row are read as zeros)
+    GWB_CUDA_TRY(cudaMemsetAsync(w, 0, need, st));
+    const size_t smem = (size_t)std::max(m, TD_WARPS * 2 * 32 * TD_NB) * 8;
+    GWB_CUDA_TRY(cudaFuncSetAttribute(k_sytrd_coop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    void* kargs[] = {&args};
+    GWB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sytrd_coop, dim3(nblk), dim3(TD_THREADS), kargs, smem, st));
+    count_launches(1);
+  }
+  if (kend < m - 1) {
+    TkArgs ta{m, kend, A, lda, d, e, tau};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ch.cs);
+    cfg.blockDim = dim3(TK_THREADS);
+    cfg.dynamicSmemBytes = tk_smem_doubles(m - kend, ch.cs) * 8;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = ch.cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    if (ch.cs == 16) GWB_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_sytrd_cluster<16>, ta));
+    else GWB_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_sytrd_cluster<8>, ta));
+    count_launches(1);
+  }
   return GWB_OK;
 }
 

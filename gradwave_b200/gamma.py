@@ -657,9 +657,11 @@ def _embed_rows(c: torch.Tensor, npad: int) -> torch.Tensor:
 
 
 class _LearnedGamma:
-    """The learned preconditioner on the Gamma path: the network's complex-row
-    kernel (``gwb::precond_apply``) on the sqrt(w)-scaled half-sphere rows of
-    the selected bands, with the stall rule of the complex solver (a band
+    """The learned preconditioner on the Gamma path: the network on the
+    tcgen05 tensor cores (``gwb_precond_learned_gamma``), reading the
+    selected bands' embedded real rows as their sqrt(w)-scaled half-sphere
+    rows and writing the result in the same embedding, with the stall rule
+    of the complex solver (a band
     whose residual has not improved on its best by 10 % for 3 rounds keeps
     TPA from then on; ``gwb_stall_update``; GWB_STALL_RATIO and
     GWB_STALL_PATIENCE change the 0.9 and the 3). Its per-band state follows
@@ -675,6 +677,7 @@ class _LearnedGamma:
         self.best = torch.full((nb,), float("inf"), dtype=torch.float64, device=dev)
         self.count = torch.zeros(nb, dtype=torch.uint8, device=dev)
         self.tpa_only = torch.zeros(nb, dtype=torch.uint8, device=dev)
+        self._work = None
 
     def keep(self, mask: torch.Tensor) -> None:
         self.best, self.count, self.tpa_only = self.best[mask], self.count[mask], self.tpa_only[mask]
@@ -689,12 +692,19 @@ class _LearnedGamma:
         _lib.call("gwb_stall_update", rn.data_ptr(), self.best.data_ptr(), self.count.data_ptr(),
                   self.tpa_only.data_ptr(), n_all, self.ratio, self.patience, _lib.stream_ptr(rn.device))
         nhalf = int(self.t_half.shape[1])
-        xs, rs = _half_rows(x[sel], nhalf), _half_rows(r[sel], nhalf)
-        n = int(xs.shape[0])
-        idx = torch.arange(n, dtype=torch.int32, device=x.device).reshape(1, n)
-        d = torch.ops.gwb.precond_apply(xs[None], rs[None], self.t_half, idx, eig[sel].reshape(1, n),
-                                        self.params, self.tpa_only[sel].reshape(1, n))
-        return _embed_rows(d[0], npad)
+        x, r, eig = x.contiguous(), r.contiguous(), eig.contiguous()
+        sl = sel.to(torch.int32).contiguous()
+        n = int(sl.shape[0])
+        d = torch.empty(n, npad, dtype=torch.float64, device=x.device)
+        need = int(_lib.load().gwb_precond_learned_gamma_work_bytes(n, nhalf))
+        if self._work is None or self._work.numel() < need:
+            self._work = torch.empty(need, dtype=torch.uint8, device=x.device)
+        # the embedded rows in place: no gather, no complex copies
+        _lib.call("gwb_precond_learned_gamma", self.params.data_ptr(), n_all, n, nhalf, npad, x.data_ptr(),
+                  x.stride(0), r.data_ptr(), r.stride(0), self.t_half.data_ptr(), eig.data_ptr(), sl.data_ptr(),
+                  self.tpa_only.data_ptr(), d.data_ptr(), npad, self._work.data_ptr(), self._work.numel(),
+                  _lib.stream_ptr(x.device))
+        return d
 
 
 class _Locked:

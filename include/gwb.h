@@ -340,6 +340,13 @@ size_t gwb_sytrd_work_bytes(int32_t m);
 /* Blocks of gwb_sytrd's cooperative launch (0: one per SM): fewer blocks make
  * the grid barrier cheaper and leave less bandwidth for the products. */
 int gwb_sytrd_set_blocks(int32_t blocks);
+/* The trailing part of gwb_sytrd inside one thread-block cluster: once the
+ * trailing matrix fits the cluster's distributed shared memory (about 620
+ * rows with 16 CTAs of 1024 threads), a second launch of size x 1 x 1 CTAs
+ * finishes the reduction there (two cluster barriers per column instead of
+ * two grid barriers). size: -1 the largest cluster the device schedules (16,
+ * else 8; the default), 0 the cooperative launch alone, 8 or 16 that size. */
+int gwb_sytrd_set_cluster(int32_t size);
 /* Phase trace of gwb_sytrd (NULL: off): later launches add the SM cycles of
  * block 0 to cycles6[0..5] = before the product, the product y = A v, the
  * barrier after it, the column's w and the next column's update, the
@@ -459,13 +466,34 @@ int gwb_precond_features(int32_t nk, int32_t nb, int32_t n_add, int32_t npw, con
                          float* feats, void* stream);
 /* As gwb_precond_teter with the coefficient TPA * exp(clamp(network, -3, 3));
  * bands with tpa_only[k][b] != 0 (uint8 (nk, nb), may be NULL) keep TPA.
- * work: device scratch of gwb_precond_learned_work_bytes(nk, n_add, npw) bytes
- * (per-row statistics and per-chunk partial norms, 8-byte aligned). */
+ * The network runs on the tcgen05 tensor cores (128 plane waves per MMA
+ * tile, accumulators in TMEM), or with gwb_precond_set_kernel(0) on the
+ * mma.sync path. work: device scratch of gwb_precond_learned_work_bytes(nk,
+ * n_add, npw) bytes (per-row statistics, per-tile partial norms, and in its
+ * last 8 bytes an int status that a tensor-core wait which ran out sets to
+ * GWB_ERR_TIMEOUT; 8-byte aligned). */
 int64_t gwb_precond_learned_work_bytes(int32_t nk, int32_t n_add, int32_t npw);
 int gwb_precond_learned(const float* params, int32_t nk, int32_t nb, int32_t n_add, int32_t npw, const void* x,
                         int64_t x_kstride, const void* r, int64_t r_kstride, const double* t, const double* eig,
                         const int32_t* sel, const uint8_t* tpa_only, void* d, int64_t d_kstride, void* work,
                         size_t work_bytes, void* stream);
+/* Inference kernel of gwb_precond_learned: 1 tcgen05 (the default), 0 mma.sync. */
+int gwb_precond_set_kernel(int32_t which);
+/* The learned preconditioner on the Gamma path's embedded real rows (gradwave
+ * core/gamma.py:70-160 half-sphere layout): row b of x and r (nb rows,
+ * x_row / r_row doubles apart) holds phi with half-sphere coefficient
+ * c_G = phi[2G-1] + i phi[2G] (c_0 = phi[0]), G < nhalf. For s < n_add the
+ * unit row d[s] (d_row doubles apart; coordinates from 2 nhalf - 1 to npad
+ * set to zero) is the preconditioned residual of band sel[s] in the same
+ * embedding: TPA * exp(clamp(network, -3, 3)) on the tcgen05 tensor cores
+ * (TPA alone when tpa_only[b] != 0; may be NULL). t_half: kinetic diagonal
+ * per half-sphere slot; eig: nb. work: gwb_precond_learned_gamma_work_bytes
+ * (status int in its last 8 bytes, as above). */
+int64_t gwb_precond_learned_gamma_work_bytes(int32_t n_add, int32_t nhalf);
+int gwb_precond_learned_gamma(const float* params, int32_t nb, int32_t n_add, int32_t nhalf, int32_t npad,
+                              const double* x, int64_t x_row, const double* r, int64_t r_row, const double* t_half,
+                              const double* eig, const int32_t* sel, const uint8_t* tpa_only, double* d,
+                              int64_t d_row, void* work, size_t work_bytes, void* stream);
 /* Stall fallback: count[i] = rounds since rn[i] last fell below ratio * rn_best[i]
  * (rn_best starts at +inf, count at 0); tpa_only[i] = 1 once count[i] >= patience. */
 int gwb_stall_update(const double* rn, double* rn_best, uint8_t* count, uint8_t* tpa_only, int32_t n, double ratio,

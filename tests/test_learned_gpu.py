@@ -169,9 +169,19 @@ def test_committed_network_gains_on_heldout_cell(cuda_device):
     assert rl.n_iter < rt.n_iter
 
 
-def test_tensor_core_inference_matches_reference_forward(cuda_device):
-    """The mma.sync inference path of gwb_precond_learned against features +
-    the CUDA-core forward + TPA, on random parameters."""
+@pytest.fixture(params=[1, 0], ids=["tcgen05", "mma_sync"])
+def precond_kernel(request):
+    """Both inference kernels of gwb_precond_learned."""
+    from gradwave_b200 import _lib
+    _lib.call("gwb_precond_set_kernel", request.param)
+    yield request.param
+    _lib.call("gwb_precond_set_kernel", 1)
+
+
+def test_tensor_core_inference_matches_reference_forward(cuda_device, precond_kernel):
+    """The tensor-core inference paths of gwb_precond_learned (tcgen05 and
+    mma.sync) against features + the CUDA-core forward + TPA, on random
+    parameters; 1000 plane waves per row leave a ragged last tile."""
     from gradwave_b200 import _lib, learned
     rng = np.random.default_rng(21)
     nk, nb, npw, n_add = 2, 4, 1000, 3
@@ -222,3 +232,49 @@ def test_stall_rule(cuda_device):
         _lib.call("gwb_stall_update", rn.data_ptr(), best.data_ptr(), cnt.data_ptr(), tpa.data_ptr(), n, 0.9, 3, s)
     torch.cuda.synchronize()
     assert tpa.tolist() == [0, 1, 1]
+
+
+def test_gamma_embedded_rows_match_half_rows(cuda_device):
+    """gwb_precond_learned_gamma on the Gamma path's embedded real rows equals
+    the complex-row kernel on the same rows as sqrt(w)-scaled half-sphere rows
+    (gamma._half_rows / _embed_rows), including a band kept on TPA and a
+    ragged last tile; the pad coordinates come back zero."""
+    from gradwave_b200 import _lib, learned
+    from gradwave_b200.gamma import _embed_rows, _half_rows
+    rng = np.random.default_rng(31)
+    nb, nhalf = 6, 777
+    nphi = 2 * nhalf - 1
+    npad = nphi + 1
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(cuda_device)
+    x = rng.standard_normal((nb, npad))
+    r = rng.standard_normal((nb, npad)) * rng.uniform(0, 2, npad)
+    x[:, nphi:] = 0.0
+    r[:, nphi:] = 0.0
+    X, R = T(x), T(r)
+    th = T(np.abs(rng.standard_normal(nhalf)) * 60)
+    eig = T(rng.standard_normal(nb) * 5)
+    sel = torch.tensor([4, 0, 2, 5], dtype=torch.int32, device=cuda_device)
+    tpa = torch.zeros(nb, dtype=torch.uint8, device=cuda_device)
+    tpa[2] = 1
+    p = learned.init_params(7)
+    p[-65:] = rng.standard_normal(65).astype(np.float32) * 0.2
+    P = torch.from_numpy(p).to(cuda_device)
+    n = int(sel.shape[0])
+    D = torch.full((n, npad), 7.0, dtype=torch.float64, device=cuda_device)
+    W = torch.empty(int(_lib.load().gwb_precond_learned_gamma_work_bytes(n, nhalf)), dtype=torch.uint8,
+                    device=cuda_device)
+    s = _lib.stream_ptr(cuda_device)
+    _lib.call("gwb_precond_learned_gamma", P.data_ptr(), nb, n, nhalf, npad, X.data_ptr(), npad, R.data_ptr(), npad,
+              th.data_ptr(), eig.data_ptr(), sel.data_ptr(), tpa.data_ptr(), D.data_ptr(), npad, W.data_ptr(),
+              W.numel(), s)
+    sl = sel.long()
+    xs, rs = _half_rows(X[sl], nhalf), _half_rows(R[sl], nhalf)
+    idx = torch.arange(n, dtype=torch.int32, device=cuda_device).reshape(1, n)
+    ref = torch.ops.gwb.precond_apply(xs[None], rs[None], th.reshape(1, -1), idx, eig[sl].reshape(1, n), P,
+                                      tpa[sl].reshape(1, n))
+    ref = _embed_rows(ref[0], npad)
+    torch.cuda.synchronize()
+    assert float((D - ref).abs().max()) <= 1e-12
+    assert float(D[:, nphi:].abs().max()) == 0.0
+    assert torch.allclose(torch.linalg.vector_norm(D, dim=1), torch.ones(n, dtype=torch.float64,
+                                                                         device=cuda_device), atol=1e-12)

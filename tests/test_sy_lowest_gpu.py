@@ -8,7 +8,9 @@ against LAPACK (numpy's eigh / eigvalsh):
   orthonormality of U, all at float64 round-off of |A|;
 * exact degenerate clusters (a triple, a sextuple), a pair 1e-13 apart, the
   Wilkinson matrices W21+ and W201+ (pairs equal to ~1e-14), and a block
-  diagonal matrix (reflectors with tau = 0).
+  diagonal matrix (reflectors with tau = 0);
+* each both with the trailing part in a thread-block cluster (the default)
+  and with the cooperative launch alone (``gwb_sytrd_set_cluster``).
 """
 
 import numpy as np
@@ -16,6 +18,17 @@ import pytest
 import torch
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(params=[-1, 0], ids=["cluster", "coop"])
+def cluster(request):
+    """Both forms of the tridiagonalisation: the cooperative launch with the
+    trailing part in one thread-block cluster (the default), and the
+    cooperative launch alone."""
+    from gradwave_b200 import _lib
+    _lib.call("gwb_sytrd_set_cluster", request.param)
+    yield request.param
+    _lib.call("gwb_sytrd_set_cluster", -1)
 
 
 def _sytrd(a, dev):
@@ -76,8 +89,10 @@ def _check(a, nev, dev):
     assert np.abs(u.T @ u - np.eye(nev)).max() <= 1e-12
 
 
-@pytest.mark.parametrize("m", [2, 3, 9, 200])
-def test_tridiagonalisation_rebuilds_q(cuda_device, m):
+@pytest.mark.parametrize("m", [2, 3, 9, 17, 200, 700, 1100])
+def test_tridiagonalisation_rebuilds_q(cuda_device, cluster, m):
+    """Q^T A Q = T with Q rebuilt from the stored reflectors; 700 and 1100
+    hand the trailing part from the cooperative launch to the cluster."""
     a = _rand(m, m)
     A, d, e, tau = _sytrd(a, cuda_device)
     T = np.diag(d) + np.diag(e, 1) + np.diag(e, -1)
@@ -86,18 +101,18 @@ def test_tridiagonalisation_rebuilds_q(cuda_device, m):
         v = np.zeros(m)
         v[j + 1] = 1.0
         v[j + 2:] = A[j, j + 2:]
-        Q = Q @ (np.eye(m) - tau[j] * np.outer(v, v))
+        Q -= tau[j] * np.outer(Q @ v, v)
     scale = float(np.abs(np.linalg.eigvalsh(a)).max())
     assert np.abs(Q.T @ a @ Q - T).max() <= 1e-13 * scale
     assert np.abs(Q.T @ Q - np.eye(m)).max() <= 1e-13
 
 
-@pytest.mark.parametrize("m,nev", [(2, 2), (3, 3), (50, 50), (641, 320), (1920, 496)])
-def test_lowest_pairs_random(cuda_device, m, nev):
+@pytest.mark.parametrize("m,nev", [(2, 2), (3, 3), (50, 50), (600, 300), (641, 320), (1920, 496)])
+def test_lowest_pairs_random(cuda_device, cluster, m, nev):
     _check(_rand(m, m + 1), nev, cuda_device)
 
 
-def test_lowest_pairs_degenerate_clusters(cuda_device):
+def test_lowest_pairs_degenerate_clusters(cuda_device, cluster):
     m = 700
     lam = np.linspace(-5.0, 80.0, m)
     lam[10:13] = lam[10]
@@ -107,11 +122,11 @@ def test_lowest_pairs_degenerate_clusters(cuda_device):
 
 
 @pytest.mark.parametrize("m", [21, 201])
-def test_wilkinson(cuda_device, m):
+def test_wilkinson(cuda_device, cluster, m):
     _check(_wilkinson(m), m, cuda_device)
 
 
-def test_block_diagonal_needs_no_reflection(cuda_device):
+def test_block_diagonal_needs_no_reflection(cuda_device, cluster):
     a = np.zeros((300, 300))
     a[:120, :120] = _rand(120, 7)
     a[120:, 120:] = _rand(180, 8) + 3.0 * np.eye(180)
