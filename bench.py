@@ -912,16 +912,27 @@ def run_eigh(args):
         ref = torch.linalg.eigvalsh(a)[:nev]
         out["eig_err_rel"] = float((w - ref).abs().max() / ref.abs().max())
         if args.eigh_trace:
-            # the trace covers the cooperative launch: run it over all columns
-            tr = torch.zeros(6, dtype=torch.int64, device=dev)
+            # the cooperative launch over all columns, then the default
+            # split (its cluster part per cluster column)
+            tr = torch.zeros(10, dtype=torch.int64, device=dev)
             _lib.call("gwb_sytrd_set_cluster", 0)
             _lib.call("gwb_sytrd_set_trace", tr.data_ptr())
             trd()
             torch.cuda.synchronize()
-            _lib.call("gwb_sytrd_set_trace", None)
             _lib.call("gwb_sytrd_set_cluster", -1)
+            tc = torch.zeros(10, dtype=torch.int64, device=dev)
+            _lib.call("gwb_sytrd_set_trace", tc.data_ptr())
+            trd()
+            torch.cuda.synchronize()
+            _lib.call("gwb_sytrd_set_trace", None)
+            nc = int(lib.gwb_sytrd_cluster_rows(m))
+            out["cluster_rows"] = nc
+            if nc > 1:
+                cn = ["column_and_reflector", "row_pass", "exchange", "cluster_barrier"]
+                out["cluster_us_per_column"] = {k: round(v / 1.9e3 / (nc - 1), 3)
+                                                for k, v in zip(cn, tc.cpu().tolist()[6:])}
             names = ["reflector", "row_products", "barrier_1", "w_and_next_column", "barrier_2", "trailing_update"]
-            out["us_per_column"] = {n: round(c / 1.9e3 / (m - 1), 3) for n, c in zip(names, tr.cpu().tolist())}
+            out["us_per_column"] = {n: round(c / 1.9e3 / (m - 1), 3) for n, c in zip(names, tr.cpu().tolist()[:6])}
         out["status"] = int(st.item())
         print(json.dumps(out), flush=True)
     return 0

@@ -404,24 +404,29 @@ __global__ void __launch_bounds__(TD_THREADS, 1) k_sytrd_coop(TdArgs a) {
 // matrix (n = m - t0 rows, fully updated, both triangles) fits in the
 // cluster's distributed shared memory, the rest of the reduction runs there:
 // CTA c of the cluster keeps rows c, c + CS, c + 2 CS, ... (full rows), and a
-// column costs two cluster barriers and one pass over the local rows instead
+// column costs one cluster barrier and one pass over the local rows instead
 // of two grid barriers and several L2 round trips.
 //
 // Unblocked form (LAPACK dsytd2: p = tau A v, w = p - (tau/2)(p.v) v,
-// A <- A - v w^T - w v^T), with the rank-2 update of column j deferred into
-// the pass that forms the product of column j + 1:
-//   entry of column j: every CTA holds column j, fully updated, in abuf (its
-//     rows were broadcast by their owners) and forms the reflector from it
-//     with the same arithmetic, so all CTAs hold identical v_j and tau_j;
-//   pass F(j): own rows i > j, columns k > j: A_ik -= v_i w_k + w_i v_k with
-//     reflector j - 1, and y_i = sum_k A_ik v_j[k] on the updated values;
-//     p_i = tau_j y_i and the CTA's part of p.v go to every CTA;
-//   barrier; step O(j): every CTA forms w_j from the gathered p; each owner
-//     brings its rows' element of column j + 1 up to date with reflector j
-//     and sends it to every CTA's abuf; barrier.
-// Sums that every CTA needs (|x|^2, p.v) are formed in the same fixed order
-// in every CTA. The cluster barriers are hardware barriers that every thread
-// of every CTA reaches the same number of times.
+// A <- A - v w^T - w v^T), with the rank-2 update of reflector j - 1
+// deferred into the pass that forms the product of reflector j:
+//   R(j), in every CTA with the same arithmetic: w_{j-1} = p - K v_{j-1}
+//     from the gathered p and the partial sums of p.v; column j brought up
+//     to date from its gathered entries, a_k = raw_k - v_k w_j - w_k v_j
+//     (reflector j - 1); the reflector v_j, tau_j from it. Every CTA thus
+//     holds identical w_{j-1}, v_j and tau_j;
+//   F(j), own rows i > j, columns k > j: A_ik -= v_i w_k + w_i v_k
+//     (reflector j - 1) and y_i = sum_k A_ik v_j[k] on the updated values;
+//     each owner sends p_i = tau_j y_i, its row's element of column j + 1
+//     (raw, updated through reflector j - 1) and the CTA's part of p.v to
+//     every CTA;
+//   one cluster barrier.
+// The gathered vectors are double-buffered by the parity of j: a CTA still
+// reading column j's values while another already sends column j + 1's uses
+// the other buffer, and the barrier after j + 1 orders the next reuse. Sums
+// that every CTA needs are formed in one fixed order in every CTA. The
+// cluster barriers are hardware barriers that every thread of every CTA
+// reaches the same number of times.
 constexpr int TK_THREADS = 1024;
 constexpr int TK_WARPS = TK_THREADS / 32;
 constexpr int TK_SEG = 128;    // columns per warp item of the pass (4 per lane)
@@ -432,11 +437,12 @@ struct TkArgs {
   double* A;
   int64_t lda;
   double *d, *e, *tau;
+  long long* trace;  // cycles of CTA 0 in R, F, the exchange, the barrier (4 slots), or null
 };
 
 __host__ __device__ inline size_t tk_smem_doubles(int n, int cs) {
   const int nl = (n + cs - 1) / cs;
-  return (size_t)nl * n + 6 * (size_t)n + (size_t)nl * TK_NSEG;
+  return (size_t)nl * n + 8 * (size_t)n + (size_t)nl * TK_NSEG;
 }
 
 // Sum over the block, formed in one fixed order (every thread gets it).
@@ -451,12 +457,21 @@ __device__ __forceinline__ double tk_block_sum(double v, double* red) {
   return s;
 }
 
+#define TK_MARK(slot)                                      \
+  do {                                                     \
+    if (a.trace && c == 0 && tid == 0) {                   \
+      const long long _now = clock64();                   \
+      a.trace[(slot)] += _now - tk_t;                      \
+      tk_t = _now;                                         \
+    }                                                      \
+  } while (0)
+
 template <int CS>
 __global__ void __launch_bounds__(TK_THREADS, 1) k_sytrd_cluster(TkArgs a) {
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
   extern __shared__ __align__(16) double tk_smem[];
-  __shared__ double part[CS];
+  __shared__ double part[2][CS];
   __shared__ double red[TK_WARPS];
   const int c = (int)cl.block_rank();
   const int n = a.m - a.t0, t0 = a.t0;
@@ -464,52 +479,70 @@ __global__ void __launch_bounds__(TK_THREADS, 1) k_sytrd_cluster(TkArgs a) {
   const int64_t lda = a.lda;
   double* A = a.A + t0 + (int64_t)t0 * lda;  // the trailing block's origin
   double* Al = tk_smem;                       // local row li = trailing row c + li CS, n columns
-  double* abuf = Al + (size_t)nl * n;         // [2][n]: column j, fully updated
-  double* vbuf = abuf + 2 * (size_t)n;        // [2][n]: v_j
-  double* wbuf = vbuf + 2 * (size_t)n;        // w_j
-  double* pbuf = wbuf + n;                    // p_j, gathered
-  double* ypart = pbuf + n;                   // [nl][TK_NSEG] row partial products
+  double* col = Al + (size_t)nl * n;          // column j, fully updated
+  double* vbuf = col + n;                     // [2][n]: v_j by parity of j
+  double* wbuf = vbuf + 2 * (size_t)n;        // w_{j-1}
+  double* pbuf = wbuf + n;                    // [2][n]: gathered p by parity
+  double* rbuf = pbuf + 2 * (size_t)n;        // [2][n]: gathered raw column entries by parity
+  double* ypart = rbuf + 2 * (size_t)n;       // [nl][TK_NSEG] row partial products
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  long long tk_t = clock64();
 
   for (int t = tid; t < nl * n; t += TK_THREADS) {
     const int li = t / n, k = t - li * n, i = c + li * CS;
     Al[t] = i < n ? A[k + (int64_t)i * lda] : 0.0;  // column i = row i
   }
-  for (int k = tid; k < n; k += TK_THREADS) abuf[k] = A[k];
+  for (int k = tid; k < n; k += TK_THREADS) col[k] = A[k];
   cl.sync();  // every CTA of the cluster runs: shared windows are valid
 
+  double tau_prev = 0.0;
   for (int j = 0; j + 1 < n; ++j) {
-    const double* aj = abuf + (size_t)(j & 1) * n;
-    double* vj = vbuf + (size_t)(j & 1) * n;
-    const double* vq = vbuf + (size_t)((j + 1) & 1) * n;  // v_{j-1}
-    // ---- reflector j from column j (identical in every CTA) ----
+    const int q = j & 1, qp = q ^ 1;
+    double* vj = vbuf + (size_t)q * n;
+    const double* vq = vbuf + (size_t)qp * n;  // v_{j-1}
+    // ---- R(j): w_{j-1}, column j, reflector j (identical in every CTA) ----
+    if (j > 0) {
+      double K = 0.0;
+      for (int r = 0; r < CS; ++r) K += part[qp][r];
+      K *= 0.5 * tau_prev;
+      const double* pg = pbuf + (size_t)qp * n;
+      for (int k = j + tid; k < n; k += TK_THREADS) wbuf[k] = pg[k] - K * vq[k];
+      __syncthreads();
+      const double* rg = rbuf + (size_t)qp * n;
+      const double wj = wbuf[j], vjj = vq[j];
+      for (int k = j + tid; k < n; k += TK_THREADS) col[k] = rg[k] - vq[k] * wj - wbuf[k] * vjj;
+      __syncthreads();
+    }
     double s = 0.0;
-    for (int k = j + 2 + tid; k < n; k += TK_THREADS) s += aj[k] * aj[k];
+    for (int k = j + 2 + tid; k < n; k += TK_THREADS) s += col[k] * col[k];
     s = tk_block_sum(s, red);
-    const double alpha = aj[j + 1];
+    const double alpha = col[j + 1];
     double tau = 0.0, beta = alpha, scl = 0.0;
     if (s > 0.0) {
       beta = -copysign(sqrt(alpha * alpha + s), alpha);
       tau = (beta - alpha) / beta;
       scl = 1.0 / (alpha - beta);
     }
-    for (int k = j + 1 + tid; k < n; k += TK_THREADS) vj[k] = k == j + 1 ? 1.0 : aj[k] * scl;
+    for (int k = j + 1 + tid; k < n; k += TK_THREADS) vj[k] = k == j + 1 ? 1.0 : col[k] * scl;
     if (c == 0) {
-      for (int k = j + 2 + tid; k < n; k += TK_THREADS) A[k + (int64_t)j * lda] = aj[k] * scl;
+      for (int k = j + 2 + tid; k < n; k += TK_THREADS) A[k + (int64_t)j * lda] = col[k] * scl;
       if (tid == 0) {
-        a.d[t0 + j] = aj[j];
+        a.d[t0 + j] = col[j];
         a.e[t0 + j] = beta;
         a.tau[t0 + j] = tau;
-        A[j + (int64_t)j * lda] = aj[j];
+        A[j + (int64_t)j * lda] = col[j];
         A[j + 1 + (int64_t)j * lda] = beta;
       }
     }
     __syncthreads();
-    // ---- pass F(j): update with reflector j - 1, product with v_j ----
+    TK_MARK(0);
+    // ---- F(j): update with reflector j - 1, product with v_j ----
     const int kb = j + 1, ncol = n - kb;
     const int nseg = (ncol + TK_SEG - 1) / TK_SEG;
     const int wps = TK_WARPS / nseg;  // warps per segment
     const int li0 = kb > c ? (kb - c + CS - 1) / CS : 0;
+    double* pg = pbuf + (size_t)q * n;
+    double* rg = rbuf + (size_t)q * n;
     if (warp < nseg * wps) {
       const int sg = warp / wps, wr = warp - sg * wps;
       const int klo = kb + sg * TK_SEG, khi = min(n, klo + TK_SEG);
@@ -537,6 +570,7 @@ __global__ void __launch_bounds__(TK_THREADS, 1) k_sytrd_cluster(TkArgs a) {
               x -= vi * wk[u] + wi * qk[u];
               row[k] = x;
             }
+            if (u == 0 && sg == 0 && lane == 0) rg[i] = x;  // column j + 1's entry (k = kb)
             y += x * vk[u];
           }
         }
@@ -545,7 +579,8 @@ __global__ void __launch_bounds__(TK_THREADS, 1) k_sytrd_cluster(TkArgs a) {
       }
     }
     __syncthreads();
-    // p_i = tau y_i for own rows into the local gather; the CTA's part of p.v
+    TK_MARK(1);
+    // p_i = tau y_i for own rows; the CTA's part of p.v; everything to every CTA
     double pv = 0.0;
     for (int li = li0 + tid; li < nl; li += TK_THREADS) {
       const int i = c + li * CS;
@@ -553,7 +588,7 @@ __global__ void __launch_bounds__(TK_THREADS, 1) k_sytrd_cluster(TkArgs a) {
         double y = 0.0;
         for (int sg = 0; sg < nseg; ++sg) y += ypart[(size_t)li * TK_NSEG + sg];
         const double p = tau * y;
-        pbuf[i] = p;
+        pg[i] = p;
         pv += p * vj[i];
       }
     }
@@ -561,31 +596,35 @@ __global__ void __launch_bounds__(TK_THREADS, 1) k_sytrd_cluster(TkArgs a) {
     const int nown = nl - li0;
     for (int t = tid; t < nown * CS; t += TK_THREADS) {
       const int li = li0 + t / CS, r = t % CS, i = c + li * CS;
-      if (i < n && r != c) *cl.map_shared_rank(pbuf + i, r) = pbuf[i];
+      if (i < n && r != c) {
+        *cl.map_shared_rank(pg + i, r) = pg[i];
+        *cl.map_shared_rank(rg + i, r) = rg[i];
+      }
     }
-    if (tid < CS) *cl.map_shared_rank(part + c, tid) = pv;
+    if (tid < CS) *cl.map_shared_rank(&part[q][c], tid) = pv;
+    tau_prev = tau;
+    TK_MARK(2);
     cl.sync();
-    // ---- step O(j): w_j, and the own rows of column j + 1 to every CTA ----
-    double K = 0.0;
-    for (int r = 0; r < CS; ++r) K += part[r];
-    K *= 0.5 * tau;
-    for (int k = kb + tid; k < n; k += TK_THREADS) wbuf[k] = pbuf[k] - K * vj[k];
-    __syncthreads();
-    double* an = abuf + (size_t)((j + 1) & 1) * n;
-    const double wn = wbuf[kb], vn = vj[kb];
-    for (int t = tid; t < nown * CS; t += TK_THREADS) {
-      const int li = li0 + t / CS, r = t % CS, i = c + li * CS;
-      if (i < n) *cl.map_shared_rank(an + i, r) = Al[(size_t)li * n + kb] - vj[i] * wn - wbuf[i] * vn;
-    }
-    cl.sync();
+    TK_MARK(3);
   }
-  if (c == 0 && tid == 0) {
-    const double dl = abuf[(size_t)((n - 1) & 1) * n + (n - 1)];
-    a.d[t0 + n - 1] = dl;
-    A[(n - 1) + (int64_t)(n - 1) * lda] = dl;
+  if (c == 0) {
+    // the last diagonal element: column n - 1 through the last reflector
+    double dl = col[0];
+    if (n >= 2) {
+      const int j = n - 1, qp = (j - 1) & 1;
+      double K = 0.0;
+      for (int r = 0; r < CS; ++r) K += part[qp][r];
+      K *= 0.5 * tau_prev;
+      const double* vq = vbuf + (size_t)qp * n;
+      const double w = pbuf[(size_t)qp * n + j] - K * vq[j];
+      dl = rbuf[(size_t)qp * n + j] - 2.0 * vq[j] * w;
+    }
+    if (tid == 0) {
+      a.d[t0 + n - 1] = dl;
+      A[(n - 1) + (int64_t)(n - 1) * lda] = dl;
+    }
   }
 }
-
 
 // ---------------------------------------------------------------------------
 // The lowest nev eigenpairs of the tridiagonal (d, e), then of A.
@@ -1049,9 +1088,18 @@ TkChoice tk_choice(int dev, int want) {
 }
 }  // namespace
 
+extern "C" int32_t gwb_sytrd_cluster_rows(int32_t m) {
+  int dev = 0;
+  if (m <= 1 || g_sytrd_cluster == 0 || cudaGetDevice(&dev) != cudaSuccess) return 0;
+  const TkChoice ch = tk_choice(dev, g_sytrd_cluster);
+  if (ch.cs == 0) return 0;
+  const int kend = m <= ch.nmax ? 0 : (m - ch.nmax + TD_NB - 1) / TD_NB * TD_NB;
+  return kend < m - 1 ? m - kend : 0;
+}
 
-extern "C" int gwb_sytrd_set_trace(long long* cycles6) {
-  g_sytrd_trace = cycles6;
+
+extern "C" int gwb_sytrd_set_trace(long long* cycles10) {
+  g_sytrd_trace = cycles10;
   return GWB_OK;
 }
 
@@ -1128,7 +1176,7 @@ extern "C" int gwb_sytrd(int32_t m, double* A, int64_t lda, double* d, double* e
     count_launches(1);
   }
   if (kend < m - 1) {
-    TkArgs ta{m, kend, A, lda, d, e, tau};
+    TkArgs ta{m, kend, A, lda, d, e, tau, g_sytrd_trace ? g_sytrd_trace + 6 : nullptr};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ch.cs);
     cfg.blockDim = dim3(TK_THREADS);

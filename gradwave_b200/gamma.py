@@ -384,27 +384,6 @@ class _TcProjection:
             return keep - (keep @ v.T) @ v
         return t
 
-    def cholqr(self, y: torch.Tensor):
-        """Cholesky-QR of the rows of y with the Gram y y^T and the product
-        L^-1 y on the tensor cores (~1e-6 of unit rows, the float32 phase's
-        level); None when a Cholesky pivot falls below 1e-4 (the block is too
-        ill-conditioned for products at that level)."""
-        from .tc import OP_H, OP_N, zgemm_tc
-        n = y.shape[0]
-        y = y.contiguous()
-        self.pt.write(self._cx(y), n, src_ld=self.nc, src_kstride=0)
-        c = torch.empty(n, n, dtype=torch.complex128, device=y.device)
-        zgemm_tc(OP_H, n, n, self.nc, self.pt, self.pt, c, n, n * n)
-        g = c.real
-        L, info = torch.linalg.cholesky_ex(0.5 * (g + g.T))
-        if int(info.max()) != 0 or float(torch.diagonal(L).min()) <= 1e-4:
-            return None
-        li = torch.linalg.solve_triangular(L, torch.eye(n, dtype=L.dtype, device=L.device), upper=False)
-        self.pc.write(li.to(torch.complex128), n, src_ld=n, src_kstride=0, cols=n)
-        out = torch.empty(n, 2 * self.nc, dtype=torch.float64, device=y.device)
-        zgemm_tc(OP_N, n, self.nc, n, self.pc, self.pt, self._cx(out), self.nc, n * self.nc)
-        return out
-
     def subspace(self, hv_new: torch.Tensor, m: int, m0: int) -> torch.Tensor:
         """V[:m] HV[m0:m]^T (m x (m - m0)); hv_new = HV[m0:m]. From m0 = 0
         (after a restart) the kept planes of both serve directly."""
@@ -563,11 +542,6 @@ def _cholqr_images(x: torch.Tensor, hx: torch.Tensor, mm: _Products = _CUBLAS):
     return x, hx
 
 
-# Cholesky-QR of the float32 phase on the tensor cores with GWB_TC_CHOLQR=1
-# (default: float64 Gram and product)
-_TC_CHOLQR = __import__("os").environ.get("GWB_TC_CHOLQR", "0") == "1"
-
-
 def _expand(t: torch.Tensor, v: torch.Tensor, tcp: _TcProjection | None = None,
             locked: torch.Tensor | None = None, mm: _Products = _CUBLAS, low: bool = False) -> torch.Tensor:
     """New directions from preconditioned residuals: unit rows, two
@@ -585,24 +559,20 @@ def _expand(t: torch.Tensor, v: torch.Tensor, tcp: _TcProjection | None = None,
     when the first already left the Gram matrix within 1e-13 of the identity
     (it would change the rows by that much).
 
-    ``low`` (the float32 phase, with ``tcp``): both projection passes and
-    both Cholesky-QR rounds (Gram and L^-1 y) on the tensor cores. The first
-    pass leaves components along v of ~1e-6 that the Cholesky-QR may amplify
-    by the block's condition number; the second pass brings them back to
-    ~1e-6 of unit rows, and the second Cholesky-QR (of a nearly orthonormal
-    block) restores orthonormality among the new rows. The basis of the
-    float32 phase is thus orthonormal to ~1e-6, the level of its float32
-    applies. A block too ill-conditioned for that (a Cholesky pivot below
-    1e-4) takes the float64 path below."""
+    ``low`` (the float32 phase, with ``tcp``): both projection passes on the
+    tensor cores, each followed by a float64 Cholesky-QR. The first pass
+    leaves components along v of ~1e-6 that the Cholesky-QR may amplify by
+    the block's condition number; the second pass brings them back to ~1e-6
+    of unit rows, and the second Cholesky-QR (of a nearly orthonormal block)
+    restores orthonormality among the new rows. The basis of the float32
+    phase is thus orthonormal to ~1e-6, the level of its float32 applies. A
+    block whose Cholesky factorisation breaks down takes the float64 path
+    below."""
     t = t / torch.linalg.vector_norm(t, dim=1, keepdim=True).clamp_min(1e-300)
     lk = locked if locked is not None else v[:0]
     if low and tcp is not None and lk.shape[0] == 0:
-        if _TC_CHOLQR:
-            y = tcp.cholqr(tcp.project(t, v))
-            y2 = tcp.cholqr(tcp.project(y, v)) if y is not None else None
-        else:
-            y = _cholqr(tcp.project(t, v), mm)
-            y2 = _cholqr(tcp.project(y, v), mm) if y is not None else None
+        y = _cholqr(tcp.project(t, v), mm)
+        y2 = _cholqr(tcp.project(y, v), mm) if y is not None else None
         if y2 is not None:
             return y2
     _project_out(t, lk, mm)

@@ -347,11 +347,15 @@ int gwb_sytrd_set_blocks(int32_t blocks);
  * two grid barriers). size: -1 the largest cluster the device schedules (16,
  * else 8; the default), 0 the cooperative launch alone, 8 or 16 that size. */
 int gwb_sytrd_set_cluster(int32_t size);
+/* Rows of an m x m matrix that gwb_sytrd reduces inside the cluster (0: none). */
+int32_t gwb_sytrd_cluster_rows(int32_t m);
 /* Phase trace of gwb_sytrd (NULL: off): later launches add the SM cycles of
- * block 0 to cycles6[0..5] = before the product, the product y = A v, the
+ * block 0 to cycles10[0..5] = before the product, the product y = A v, the
  * barrier after it, the column's w and the next column's update, the
- * barrier after that, the trailing updates. For tuning. */
-int gwb_sytrd_set_trace(long long* cycles6);
+ * barrier after that, the trailing updates (the cooperative launch); and of
+ * the cluster's CTA 0 to cycles10[6..9] = the column and its reflector, the
+ * pass over the rows, the exchange, the cluster barrier. For tuning. */
+int gwb_sytrd_set_trace(long long* cycles10);
 int gwb_sytrd(int32_t m, double* A, int64_t lda, double* d, double* e, double* tau, void* work, size_t work_bytes,
               int* status, void* stream);
 /* The nev lowest eigenpairs of a real symmetric m x m matrix (m <= 4096):
