@@ -743,25 +743,52 @@ __global__ void __launch_bounds__(PU_THREADS) k_precond_learned_umma(PuArgs a) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   };
 
-  for (int w = blockIdx.x; w < a.total; w += gridDim.x) {
-    const int row = w / a.tiles, tile = w - row * a.tiles;
-    const int k = row / a.n_add, s = row - k * a.n_add;
-    const int b = a.sel[(int64_t)k * a.n_add + s];
-    const bool plain = a.tpa_only && a.tpa_only[(int64_t)k * a.nb + b];
-    const double tbv = a.stats[2 * row], rrms = a.stats[2 * row + 1], eps = a.eig[(int64_t)k * a.nb + b];
-    const int gi = tile * PU_TILE + tid;
-    const bool valid = gi < a.npw;
-    cplx<double> rv = mk<double>(0.0, 0.0);
-    double tg = 0.0;
-    if (valid) {
-      tg = a.t[(int64_t)k * a.npw + gi];
+  // a tile's inputs: its row's band, statistics and eigenvalue, this
+  // thread's residual coefficient and kinetic energy. The next tile's are
+  // loaded before the current tile's MMA chain, so their latency (a
+  // dependent chain sel -> band -> row) overlaps the network.
+  struct TileIn {
+    int row, tile, k, s, b;
+    bool plain, valid;
+    double tbv, rrms, eps, tg;
+    cplx<double> rv;
+  };
+  auto fetch = [&](int w) {
+    TileIn in;
+    in.row = w / a.tiles;
+    in.tile = w - in.row * a.tiles;
+    in.k = in.row / a.n_add;
+    in.s = in.row - in.k * a.n_add;
+    in.b = a.sel[(int64_t)in.k * a.n_add + in.s];
+    in.plain = a.tpa_only && a.tpa_only[(int64_t)in.k * a.nb + in.b];
+    in.tbv = a.stats[2 * in.row];
+    in.rrms = a.stats[2 * in.row + 1];
+    in.eps = a.eig[(int64_t)in.k * a.nb + in.b];
+    const int gi = in.tile * PU_TILE + tid;
+    in.valid = gi < a.npw;
+    in.rv = mk<double>(0.0, 0.0);
+    in.tg = 0.0;
+    if (in.valid) {
+      in.tg = a.t[(int64_t)in.k * a.npw + gi];
       if (GAMMA) {
-        const double* rr = static_cast<const double*>(a.r) + (int64_t)b * a.r_row;
-        rv = gi == 0 ? mk<double>(rr[0], 0.0) : mk<double>(rr[2 * gi - 1], rr[2 * gi]);
+        const double* rr = static_cast<const double*>(a.r) + (int64_t)in.b * a.r_row;
+        in.rv = gi == 0 ? mk<double>(rr[0], 0.0) : mk<double>(rr[2 * gi - 1], rr[2 * gi]);
       } else {
-        rv = static_cast<const cplx<double>*>(a.r)[k * a.rk + (int64_t)b * a.npw + gi];
+        in.rv = static_cast<const cplx<double>*>(a.r)[in.k * a.rk + (int64_t)in.b * a.npw + gi];
       }
     }
+    return in;
+  };
+  TileIn nxt;
+  if (blockIdx.x < a.total) nxt = fetch(blockIdx.x);
+  for (int w = blockIdx.x; w < a.total; w += gridDim.x) {
+    const TileIn cur = nxt;
+    if (w + (int)gridDim.x < a.total) nxt = fetch(w + gridDim.x);
+    const int row = cur.row, tile = cur.tile, k = cur.k, s = cur.s;
+    const bool plain = cur.plain, valid = cur.valid;
+    const double tbv = cur.tbv, rrms = cur.rrms, eps = cur.eps, tg = cur.tg;
+    const cplx<double> rv = cur.rv;
+    const int gi = tile * PU_TILE + tid;
     double c = tpa_coeff(tg, tbv);
     if (!plain) {
       float u[NIN] = {0.f, 0.f, 0.f, 0.f};

@@ -440,9 +440,12 @@ struct TkArgs {
   long long* trace;  // cycles of CTA 0 in R, F, the exchange, the barrier (4 slots), or null
 };
 
+// local rows (padded to an even count of doubles, so the exchange buffers
+// after them are 16-byte aligned), column, v [2], w, (p, raw) pairs [2],
+// row partial products
 __host__ __device__ inline size_t tk_smem_doubles(int n, int cs) {
-  const int nl = (n + cs - 1) / cs;
-  return (size_t)nl * n + 8 * (size_t)n + (size_t)nl * TK_NSEG;
+  const size_t nl = (size_t)(n + cs - 1) / cs;
+  return (nl * n + 1) / 2 * 2 + 8 * (size_t)n + nl * TK_NSEG;
 }
 
 // Sum over the block, formed in one fixed order (every thread gets it).
@@ -479,12 +482,11 @@ __global__ void __launch_bounds__(TK_THREADS, 1) k_sytrd_cluster(TkArgs a) {
   const int64_t lda = a.lda;
   double* A = a.A + t0 + (int64_t)t0 * lda;  // the trailing block's origin
   double* Al = tk_smem;                       // local row li = trailing row c + li CS, n columns
-  double* col = Al + (size_t)nl * n;          // column j, fully updated
+  double* col = Al + ((size_t)nl * n + 1) / 2 * 2;  // column j, fully updated
   double* vbuf = col + n;                     // [2][n]: v_j by parity of j
   double* wbuf = vbuf + 2 * (size_t)n;        // w_{j-1}
-  double* pbuf = wbuf + n;                    // [2][n]: gathered p by parity
-  double* rbuf = pbuf + 2 * (size_t)n;        // [2][n]: gathered raw column entries by parity
-  double* ypart = rbuf + 2 * (size_t)n;       // [nl][TK_NSEG] row partial products
+  double2* prbuf = reinterpret_cast<double2*>(wbuf + n);  // [2][n]: gathered (p, raw) by parity
+  double* ypart = reinterpret_cast<double*>(prbuf + 2 * (size_t)n);  // [nl][TK_NSEG] row partial products
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   long long tk_t = clock64();
 
@@ -501,21 +503,27 @@ __global__ void __launch_bounds__(TK_THREADS, 1) k_sytrd_cluster(TkArgs a) {
     double* vj = vbuf + (size_t)q * n;
     const double* vq = vbuf + (size_t)qp * n;  // v_{j-1}
     // ---- R(j): w_{j-1}, column j, reflector j (identical in every CTA) ----
+    double s = 0.0;
     if (j > 0) {
       double K = 0.0;
       for (int r = 0; r < CS; ++r) K += part[qp][r];
       K *= 0.5 * tau_prev;
-      const double* pg = pbuf + (size_t)qp * n;
-      for (int k = j + tid; k < n; k += TK_THREADS) wbuf[k] = pg[k] - K * vq[k];
-      __syncthreads();
-      const double* rg = rbuf + (size_t)qp * n;
-      const double wj = wbuf[j], vjj = vq[j];
-      for (int k = j + tid; k < n; k += TK_THREADS) col[k] = rg[k] - vq[k] * wj - wbuf[k] * vjj;
-      __syncthreads();
+      const double2* pr = prbuf + (size_t)qp * n;
+      const double vjj = vq[j];
+      const double wj = pr[j].x - K * vjj;
+      for (int k = j + tid; k < n; k += TK_THREADS) {
+        const double2 x = pr[k];
+        const double vk = vq[k];
+        const double wk = x.x - K * vk;
+        const double ck = x.y - vk * wj - wk * vjj;
+        wbuf[k] = wk;
+        col[k] = ck;
+        if (k >= j + 2) s += ck * ck;
+      }
+    } else {
+      for (int k = j + 2 + tid; k < n; k += TK_THREADS) s += col[k] * col[k];
     }
-    double s = 0.0;
-    for (int k = j + 2 + tid; k < n; k += TK_THREADS) s += col[k] * col[k];
-    s = tk_block_sum(s, red);
+    s = tk_block_sum(s, red);  // its barriers also publish col and w
     const double alpha = col[j + 1];
     double tau = 0.0, beta = alpha, scl = 0.0;
     if (s > 0.0) {
@@ -541,8 +549,7 @@ __global__ void __launch_bounds__(TK_THREADS, 1) k_sytrd_cluster(TkArgs a) {
     const int nseg = (ncol + TK_SEG - 1) / TK_SEG;
     const int wps = TK_WARPS / nseg;  // warps per segment
     const int li0 = kb > c ? (kb - c + CS - 1) / CS : 0;
-    double* pg = pbuf + (size_t)q * n;
-    double* rg = rbuf + (size_t)q * n;
+    double2* pr = prbuf + (size_t)q * n;
     if (warp < nseg * wps) {
       const int sg = warp / wps, wr = warp - sg * wps;
       const int klo = kb + sg * TK_SEG, khi = min(n, klo + TK_SEG);
@@ -570,7 +577,7 @@ __global__ void __launch_bounds__(TK_THREADS, 1) k_sytrd_cluster(TkArgs a) {
               x -= vi * wk[u] + wi * qk[u];
               row[k] = x;
             }
-            if (u == 0 && sg == 0 && lane == 0) rg[i] = x;  // column j + 1's entry (k = kb)
+            if (u == 0 && sg == 0 && lane == 0) pr[i].y = x;  // column j + 1's entry (k = kb)
             y += x * vk[u];
           }
         }
@@ -588,7 +595,7 @@ __global__ void __launch_bounds__(TK_THREADS, 1) k_sytrd_cluster(TkArgs a) {
         double y = 0.0;
         for (int sg = 0; sg < nseg; ++sg) y += ypart[(size_t)li * TK_NSEG + sg];
         const double p = tau * y;
-        pg[i] = p;
+        pr[i].x = p;
         pv += p * vj[i];
       }
     }
@@ -596,10 +603,7 @@ __global__ void __launch_bounds__(TK_THREADS, 1) k_sytrd_cluster(TkArgs a) {
     const int nown = nl - li0;
     for (int t = tid; t < nown * CS; t += TK_THREADS) {
       const int li = li0 + t / CS, r = t % CS, i = c + li * CS;
-      if (i < n && r != c) {
-        *cl.map_shared_rank(pg + i, r) = pg[i];
-        *cl.map_shared_rank(rg + i, r) = rg[i];
-      }
+      if (i < n && r != c) *cl.map_shared_rank(pr + i, r) = pr[i];
     }
     if (tid < CS) *cl.map_shared_rank(&part[q][c], tid) = pv;
     tau_prev = tau;
@@ -616,8 +620,9 @@ __global__ void __launch_bounds__(TK_THREADS, 1) k_sytrd_cluster(TkArgs a) {
       for (int r = 0; r < CS; ++r) K += part[qp][r];
       K *= 0.5 * tau_prev;
       const double* vq = vbuf + (size_t)qp * n;
-      const double w = pbuf[(size_t)qp * n + j] - K * vq[j];
-      dl = rbuf[(size_t)qp * n + j] - 2.0 * vq[j] * w;
+      const double2 x = prbuf[(size_t)qp * n + j];
+      const double w = x.x - K * vq[j];
+      dl = x.y - 2.0 * vq[j] * w;
     }
     if (tid == 0) {
       a.d[t0 + n - 1] = dl;
