@@ -429,6 +429,7 @@ __global__ void __launch_bounds__(TD_THREADS, 1) k_sytrd_coop(TdArgs a) {
 // reaches the same number of times.
 constexpr int TK_THREADS = 1024;
 constexpr int TK_WARPS = TK_THREADS / 32;
+static_assert(TK_WARPS == 32, "tk_block_sum reduces one warp sum per lane");
 constexpr int TK_SEG = 128;    // columns per warp item of the pass (4 per lane)
 constexpr int TK_NSEG = 8;     // segments per row at most (n <= 1024)
 
@@ -448,15 +449,24 @@ __host__ __device__ inline size_t tk_smem_doubles(int n, int cs) {
   return (nl * n + 1) / 2 * 2 + 8 * (size_t)n + nl * TK_NSEG;
 }
 
-// Sum over the block, formed in one fixed order (every thread gets it).
+// Sum over the block: each warp's sum by shuffles, then every warp reduces
+// the 32 warp sums by shuffles in the same order, so every thread gets the
+// same value.
 __device__ __forceinline__ double tk_block_sum(double v, double* red) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   __syncthreads();
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
   __syncthreads();
-  double s = 0.0;
-#pragma unroll 8
-  for (int w = 0; w < TK_WARPS; ++w) s += red[w];
+  double s = red[threadIdx.x & 31];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
+// Sum of the CS per-CTA parts, by shuffles (the same order in every warp).
+template <int CS>
+__device__ __forceinline__ double tk_part_sum(const double* part) {
+  double s = (threadIdx.x & 31) < CS ? part[threadIdx.x & 31] : 0.0;
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   return s;
 }
 
@@ -505,9 +515,7 @@ __global__ void __launch_bounds__(TK_THREADS, 1) k_sytrd_cluster(TkArgs a) {
     // ---- R(j): w_{j-1}, column j, reflector j (identical in every CTA) ----
     double s = 0.0;
     if (j > 0) {
-      double K = 0.0;
-      for (int r = 0; r < CS; ++r) K += part[qp][r];
-      K *= 0.5 * tau_prev;
+      const double K = tk_part_sum<CS>(part[qp]) * (0.5 * tau_prev);
       const double2* pr = prbuf + (size_t)qp * n;
       const double vjj = vq[j];
       const double wj = pr[j].x - K * vjj;
@@ -616,9 +624,7 @@ __global__ void __launch_bounds__(TK_THREADS, 1) k_sytrd_cluster(TkArgs a) {
     double dl = col[0];
     if (n >= 2) {
       const int j = n - 1, qp = (j - 1) & 1;
-      double K = 0.0;
-      for (int r = 0; r < CS; ++r) K += part[qp][r];
-      K *= 0.5 * tau_prev;
+      const double K = tk_part_sum<CS>(part[qp]) * (0.5 * tau_prev);
       const double* vq = vbuf + (size_t)qp * n;
       const double2 x = prbuf[(size_t)qp * n + j];
       const double w = x.x - K * vq[j];
