@@ -109,6 +109,7 @@ _SIGNATURES = {
     "gwb_sytrd_set_trace": [_P],
     "gwb_sytrd_set_cluster": [_I],
     "gwb_sytrd_cluster_rows": [_I],
+    "gwb_sytrd_set_grid": [_I],
     "gwb_precond_set_kernel": [_I],
     "gwb_precond_learned_gamma_work_bytes": [_I, _I],
     "gwb_precond_learned_gamma": [_P, _I, _I, _I, _I, _P, _I64, _P, _I64, _P, _P, _P, _P, _P, _I64, _P, _SZ, _P],

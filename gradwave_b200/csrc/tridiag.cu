@@ -636,6 +636,229 @@ __global__ void __launch_bounds__(TK_THREADS, 1) k_sytrd_cluster(TkArgs a) {
     }
   }
 }
+// ---------------------------------------------------------------------------
+// The middle part across the whole GPU with the trailing matrix in shared
+// memory. Once the trailing matrix (n = m - t0 rows, fully updated, both
+// triangles) fits the shared memory of all the SMs (~1790 rows with one
+// 1024-thread CTA per SM), columns t0 .. t1 - 1 are reduced as in
+// k_sytrd_cluster, with the exchange through global memory: CTA c keeps rows
+// c, c + G, ... (G = the grid); per column every CTA forms w of the previous
+// reflector, the column and the reflector from the gathered (p, raw) pairs
+// (the same arithmetic everywhere), passes over its rows (the previous
+// reflector's rank-2 update fused with the product of the current one),
+// writes its rows' p and next-column entries and its part of p.v, and meets
+// the others at one grid barrier. The pairs and parts are double-buffered by
+// the parity of the column and read past L1 (ld.global.cg). When t1 < m - 1
+// the trailing part at t1, brought up to date with reflector t1 - 1, is
+// written back (both triangles) for the cluster kernel.
+constexpr int TG_NSEG = 16;  // segments of 128 columns per row at most (n <= 2048)
+
+struct TgArgs {
+  int m, t0, t1;
+  double* A;
+  int64_t lda;
+  double *d, *e, *tau;
+  double2* pr;     // [2][n] (p, raw) by parity
+  double* part;    // [2][gridDim.x] parts of p.v by parity
+  unsigned* bar;
+  int* status;
+  long long wait_cycles;
+};
+
+__host__ __device__ inline size_t tg_smem_doubles(int n, int g) {
+  const size_t nl = (size_t)(n + g - 1) / g;
+  return (nl * n + 1) / 2 * 2 + 3 * (size_t)n + nl * TG_NSEG;
+}
+
+// Sum of the g parts, read past L1, in the same order in every warp.
+__device__ __forceinline__ double tg_part_sum(const double* part, int g) {
+  double s = 0.0;
+  for (int i = (threadIdx.x & 31); i < g; i += 32) s += __ldcg(part + i);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
+__global__ void __launch_bounds__(TK_THREADS, 1) k_sytrd_grid(TgArgs a) {
+  extern __shared__ __align__(16) double tg_smem[];
+  __shared__ double red[TK_WARPS];
+  __shared__ double sc[2];
+  __shared__ int s_abort;
+  const int G = gridDim.x, c = blockIdx.x;
+  const int n = a.m - a.t0, t0 = a.t0, ncols = a.t1 - a.t0;
+  const int nl = (n + G - 1) / G;
+  const int64_t lda = a.lda;
+  double* A = a.A + t0 + (int64_t)t0 * lda;
+  double* Al = tg_smem;                                  // local row li = trailing row c + li G
+  double* vbuf = Al + ((size_t)nl * n + 1) / 2 * 2;      // [2][n]: v_j by parity
+  double* wbuf = vbuf + 2 * (size_t)n;                   // w_{j-1}
+  double* ypart = wbuf + n;                              // [nl][TG_NSEG]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_abort = 0;
+  for (int t = tid; t < nl * n; t += TK_THREADS) {
+    const int li = t / n, k = t - li * n, i = c + li * G;
+    Al[t] = i < n ? A[k + (int64_t)i * lda] : 0.0;  // column i = row i
+  }
+  // column 0 into registers before any CTA writes reflector 0 into it
+  double c0[2];
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int k = tid + TK_THREADS * r;
+    c0[r] = k < n ? A[k] : 0.0;
+  }
+  if (!grid_barrier(a.bar, a.status, a.wait_cycles, &s_abort)) return;
+
+  double tau_prev = 0.0;
+  for (int j = 0; j < ncols; ++j) {
+    const int q = j & 1, qp = q ^ 1;
+    double* vj = vbuf + (size_t)q * n;
+    const double* vq = vbuf + (size_t)qp * n;  // v_{j-1}
+    const double2* prq = a.pr + (size_t)qp * n;
+    // ---- R(j): w_{j-1}, column j (two entries per thread), reflector j ----
+    double ck[2] = {0.0, 0.0};
+    double s = 0.0;
+    double K = 0.0, wj = 0.0, vjj = 0.0;
+    if (j > 0) {
+      K = tg_part_sum(a.part + (size_t)qp * G, G) * (0.5 * tau_prev);
+      vjj = vq[j];
+      wj = __ldcg(&prq[j].x) - K * vjj;
+    }
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int k = j + tid + TK_THREADS * r;
+      if (k < n) {
+        double x;
+        if (j > 0) {
+          const double2 e2 = __ldcg(&prq[k]);
+          const double vk = vq[k];
+          const double wk = e2.x - K * vk;
+          wbuf[k] = wk;
+          x = e2.y - vk * wj - wk * vjj;
+        } else {
+          x = c0[r];  // column 0 (k = tid + 1024 r at j = 0)
+        }
+        ck[r] = x;
+        if (k >= j + 2) s += x * x;
+        if (k == j) sc[1] = x;
+        if (k == j + 1) sc[0] = x;
+      }
+    }
+    s = tk_block_sum(s, red);  // its barriers also publish sc and w
+    const double alpha = sc[0], dj = sc[1];
+    double tau = 0.0, beta = alpha, scl = 0.0;
+    if (s > 0.0) {
+      beta = -copysign(sqrt(alpha * alpha + s), alpha);
+      tau = (beta - alpha) / beta;
+      scl = 1.0 / (alpha - beta);
+    }
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int k = j + tid + TK_THREADS * r;
+      if (k >= j + 1 && k < n) {
+        const double v = k == j + 1 ? 1.0 : ck[r] * scl;
+        vj[k] = v;
+        if (c == 0 && k >= j + 2) A[k + (int64_t)j * lda] = v;
+      }
+    }
+    if (c == 0 && tid == 0) {
+      a.d[t0 + j] = dj;
+      a.e[t0 + j] = beta;
+      a.tau[t0 + j] = tau;
+      A[j + (int64_t)j * lda] = dj;
+      A[j + 1 + (int64_t)j * lda] = beta;
+    }
+    __syncthreads();
+    // ---- F(j): update with reflector j - 1, product with v_j ----
+    const int kb = j + 1, ncol = n - kb;
+    const int nseg = (ncol + TK_SEG - 1) / TK_SEG;
+    const int wps = TK_WARPS / nseg;
+    const int li0 = kb > c ? (kb - c + G - 1) / G : 0;
+    double2* prw = a.pr + (size_t)q * n;
+    if (warp < nseg * wps) {
+      const int sg = warp / wps, wr = warp - sg * wps;
+      const int klo = kb + sg * TK_SEG, khi = min(n, klo + TK_SEG);
+      double vk[4], wk[4], qk[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int k = klo + lane + 32 * u;
+        const bool in = k < khi;
+        vk[u] = in ? vj[k] : 0.0;
+        wk[u] = (in && j > 0) ? wbuf[k] : 0.0;
+        qk[u] = (in && j > 0) ? vq[k] : 0.0;
+      }
+      for (int li = li0 + wr; li < nl; li += wps) {
+        const int i = c + li * G;
+        if (i >= n) break;
+        double* row = Al + (size_t)li * n;
+        const double vi = j > 0 ? vq[i] : 0.0, wi = j > 0 ? wbuf[i] : 0.0;
+        double y = 0.0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int k = klo + lane + 32 * u;
+          if (k < khi) {
+            double x = row[k];
+            if (j > 0) {
+              x -= vi * wk[u] + wi * qk[u];
+              row[k] = x;
+            }
+            if (u == 0 && sg == 0 && lane == 0) prw[i].y = x;  // column j + 1's entry (k = kb)
+            y += x * vk[u];
+          }
+        }
+        for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+        if (lane == 0) ypart[(size_t)li * TG_NSEG + sg] = y;
+      }
+    }
+    __syncthreads();
+    double pv = 0.0;
+    for (int li = li0 + tid; li < nl; li += TK_THREADS) {
+      const int i = c + li * G;
+      if (i < n) {
+        double y = 0.0;
+        for (int sg = 0; sg < nseg; ++sg) y += ypart[(size_t)li * TG_NSEG + sg];
+        const double p = tau * y;
+        prw[i].x = p;
+        pv += p * vj[i];
+      }
+    }
+    pv = tk_block_sum(pv, red);
+    if (tid == 0) a.part[(size_t)q * G + c] = pv;
+    tau_prev = tau;
+    if (!grid_barrier(a.bar, a.status, a.wait_cycles, &s_abort)) return;
+  }
+  const int J = ncols;  // the first column not reduced here
+  if (J >= n - 1) {
+    // to the end: the last diagonal element through the last reflector
+    if (c == 0 && n >= 2) {
+      const int qp = (J - 1) & 1;
+      const double K = tg_part_sum(a.part + (size_t)qp * G, G) * (0.5 * tau_prev);
+      const double* vq = vbuf + (size_t)qp * n;
+      const double2 x = __ldcg(&a.pr[(size_t)qp * n + (n - 1)]);
+      const double w = x.x - K * vq[n - 1];
+      const double dl = x.y - 2.0 * vq[n - 1] * w;
+      if (tid == 0) {
+        a.d[t0 + n - 1] = dl;
+        A[(n - 1) + (int64_t)(n - 1) * lda] = dl;
+      }
+    }
+    return;
+  }
+  // the trailing part at J through reflector J - 1, back to global memory
+  if (J > 0) {
+    const int qp = (J - 1) & 1;
+    const double K = tg_part_sum(a.part + (size_t)qp * G, G) * (0.5 * tau_prev);
+    const double* vq = vbuf + (size_t)qp * n;
+    const double2* prq = a.pr + (size_t)qp * n;
+    for (int k = J + tid; k < n; k += TK_THREADS) wbuf[k] = __ldcg(&prq[k].x) - K * vq[k];
+    __syncthreads();
+    for (int li = 0; li < nl; ++li) {
+      const int i = c + li * G;
+      if (i < J || i >= n) continue;
+      const double vi = vq[i], wi = wbuf[i];
+      const double* row = Al + (size_t)li * n;
+      for (int k = J + tid; k < n; k += TK_THREADS) A[k + (int64_t)i * lda] = row[k] - vi * wbuf[k] - wi * vq[k];
+    }
+  }
+}
 
 // ---------------------------------------------------------------------------
 // The lowest nev eigenpairs of the tridiagonal (d, e), then of A.
@@ -1099,13 +1322,84 @@ TkChoice tk_choice(int dev, int want) {
 }
 }  // namespace
 
+// the shared-memory-resident grid part: 0 off (the default: measured no
+// faster than the cooperative launch, ~11 us per column), 1 on
+static int g_sytrd_grid = 0;
+
+extern "C" int gwb_sytrd_set_grid(int32_t on) {
+  GWB_REQUIRE(on == 0 || on == 1, "on must be 0 or 1");
+  g_sytrd_grid = on;
+  return GWB_OK;
+}
+
+namespace {
+// The largest trailing part the grid kernel holds with one CTA per SM (0: none).
+int tg_nmax(int dev, int sms) {
+  static std::mutex mu;
+  static int cache[64];
+  static bool done[64];
+  std::lock_guard<std::mutex> g(mu);
+  if (dev < 0 || dev >= 64) return 0;
+  if (!done[dev]) {
+    int nmax = 0, optin = 0;
+    cudaFuncAttributes fa{};
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess &&
+        cudaFuncGetAttributes(&fa, k_sytrd_grid) == cudaSuccess) {
+      for (int n = TG_NSEG * TK_SEG; n >= 2; --n)
+        if (tg_smem_doubles(n, sms) * 8 + fa.sharedSizeBytes <= (size_t)optin) {
+          nmax = n;
+          break;
+        }
+      int per_sm = 0;
+      if (nmax >= 2 &&
+          (cudaFuncSetAttribute(k_sytrd_grid, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(tg_smem_doubles(nmax, sms) * 8)) != cudaSuccess ||
+           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sytrd_grid, TK_THREADS,
+                                                         tg_smem_doubles(nmax, sms) * 8) != cudaSuccess ||
+           per_sm < 1)) {
+        cudaGetLastError();
+        nmax = 0;
+      }
+    }
+    cache[dev] = nmax;
+    done[dev] = true;
+  }
+  return cache[dev];
+}
+
+// Where gwb_sytrd hands over: columns [0, k1) in the cooperative launch,
+// [k1, k2) in the grid kernel, [k2, m - 1) in the cluster.
+struct SyPlan {
+  int k1, k2;
+  TkChoice ch;
+};
+
+SyPlan sy_plan(int m, int dev, int sms) {
+  SyPlan p{m, m, TkChoice{0, 0}};
+  if (m <= 1) return p;
+  p.ch = g_sytrd_cluster != 0 ? tk_choice(dev, g_sytrd_cluster) : TkChoice{0, 0};
+  const int gmax = g_sytrd_grid ? tg_nmax(dev, sms) : 0;
+  // the cluster's first column: the trailing part fits its shared memory
+  const int kc = p.ch.cs > 0 ? std::max(0, m - p.ch.nmax) : m - 1;
+  if (gmax >= 2 && kc > 0) {
+    p.k1 = m <= gmax ? 0 : (m - gmax + TD_NB - 1) / TD_NB * TD_NB;
+    p.k2 = std::max(p.k1, kc);
+    if (p.k2 == p.k1 && p.ch.cs == 0) p.k2 = m - 1;
+  } else if (p.ch.cs > 0) {
+    p.k1 = p.k2 = m <= p.ch.nmax ? 0 : (m - p.ch.nmax + TD_NB - 1) / TD_NB * TD_NB;
+  }
+  if (p.k1 >= m - 1) p.k1 = p.k2 = m;  // all in the cooperative launch
+  return p;
+}
+}  // namespace
+
 extern "C" int32_t gwb_sytrd_cluster_rows(int32_t m) {
   int dev = 0;
   if (m <= 1 || g_sytrd_cluster == 0 || cudaGetDevice(&dev) != cudaSuccess) return 0;
-  const TkChoice ch = tk_choice(dev, g_sytrd_cluster);
-  if (ch.cs == 0) return 0;
-  const int kend = m <= ch.nmax ? 0 : (m - ch.nmax + TD_NB - 1) / TD_NB * TD_NB;
-  return kend < m - 1 ? m - kend : 0;
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  const SyPlan p = sy_plan(m, dev, sms);
+  return p.k2 < m - 1 ? m - p.k2 : 0;
 }
 
 
@@ -1150,14 +1444,15 @@ extern "C" int gwb_sytrd(int32_t m, double* A, int64_t lda, double* d, double* e
   // blocks of the cooperative launch: one per SM, or fewer (a cheaper grid
   // barrier against less bandwidth for the products; gwb_sytrd_set_blocks)
   const int nblk = std::max((m + TD_THREADS - 1) / TD_THREADS, g_sytrd_blocks > 0 ? std::min(g_sytrd_blocks, sms) : sms);
-  // the trailing part that fits one cluster's shared memory goes to the
-  // cluster kernel; the cooperative kernel reduces whole panels before it
-  const TkChoice ch = (g_sytrd_cluster != 0 && m > 1) ? tk_choice(dev, g_sytrd_cluster) : TkChoice{0, 0};
-  int kend = m;
-  if (ch.cs > 0) kend = m <= ch.nmax ? 0 : (m - ch.nmax + TD_NB - 1) / TD_NB * TD_NB;
+  // whole panels in the cooperative launch until the trailing part fits the
+  // shared memory of all SMs, then the grid kernel until it fits one
+  // cluster's, then the cluster
+  const SyPlan plan = sy_plan(m, dev, sms);
+  const TkChoice ch = plan.ch;
+  const int kend = plan.k1;
   if (m > 1) GWB_CUDA_TRY(cudaMemsetAsync(tau + (m - 1), 0, sizeof(double), st));
-  if (kend < m - 1) {
-    GWB_REQUIRE(m - kend <= ch.nmax, "internal: trailing part larger than the cluster holds");
+  if (plan.k2 < m - 1) {
+    GWB_REQUIRE(ch.cs > 0 && m - plan.k2 <= ch.nmax, "internal: trailing part larger than the cluster holds");
   }
   TdArgs args;
   args.m = m;
@@ -1186,12 +1481,36 @@ extern "C" int gwb_sytrd(int32_t m, double* A, int64_t lda, double* d, double* e
     GWB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sytrd_coop, dim3(nblk), dim3(TD_THREADS), kargs, smem, st));
     count_launches(1);
   }
-  if (kend < m - 1) {
-    TkArgs ta{m, kend, A, lda, d, e, tau, g_sytrd_trace ? g_sytrd_trace + 6 : nullptr};
+  if (plan.k2 > plan.k1) {
+    GWB_REQUIRE(m - plan.k1 <= tg_nmax(dev, sms), "internal: trailing part larger than the grid holds");
+    TgArgs ga;
+    ga.m = m;
+    ga.t0 = plan.k1;
+    ga.t1 = plan.k2;
+    ga.A = A;
+    ga.lda = lda;
+    ga.d = d;
+    ga.e = e;
+    ga.tau = tau;
+    ga.pr = reinterpret_cast<double2*>(w);  // the cooperative launch's panel vectors, free by now
+    ga.part = w + 4 * (size_t)m;
+    ga.bar = args.bar;
+    ga.status = status;
+    ga.wait_cycles = args.wait_cycles;
+    const size_t smem = tg_smem_doubles(m - plan.k1, sms) * 8;
+    // the barrier counter starts at zero (its low bits are the arrival count)
+    GWB_CUDA_TRY(cudaMemsetAsync(args.bar, 0, sizeof(unsigned), st));
+    void* kargs[] = {&ga};
+    GWB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sytrd_grid, dim3(sms), dim3(TK_THREADS), kargs, smem, st));
+    count_launches(1);
+  }
+  if (plan.k2 < m - 1) {
+    const int kend2 = plan.k2;
+    TkArgs ta{m, kend2, A, lda, d, e, tau, g_sytrd_trace ? g_sytrd_trace + 6 : nullptr};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ch.cs);
     cfg.blockDim = dim3(TK_THREADS);
-    cfg.dynamicSmemBytes = tk_smem_doubles(m - kend, ch.cs) * 8;
+    cfg.dynamicSmemBytes = tk_smem_doubles(m - kend2, ch.cs) * 8;
     cfg.stream = st;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;

@@ -347,6 +347,12 @@ int gwb_sytrd_set_blocks(int32_t blocks);
  * two grid barriers). size: -1 the largest cluster the device schedules (16,
  * else 8; the default), 0 the cooperative launch alone, 8 or 16 that size. */
 int gwb_sytrd_set_cluster(int32_t size);
+/* The middle part of gwb_sytrd across the GPU with the trailing matrix in
+ * the shared memory of all SMs (up to ~1790 rows, one 1024-thread CTA per
+ * SM, one grid barrier per column), between the panels of the cooperative
+ * launch and the cluster: on = 1, or 0 (the default; it measures ~11 us per
+ * column, no faster than the cooperative launch). */
+int gwb_sytrd_set_grid(int32_t on);
 /* Rows of an m x m matrix that gwb_sytrd reduces inside the cluster (0: none). */
 int32_t gwb_sytrd_cluster_rows(int32_t m);
 /* Phase trace of gwb_sytrd (NULL: off): later launches add the SM cycles of

@@ -9,8 +9,11 @@ against LAPACK (numpy's eigh / eigvalsh):
 * exact degenerate clusters (a triple, a sextuple), a pair 1e-13 apart, the
   Wilkinson matrices W21+ and W201+ (pairs equal to ~1e-14), and a block
   diagonal matrix (reflectors with tau = 0);
-* each both with the trailing part in a thread-block cluster (the default)
-  and with the cooperative launch alone (``gwb_sytrd_set_cluster``).
+* each with the four forms of the tridiagonalisation: cooperative panels,
+  the opt-in shared-memory-resident grid kernel and the cluster; without the
+  cluster; without the grid kernel (the default); the cooperative launch
+  alone (``gwb_sytrd_set_grid``, ``gwb_sytrd_set_cluster``); 1920 passes
+  through all three launches in the first form.
 """
 
 import numpy as np
@@ -20,14 +23,18 @@ import torch
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(params=[-1, 0], ids=["cluster", "coop"])
+@pytest.fixture(params=[(1, -1), (1, 0), (0, -1), (0, 0)], ids=["grid+cluster", "grid", "cluster", "coop"])
 def cluster(request):
-    """Both forms of the tridiagonalisation: the cooperative launch with the
-    trailing part in one thread-block cluster (the default), and the
-    cooperative launch alone."""
+    """The forms of the tridiagonalisation: cooperative panels, then the
+    shared-memory-resident grid kernel (opt-in), then one thread-block
+    cluster; without the cluster; without the grid kernel (the default);
+    the cooperative launch alone."""
     from gradwave_b200 import _lib
-    _lib.call("gwb_sytrd_set_cluster", request.param)
+    grid, cl = request.param
+    _lib.call("gwb_sytrd_set_grid", grid)
+    _lib.call("gwb_sytrd_set_cluster", cl)
     yield request.param
+    _lib.call("gwb_sytrd_set_grid", 0)
     _lib.call("gwb_sytrd_set_cluster", -1)
 
 
@@ -92,7 +99,8 @@ def _check(a, nev, dev):
 @pytest.mark.parametrize("m", [2, 3, 9, 17, 200, 700, 1100])
 def test_tridiagonalisation_rebuilds_q(cuda_device, cluster, m):
     """Q^T A Q = T with Q rebuilt from the stored reflectors; 700 and 1100
-    hand the trailing part from the cooperative launch to the cluster."""
+    hand the trailing part from the grid kernel (or the cooperative launch)
+    to the cluster."""
     a = _rand(m, m)
     A, d, e, tau = _sytrd(a, cuda_device)
     T = np.diag(d) + np.diag(e, 1) + np.diag(e, -1)
