@@ -1009,6 +1009,79 @@ def run_precond(args):
     return 0
 
 
+def run_reference_gpu(args):
+    """The reference's own float64 block Davidson on this GPU: its builders,
+    ``BatchedHamiltonian`` (torch FFT + einsum nonlocal term) and
+    ``davidson_batched`` (TPA, cuSOLVER subspace eigensolves above m = 256),
+    all on cuda, imported from the reference package staged under
+    ``baseline/_ref/gradwave`` (a copy of its ``src/gradwave``: the package
+    cannot be pip-installed here, its build backend is missing from the
+    wheelhouse) through a namespace shim that skips its ``__init__`` (which
+    needs the absent ``ase``). One untimed solve of si2_fcc (cuFFT plans,
+    library handles), then one wall-timed solve of each ``--ref-configs``
+    cell from the identity start to ``--tol``, synchronised on both sides;
+    eigenvalue error against the golden eigenvalues of the reference's
+    converged CPU solve. This is the plain float64 TPA Davidson of the
+    reference on the same B200, for comparison with the package's own."""
+    import sys as _sys
+    import types
+
+    import torch
+    src = Path(__file__).resolve().parent / "baseline" / "_ref" / "gradwave"
+    if not src.is_dir():
+        print(json.dumps({"mode": "reference_gpu", "unavailable": "the reference package is not staged under "
+                          "baseline/_ref/gradwave"}), flush=True)
+        return 0
+    mod = types.ModuleType("gradwave")
+    mod.__path__ = [str(src)]
+    _sys.modules["gradwave"] = mod
+    from gradwave.core.batch import BatchedHamiltonian, build_batched, projectors_b
+    from gradwave.core.hamiltonian import build_projector_data
+    from gradwave.grids import build_fft_grid, build_gsphere
+    from gradwave.solvers.davidson import davidson_batched
+
+    from gradwave_b200.cells import _SPEC, make_cell
+    dev = torch.device("cuda", 0)
+
+    def solve(name):
+        ci = make_cell(name)
+        grid = build_fft_grid(ci.cell, ci.ecut, shape_override=ci.shape)
+        sph = [build_gsphere(grid, ci.ecut, k) for k in ci.kpoints]
+        sp = _SPEC["species"]["Si"]
+        rc = float(sp["rc"])
+        pds = []
+        for s in sph:
+            q = torch.sqrt(s.kpg2)
+            tab = torch.stack([torch.exp(-0.5 * (q * rc) ** 2), q * rc * torch.exp(-0.5 * (q * rc) ** 2)])
+            pds.append(build_projector_data(s, [0] * len(ci.positions), [tab], [[0, 1]],
+                                            [torch.diag(torch.tensor(sp["D"], dtype=torch.float64))],
+                                            grid.volume))
+        bk = build_batched(sph, pds, device=dev)
+        p = projectors_b(bk, torch.as_tensor(ci.positions).to(dev))
+        h = BatchedHamiltonian(bk, grid.shape, torch.as_tensor(ci.v_eff_r).to(dev), p)
+        x0 = ci.identity_start().to(dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = davidson_batched(h.apply, x0, bk.t, bk.mask, tol=args.tol, max_iter=300)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, res
+
+    solve("si2_fcc")
+    for name in args.ref_configs.split(","):
+        sec, res = solve(name)
+        out = {"mode": "reference_gpu", "config": name, "tol_ev": args.tol, "ms": round(1e3 * sec, 1),
+               "n_iter": int(res.n_iter), "form": "the reference's davidson_batched, complex float64, TPA, on cuda",
+               "max_residual_ev": float(res.residual_norms.max())}
+        try:
+            out["eig_err_ev"] = _eig_err(res.eigenvalues.cpu().numpy(), _golden(name))
+        except Exception as e:  # reported, so that the timing still prints
+            out["eig_err_ev"] = f"{type(e).__name__}: {e}"
+        print(json.dumps(out), flush=True)
+        del res
+        torch.cuda.empty_cache()
+    return 0
+
+
 def run_gamma(args):
     """The Gamma real path on a Gamma-only cell: ``--warmup`` untimed and one
     wall-timed ``davidson_gamma`` from the identity start on the lowest
@@ -1097,9 +1170,11 @@ def main():
     ap.add_argument("--moduli", type=int, default=18, help="--mode oz --oz-scheme crt: residues per operand")
     ap.add_argument("--eigh-sizes", default="993,1488,1984", help="--mode eigh: matrix sizes")
     ap.add_argument("--eigh-trace", action="store_true", help="--mode eigh: per-phase cycles of the tridiagonalisation")
+    ap.add_argument("--ref-configs", default="si8_cubic,si216_vacancy",
+                    help="--mode reference_gpu: cells for the reference's own solve on the GPU")
     ap.add_argument("--precond-rows", type=int, default=400, help="--mode precond: selected bands")
     ap.add_argument("--mode", default="solve", choices=["solve", "apply", "apply_gamma", "once", "tc", "gamma", "oz", "eigh",
-                                                       "precond"],
+                                                       "precond", "reference_gpu"],
                     help="apply: only time Hamiltonian applies; once: a single solve (profiling)")
     ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64"], help="arithmetic of --mode apply")
     ap.add_argument("--solver", default="learned-mixed", choices=["plain", "fp32exp", "mixed", "learned-mixed"],
@@ -1113,6 +1188,8 @@ def main():
         return run_tc(args)
     if args.mode == "oz":
         return run_oz(args)
+    if args.mode == "reference_gpu":
+        return run_reference_gpu(args)
     if args.mode == "precond":
         return run_precond(args)
     if args.mode == "eigh":
