@@ -251,9 +251,105 @@ def _oracle_round_times(ci, tol: float, gold_eig):
         traj += 1
 
 
+REF_SRC = ROOT / "baseline" / "_ref" / "gradwave"
+
+
+def _reference_import():
+    """The reference package staged under ``baseline/_ref/gradwave`` (a copy
+    of its ``src/gradwave``), imported through a namespace shim that skips
+    its ``__init__`` (which needs the absent ``ase``); False when it is not
+    staged."""
+    import types
+    if not REF_SRC.is_dir():
+        return False
+    if "gradwave" not in sys.modules:
+        mod = types.ModuleType("gradwave")
+        mod.__path__ = [str(REF_SRC)]
+        sys.modules["gradwave"] = mod
+    return True
+
+
+def _reference_setup(name, dev):
+    """The cell ``name`` built by the reference's own builders on ``dev``:
+    (cell inputs, BatchedK, BatchedHamiltonian)."""
+    import torch
+    from gradwave.core.batch import BatchedHamiltonian, build_batched, projectors_b
+    from gradwave.core.hamiltonian import build_projector_data
+    from gradwave.grids import build_fft_grid, build_gsphere
+
+    from gradwave_b200.cells import _SPEC, make_cell
+    ci = make_cell(name)
+    grid = build_fft_grid(ci.cell, ci.ecut, shape_override=ci.shape)
+    sph = [build_gsphere(grid, ci.ecut, k) for k in ci.kpoints]
+    sp = _SPEC["species"]["Si"]
+    rc = float(sp["rc"])
+    pds = []
+    for s in sph:
+        q = torch.sqrt(s.kpg2)
+        tab = torch.stack([torch.exp(-0.5 * (q * rc) ** 2), q * rc * torch.exp(-0.5 * (q * rc) ** 2)])
+        pds.append(build_projector_data(s, [0] * len(ci.positions), [tab], [[0, 1]],
+                                        [torch.diag(torch.tensor(sp["D"], dtype=torch.float64))], grid.volume))
+    bk = build_batched(sph, pds, device=dev)
+    p = projectors_b(bk, torch.as_tensor(ci.positions).to(dev))
+    h = BatchedHamiltonian(bk, grid.shape, torch.as_tensor(ci.v_eff_r).to(dev), p)
+    return ci, bk, h
+
+
+_REF_CPU_SETUP: dict = {}
+
+
+class _RoundStamps(list):
+    """``history_out`` of the reference's ``davidson_batched`` that also
+    records the wall time of each append (one per round, after its
+    Rayleigh-Ritz step)."""
+
+    def __init__(self):
+        super().__init__()
+        self.times = []
+
+    def append(self, item):
+        self.times.append(time.perf_counter())
+        super().append(item)
+
+
+def _reference_own_rounds(name, tol, gold_eig, n_rounds, threads):
+    """``n_rounds`` Davidson rounds of the reference's own ``davidson_batched``
+    (complex float64, TPA, torch on the host cores with ``threads``
+    threads) on the cell, from the identity start; a trajectory that reaches
+    every eigenvalue within 1e-8 Ha of ``gold_eig`` ends and the next starts
+    from the identity again. Returns [(ms, round, eig_err_ev, trajectory)]."""
+    import torch
+    from gradwave.solvers.davidson import davidson_batched
+    old = torch.get_num_threads()
+    torch.set_num_threads(threads)
+    try:
+        if name not in _REF_CPU_SETUP:  # built once per process
+            _REF_CPU_SETUP[name] = _reference_setup(name, torch.device("cpu"))
+        ci, bk, h = _REF_CPU_SETUP[name]
+        x0 = ci.identity_start()
+        out, traj = [], 0
+        while len(out) < n_rounds:
+            st = _RoundStamps()
+            t0 = time.perf_counter()
+            davidson_batched(h.apply, x0, bk.t, bk.mask, tol=tol, max_iter=n_rounds - len(out), history_out=st)
+            prev = t0
+            for (it, _, eig), t in zip(st, st.times):
+                err = float(np.abs(eig.numpy() - gold_eig).max()) if gold_eig is not None else float("nan")
+                out.append(((t - prev) * 1e3, int(it), err, traj))
+                prev = t
+                if err <= EIG_TOL_EV:
+                    break
+            traj += 1
+        return out[:n_rounds]
+    finally:
+        torch.set_num_threads(old)
+
+
 def run_reference(args):
-    """The reference's algorithm on the host cores (float64 oracle port, all
-    host threads): one Davidson round of the full workload per step."""
+    """The reference's own solver on the host cores (all host threads): one
+    Davidson round of the full workload per step, from the reference package
+    staged under ``baseline/_ref`` (``cpu_baseline.kind`` "reference"), or,
+    when it is not staged, from its float64 port in ``oracle/`` ("port")."""
     ws, rank, _ = _dist()
     if rank != 0:
         return 0
@@ -263,9 +359,13 @@ def run_reference(args):
     gold = _golden(args.config)
     gold_eig = None if gold is None else gold["eigenvalues"]
     ref = _reference_rounds(args.config)
-    with _OracleThreads(threads):
-        stream = _oracle_round_times(ci, args.tol, gold_eig)
-        rounds = [next(stream) for _ in range(args.warmup + args.steps)]
+    own = _reference_import()
+    if own:
+        rounds = _reference_own_rounds(args.config, args.tol, gold_eig, args.warmup + args.steps, threads)
+    else:
+        with _OracleThreads(threads):
+            stream = _oracle_round_times(ci, args.tol, gold_eig)
+            rounds = [next(stream) for _ in range(args.warmup + args.steps)]
     timed = [r[0] for r in rounds[args.warmup:]]
     ms_round = statistics.mean(timed)
     first = [r for r in rounds if r[3] == 0]
@@ -278,8 +378,9 @@ def run_reference(args):
         value, kind = ms_round * n_rounds, f"mean timed round x {n_rounds} rounds (the reference's own count)"
     sample = (f"{args.warmup + args.steps} consecutive Davidson rounds of the full {args.config} workload "
               f"(all {ci.bk.nk} k, {ci.nbands} bands, complex128) from the identity start; a solve ends when every "
-              f"eigenvalue is within 1e-8 Ha of the golden eigenvalues; float64 numpy/scipy restatement of "
-              f"the reference's davidson_batched + BatchedHamiltonian.apply")
+              f"eigenvalue is within 1e-8 Ha of the golden eigenvalues; "
+              + ("the reference's own davidson_batched + BatchedHamiltonian.apply (torch, CPU)" if own else
+                 "float64 numpy/scipy restatement of the reference's davidson_batched + BatchedHamiltonian.apply"))
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": "ms", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_round, 1),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "c128/f64",
@@ -289,8 +390,8 @@ def run_reference(args):
                        "parallelism": "single"},
             "step": "one Davidson round", "value_kind": kind, "rounds_per_solve": n_rounds,
             "round_ms": [round(r[0], 1) for r in rounds], "round_eig_err_ev": [r[2] for r in rounds],
-            "cpu_baseline": {"value": round(value, 1), "unit": "ms", "cores": threads, "kind": "port",
-                             "cpu": _cpu_model(), "sample": sample},
+            "cpu_baseline": {"value": round(value, 1), "unit": "ms", "cores": threads,
+                             "kind": "reference" if own else "port", "cpu": _cpu_model(), "sample": sample},
             "reference_own_solve": ref,
             "e2e": {"value": round(value, 1), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -306,16 +407,22 @@ def _cpu_baseline(args, ci, gold_eig) -> dict:
     ref = _reference_rounds(args.config)
     n = 2
     out = {}
+    own = _reference_import()
     for label, th in (("all", cores), ("default", min(cores, 8))):
-        with _OracleThreads(th):
-            stream = _oracle_round_times(ci, args.tol, gold_eig)
-            ms = [next(stream)[0] for _ in range(n)]
+        if own:
+            ms = [r[0] for r in _reference_own_rounds(args.config, args.tol, gold_eig, n, th)]
+        else:
+            with _OracleThreads(th):
+                stream = _oracle_round_times(ci, args.tol, gold_eig)
+                ms = [next(stream)[0] for _ in range(n)]
         out[label] = (th, statistics.mean(ms))
     n_rounds = ref["rounds"] if ref else None
     per_round = out["all"][1]
+    what = ("the reference's own davidson_batched (torch, CPU)" if own
+            else "the float64 oracle (a restatement of the reference)")
     return {"value": None if n_rounds is None else round(per_round * n_rounds, 1), "unit": "ms",
-            "cores": cores, "kind": "port", "cpu": _cpu_model(),
-            "sample": f"first {n} Davidson rounds of the full workload with the float64 oracle; value = mean "
+            "cores": cores, "kind": "reference" if own else "port", "cpu": _cpu_model(),
+            "sample": f"first {n} Davidson rounds of the full workload with {what}; value = mean "
                       f"round x {n_rounds} rounds (the reference's own count to 1e-8 Ha)",
             "ms_per_round": round(per_round, 1),
             "ms_per_round_default_threads": round(out["default"][1], 1),
@@ -1023,42 +1130,16 @@ def run_reference_gpu(args):
     eigenvalue error against the golden eigenvalues of the reference's
     converged CPU solve. This is the plain float64 TPA Davidson of the
     reference on the same B200, for comparison with the package's own."""
-    import sys as _sys
-    import types
-
     import torch
-    src = Path(__file__).resolve().parent / "baseline" / "_ref" / "gradwave"
-    if not src.is_dir():
+    if not _reference_import():
         print(json.dumps({"mode": "reference_gpu", "unavailable": "the reference package is not staged under "
                           "baseline/_ref/gradwave"}), flush=True)
         return 0
-    mod = types.ModuleType("gradwave")
-    mod.__path__ = [str(src)]
-    _sys.modules["gradwave"] = mod
-    from gradwave.core.batch import BatchedHamiltonian, build_batched, projectors_b
-    from gradwave.core.hamiltonian import build_projector_data
-    from gradwave.grids import build_fft_grid, build_gsphere
     from gradwave.solvers.davidson import davidson_batched
-
-    from gradwave_b200.cells import _SPEC, make_cell
     dev = torch.device("cuda", 0)
 
     def solve(name):
-        ci = make_cell(name)
-        grid = build_fft_grid(ci.cell, ci.ecut, shape_override=ci.shape)
-        sph = [build_gsphere(grid, ci.ecut, k) for k in ci.kpoints]
-        sp = _SPEC["species"]["Si"]
-        rc = float(sp["rc"])
-        pds = []
-        for s in sph:
-            q = torch.sqrt(s.kpg2)
-            tab = torch.stack([torch.exp(-0.5 * (q * rc) ** 2), q * rc * torch.exp(-0.5 * (q * rc) ** 2)])
-            pds.append(build_projector_data(s, [0] * len(ci.positions), [tab], [[0, 1]],
-                                            [torch.diag(torch.tensor(sp["D"], dtype=torch.float64))],
-                                            grid.volume))
-        bk = build_batched(sph, pds, device=dev)
-        p = projectors_b(bk, torch.as_tensor(ci.positions).to(dev))
-        h = BatchedHamiltonian(bk, grid.shape, torch.as_tensor(ci.v_eff_r).to(dev), p)
+        ci, bk, h = _reference_setup(name, dev)
         x0 = ci.identity_start().to(dev)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
