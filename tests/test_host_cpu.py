@@ -99,8 +99,9 @@ def test_band_path_and_chunk_rule():
 
 def test_bench_reference_arm_contract():
     """``bench.py --impl reference`` (the reference's CPU path, timed on the
-    host cores) prints one JSON line with the contract's keys; on the 2-atom
-    cell it runs in seconds."""
+    host cores) prints one JSON line with the contract's keys and says which
+    ran (the staged reference or the port); on the 2-atom cell it runs in
+    seconds."""
     import json
     import subprocess
     import sys
@@ -112,7 +113,11 @@ def test_bench_reference_arm_contract():
                 "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
         assert key in line, key
     assert line["impl"] == "reference" and line["higher_is_better"] is False and line["value"] > 0
-    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    # the reference's own solver when its package is staged under
+    # baseline/_ref, else the float64 port
+    staged = (ROOT / "baseline" / "_ref" / "gradwave").is_dir()
+    assert line["cpu_baseline"]["kind"] == ("reference" if staged else "port")
+    assert line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
 
 
