@@ -135,3 +135,39 @@ def test_autotune_records_and_lookup(tmp_path, monkeypatch):
     assert autotune.lookup("gamma", (96, 96, 96), 864) == {"w_budget_mb": 32, "nl_target": 296}
     assert autotune.lookup("complex", (96, 96, 96), 864) is None
     monkeypatch.setattr(autotune, "_CACHE", None)
+
+
+def test_new_switches_and_gamma_preconditioner_refuse_bad_arguments():
+    """The eigensolver and preconditioner switches accept only their
+    documented values, and the Gamma preconditioner entry refuses bad sizes
+    with GWB_ERR_ARG before it touches a device."""
+    from gradwave_b200 import _lib
+    for name, bad in (("gwb_sytrd_set_cluster", 5), ("gwb_sytrd_set_grid", 2), ("gwb_precond_set_kernel", 3)):
+        with pytest.raises(_lib.GwbError) as ex:
+            _lib.call(name, bad)
+        assert ex.value.status == _lib.GWB_ERR_ARG
+    # the defaults are accepted again (and restore the state)
+    _lib.call("gwb_sytrd_set_cluster", -1)
+    _lib.call("gwb_sytrd_set_grid", 0)
+    _lib.call("gwb_precond_set_kernel", 1)
+    lib = _lib.load()
+    assert lib.gwb_precond_learned_gamma_work_bytes(0, 100) == 0
+    nhalf = 100
+    need = int(lib.gwb_precond_learned_gamma_work_bytes(4, nhalf))
+    assert need == (4 * (2 + 1) + 1) * 8
+    p = 1  # never dereferenced: the size checks come first
+    # npad shorter than the embedding (2 nhalf - 1 coordinates)
+    with pytest.raises(_lib.GwbError) as ex:
+        _lib.call("gwb_precond_learned_gamma", p, 8, 4, nhalf, 2 * nhalf - 2, p, 2 * nhalf, p, 2 * nhalf, p, p, p,
+                  None, p, 2 * nhalf, p, need, None)
+    assert ex.value.status == _lib.GWB_ERR_ARG
+    # more selected rows than bands
+    with pytest.raises(_lib.GwbError) as ex:
+        _lib.call("gwb_precond_learned_gamma", p, 3, 4, nhalf, 2 * nhalf, p, 2 * nhalf, p, 2 * nhalf, p, p, p,
+                  None, p, 2 * nhalf, p, need, None)
+    assert ex.value.status == _lib.GWB_ERR_ARG
+    # a workspace smaller than asked for
+    with pytest.raises(_lib.GwbError) as ex:
+        _lib.call("gwb_precond_learned_gamma", p, 8, 4, nhalf, 2 * nhalf, p, 2 * nhalf, p, 2 * nhalf, p, p, p,
+                  None, p, 2 * nhalf, p, need - 8, None)
+    assert ex.value.status == _lib.GWB_ERR_ARG
