@@ -586,10 +586,9 @@ constexpr int PU_THREADS = 128;
 constexpr int PU_TILE = 128;
 constexpr int PU_K1 = 16, PU_K = 80;
 constexpr int PU_A = PU_TILE * PU_K * 2;   // 20480 B
-constexpr int PU_A1 = PU_TILE * PU_K1 * 2;  // 4096 B
 constexpr int PU_B1 = HID * PU_K1 * 2;      // 2048 B
 constexpr int PU_B = HID * PU_K * 2;        // 10240 B
-constexpr int PU_SMEM = PU_A + PU_A1 + PU_B1 + 2 * PU_B + 16;
+constexpr int PU_SMEM = PU_A + PU_B1 + 2 * PU_B + 16;  // 43 KB: five CTAs per SM
 constexpr int PU_TMEM_COLS = 64;
 // kind::f16 instruction descriptor: F32 accumulator, BF16 A and B, both
 // K-major, N = 64, M = 128
@@ -634,32 +633,39 @@ struct PuArgs {
   long long wait_cycles;
 };
 
-// This warp's 32 rows of the 64 accumulator columns -> SiLU -> (unless
-// keep) the BF16 row of the next A.
-__device__ __forceinline__ void pu_hidden(uint32_t taddr, uint8_t* sA, int row, float* h, bool keep) {
-  uint32_t r[4][16];
+// This warp's 32 rows of the 64 accumulator columns, 16 at a time: SiLU,
+// then either the BF16 chunks of the next A (hidden layers) or, for the last
+// hidden layer, layer 4's dot product with w4 added to o in column order.
+__device__ __forceinline__ float pu_hidden(uint32_t taddr, uint8_t* sA, int row, const float* w4, bool last,
+                                           float o) {
 #pragma unroll
-  for (int q = 0; q < 4; ++q) tmem_ld16(taddr + 16 * q, r[q]);
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+  for (int q = 0; q < 4; ++q) {
+    uint32_t r[16];
+    tmem_ld16(taddr + 16 * q, r);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    float h[16];
 #pragma unroll
-  for (int q = 0; q < 4; ++q)
+    for (int i = 0; i < 16; ++i) h[i] = silu_fast(__uint_as_float(r[i]));
+    if (last) {
 #pragma unroll
-    for (int i = 0; i < 16; ++i) h[16 * q + i] = silu_fast(__uint_as_float(r[q][i]));
-  if (!keep) {
+      for (int i = 0; i < 16; ++i) o = fmaf(bf(h[i]), w4[16 * q + i], o);
+    } else {
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      uint4 v;
-      v.x = pack_bf16(h[8 * c + 0], h[8 * c + 1]);
-      v.y = pack_bf16(h[8 * c + 2], h[8 * c + 3]);
-      v.z = pack_bf16(h[8 * c + 4], h[8 * c + 5]);
-      v.w = pack_bf16(h[8 * c + 6], h[8 * c + 7]);
-      *reinterpret_cast<uint4*>(sA + pu_off(row, 8 * c, PU_K)) = v;
+      for (int c = 0; c < 2; ++c) {
+        uint4 v;
+        v.x = pack_bf16(h[8 * c + 0], h[8 * c + 1]);
+        v.y = pack_bf16(h[8 * c + 2], h[8 * c + 3]);
+        v.z = pack_bf16(h[8 * c + 4], h[8 * c + 5]);
+        v.w = pack_bf16(h[8 * c + 6], h[8 * c + 7]);
+        *reinterpret_cast<uint4*>(sA + pu_off(row, 16 * q + 8 * c, PU_K)) = v;
+      }
     }
   }
+  return o;
 }
 
 template <bool GAMMA>
-__global__ void __launch_bounds__(PU_THREADS) k_precond_learned_umma(PuArgs a) {
+__global__ void __launch_bounds__(PU_THREADS, 5) k_precond_learned_umma(PuArgs a) {
   extern __shared__ uint8_t pu_raw[];
   __shared__ float sW4[HID];
   __shared__ float sB4;
@@ -668,8 +674,7 @@ __global__ void __launch_bounds__(PU_THREADS) k_precond_learned_umma(PuArgs a) {
   __shared__ double red[PU_THREADS / 32];
   __shared__ int abort_f;
   uint8_t* sA = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(pu_raw) + 15) & ~(uintptr_t)15);
-  uint8_t* sA1 = sA + PU_A;
-  uint8_t* sB1 = sA1 + PU_A1;
+  uint8_t* sB1 = sA + PU_A;
   uint8_t* sB2 = sB1 + PU_B1;
   uint8_t* sB3 = sB2 + PU_B;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -688,12 +693,11 @@ __global__ void __launch_bounds__(PU_THREADS) k_precond_learned_umma(PuArgs a) {
   }
   for (int i = tid; i < HID; i += PU_THREADS) sW4[i] = bf(P[O_W4 + i]);
   if (tid == 0) sB4 = bf(P[O_B4]);
-  // the constant columns of this thread's A rows: k = 64 (A) and k = 4 (A1) hold 1
+  // the constant columns of this thread's A row for layers 2 and 3: k = 64 holds 1
   {
     const uint32_t one = 0x3F80u;  // BF16 1.0
     *reinterpret_cast<uint4*>(sA + pu_off(tid, 64, PU_K)) = make_uint4(one, 0u, 0u, 0u);
     *reinterpret_cast<uint4*>(sA + pu_off(tid, 72, PU_K)) = make_uint4(0u, 0u, 0u, 0u);
-    *reinterpret_cast<uint4*>(sA1 + pu_off(tid, 8, PU_K1)) = make_uint4(0u, 0u, 0u, 0u);
   }
   if (tid == 0) {
     mbar_init(smem_u32(&bar), 1);
@@ -713,7 +717,8 @@ __global__ void __launch_bounds__(PU_THREADS) k_precond_learned_umma(PuArgs a) {
   const uint32_t tmem = tmem_slot;
   const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16);  // this warp's 32 lanes
   const uint32_t bar_a = smem_u32(&bar);
-  const uint64_t dA1 = pu_desc(smem_u32(sA1), PU_K1), dB1 = pu_desc(smem_u32(sB1), PU_K1);
+  // layer 1 reads the first 16 columns of A (its features, a 1 at k = 4, zeros)
+  const uint64_t dA1 = pu_desc(smem_u32(sA), PU_K), dB1 = pu_desc(smem_u32(sB1), PU_K1);
   const uint32_t aA = smem_u32(sA), aB2 = smem_u32(sB2), aB3 = smem_u32(sB3);
   uint32_t parity = 0;
 
@@ -743,68 +748,40 @@ __global__ void __launch_bounds__(PU_THREADS) k_precond_learned_umma(PuArgs a) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   };
 
-  // a tile's inputs: its row's band, statistics and eigenvalue, this
-  // thread's residual coefficient and kinetic energy. The next tile's are
-  // loaded before the current tile's MMA chain, so their latency (a
-  // dependent chain sel -> band -> row) overlaps the network.
-  struct TileIn {
-    int row, tile, k, s, b;
-    bool plain, valid;
-    double tbv, rrms, eps, tg;
-    cplx<double> rv;
-  };
-  auto fetch = [&](int w) {
-    TileIn in;
-    in.row = w / a.tiles;
-    in.tile = w - in.row * a.tiles;
-    in.k = in.row / a.n_add;
-    in.s = in.row - in.k * a.n_add;
-    in.b = a.sel[(int64_t)in.k * a.n_add + in.s];
-    in.plain = a.tpa_only && a.tpa_only[(int64_t)in.k * a.nb + in.b];
-    in.tbv = a.stats[2 * in.row];
-    in.rrms = a.stats[2 * in.row + 1];
-    in.eps = a.eig[(int64_t)in.k * a.nb + in.b];
-    const int gi = in.tile * PU_TILE + tid;
-    in.valid = gi < a.npw;
-    in.rv = mk<double>(0.0, 0.0);
-    in.tg = 0.0;
-    if (in.valid) {
-      in.tg = a.t[(int64_t)in.k * a.npw + gi];
+  for (int w = blockIdx.x; w < a.total; w += gridDim.x) {
+    const int row = w / a.tiles, tile = w - row * a.tiles;
+    const int k = row / a.n_add, s = row - k * a.n_add;
+    const int b = a.sel[(int64_t)k * a.n_add + s];
+    const bool plain = a.tpa_only && a.tpa_only[(int64_t)k * a.nb + b];
+    const double tbv = a.stats[2 * row], rrms = a.stats[2 * row + 1], eps = a.eig[(int64_t)k * a.nb + b];
+    const int gi = tile * PU_TILE + tid;
+    const bool valid = gi < a.npw;
+    cplx<double> rv = mk<double>(0.0, 0.0);
+    double tg = 0.0;
+    if (valid) {
+      tg = a.t[(int64_t)k * a.npw + gi];
       if (GAMMA) {
-        const double* rr = static_cast<const double*>(a.r) + (int64_t)in.b * a.r_row;
-        in.rv = gi == 0 ? mk<double>(rr[0], 0.0) : mk<double>(rr[2 * gi - 1], rr[2 * gi]);
+        const double* rr = static_cast<const double*>(a.r) + (int64_t)b * a.r_row;
+        rv = gi == 0 ? mk<double>(rr[0], 0.0) : mk<double>(rr[2 * gi - 1], rr[2 * gi]);
       } else {
-        in.rv = static_cast<const cplx<double>*>(a.r)[in.k * a.rk + (int64_t)in.b * a.npw + gi];
+        rv = static_cast<const cplx<double>*>(a.r)[k * a.rk + (int64_t)b * a.npw + gi];
       }
     }
-    return in;
-  };
-  TileIn nxt;
-  if (blockIdx.x < a.total) nxt = fetch(blockIdx.x);
-  for (int w = blockIdx.x; w < a.total; w += gridDim.x) {
-    const TileIn cur = nxt;
-    if (w + (int)gridDim.x < a.total) nxt = fetch(w + gridDim.x);
-    const int row = cur.row, tile = cur.tile, k = cur.k, s = cur.s;
-    const bool plain = cur.plain, valid = cur.valid;
-    const double tbv = cur.tbv, rrms = cur.rrms, eps = cur.eps, tg = cur.tg;
-    const cplx<double> rv = cur.rv;
-    const int gi = tile * PU_TILE + tid;
     double c = tpa_coeff(tg, tbv);
     if (!plain) {
       float u[NIN] = {0.f, 0.f, 0.f, 0.f};
       if (valid) features(tg, tbv, eps, sqrt(norm2(rv)), rrms, u);
-      *reinterpret_cast<uint4*>(sA1 + pu_off(tid, 0, PU_K1)) =
+      // layer 1's inputs in the first two chunks of A (the second zero: the
+      // previous tile left activations there)
+      *reinterpret_cast<uint4*>(sA + pu_off(tid, 0, PU_K)) =
           make_uint4(pack_bf16(u[0], u[1]), pack_bf16(u[2], u[3]), pack_bf16(1.f, 0.f), 0u);
-      float h[HID];
+      *reinterpret_cast<uint4*>(sA + pu_off(tid, 8, PU_K)) = make_uint4(0u, 0u, 0u, 0u);
       layer(1);
-      pu_hidden(taddr, sA, tid, h, false);
+      pu_hidden(taddr, sA, tid, sW4, false, 0.f);
       layer(2);
-      pu_hidden(taddr, sA, tid, h, false);
+      pu_hidden(taddr, sA, tid, sW4, false, 0.f);
       layer(3);
-      pu_hidden(taddr, sA, tid, h, true);
-      float o = sB4;
-#pragma unroll
-      for (int i = 0; i < HID; ++i) o = fmaf(bf(h[i]), sW4[i], o);
+      const float o = pu_hidden(taddr, sA, tid, sW4, true, sB4);
       if (rv.x != 0.0 || rv.y != 0.0) c *= (double)__expf(fminf(fmaxf(o, -3.f), 3.f));
     }
     double nn = 0.0;
@@ -922,7 +899,7 @@ __global__ void k_stall_update(const double* __restrict__ rn, double* __restrict
 }
 
 // The tcgen05 inference kernel over all (row, tile) items: a persistent grid
-// of up to four CTAs per SM (47 KB of shared memory and 64 TMEM columns each).
+// of up to five CTAs per SM (43 KB of shared memory and 64 TMEM columns each).
 template <bool GAMMA>
 int precond_umma(const float* params, int nb, int n_add, int npw, const void* r, int64_t rk, int64_t r_row,
                  const double* t, const double* eig, const int* sel, const uint8_t* tpa_only, const double* stats,
@@ -954,7 +931,7 @@ int precond_umma(const float* params, int nb, int n_add, int npw, const void* r,
   GWB_CUDA_TRY(cudaFuncSetAttribute(k_precond_learned_umma<GAMMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     PU_SMEM));
   GWB_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), st));
-  const int grid = std::min(a.total, 4 * sms);
+  const int grid = std::min(a.total, 5 * sms);
   k_precond_learned_umma<GAMMA><<<grid, PU_THREADS, PU_SMEM, st>>>(a);
   GWB_LAUNCH_CHECK();
   return GWB_OK;
